@@ -1,0 +1,257 @@
+"""AFMM2D on B200: Python mirror of the reference ``AFMM`` interface.
+
+The reference (vaishna77/AFMM2D, include/AFMM2D.hpp:14-33) exposes
+
+    AFMM(int N, int MinParticlesInLeaf, int TOL_POW, Eigen::MatrixXd& loc)
+    void assemble()
+    Eigen::VectorXd computeMatVecProduct(Eigen::VectorXd)
+    void evaluateError()
+    double* sorted_Locations, *sorted_Properties;  unsigned nLevels
+
+with the kernel supplied as ``userkernel::getMatrixEntry``.  This module
+offers the same class over the C ABI of ``libafmm2d.so`` (include/afmm2d.h);
+every computation runs in the CUDA library, and importing fails loudly when
+the library is missing.  The kernel is chosen by name or id (``KERNELS``).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["AFMM", "AFMMError", "KERNELS", "PRECISIONS", "lib", "nlevels"]
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libafmm2d.so")
+
+KERNELS = {"one_over_r_scaled": 0, "log": 1, "one_over_r": 2, "gaussian": 3}
+PRECISIONS = {"fp64": 0, "mixed": 1}
+STATUS = {0: "ok", 1: "bad argument", 2: "out of device memory", 3: "CUDA error", 4: "device wait timed out",
+          5: "non-finite values", 6: "not assembled", 7: "no sm_100 device"}
+
+_vp, _i, _i64, _u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_uint64
+_SIGS = {
+    "afmm_create": [_i, _i, _i, _vp, _i, _i, _vp, _i, _vp],
+    "afmm_assemble": [_vp],
+    "afmm_matvec": [_vp, _vp, _vp, _i, _i64, _i, _i],
+    "afmm_eval_error": [_vp, _i, _u64, _vp],
+    "afmm_get_permutation": [_vp, _vp],
+    "afmm_get_sorted_locations": [_vp, _vp],
+    "afmm_get_nlevels": [_vp, _vp],
+    "afmm_get_leaves": [_vp, _vp, _vp],
+    "afmm_get_lists": [_vp, _i, _vp, _vp, _vp],
+    "afmm_get_ranks": [_vp, _i, _vp],
+    "afmm_get_skeletons": [_vp, _i, _vp, _vp],
+    "afmm_get_charge_points": [_vp, _i, _vp, _vp],
+    "afmm_get_l2p": [_vp, _i, _i, _vp, _vp, _vp],
+    "afmm_set_profiling": [_vp, _i],
+    "afmm_get_stage_times": [_vp, _i, _vp, _vp, _vp],
+    "afmm_get_setup_times": [_vp, _vp],
+    "afmm_get_counts": [_vp, _vp],
+    "afmm_get_launch_count": [_vp, _vp],
+    "afmm_get_stream": [_vp, _vp],
+    "afmm_destroy": [_vp],
+}
+_lib = None
+
+
+class AFMMError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    """Loads ``libafmm2d.so`` (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m afmm2d_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _i
+        L.afmm_last_error.argtypes = [_vp]
+        L.afmm_last_error.restype = ctypes.c_char_p
+        L.afmm_status_string.argtypes = [_i]
+        L.afmm_status_string.restype = ctypes.c_char_p
+        L.afmm_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _check(st, h=None):
+    if st != 0:
+        raise AFMMError(st, lib().afmm_last_error(h).decode())
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def nlevels(N, M):
+    """nLevels exactly as src/AFMM2D.cpp:7 computes it (integer N/M, truncated)."""
+    if N <= 0 or M <= 0 or N // M < 1:
+        return -1
+    return int(np.log(float(N // M)) / np.log(4.0))
+
+
+class AFMM:
+    """AFMM(N, MinParticlesInLeaf, TOL_POW, loc, kernel="log", kparam=None).
+
+    ``loc`` is an (N, 2) array of point coordinates (the reference's
+    ``Eigen::MatrixXd loc(N, 2)``).  Construction builds the KD-tree
+    permutation and the interaction lists on the GPU (src/AFMM2D.cpp:3-39).
+    """
+
+    def __init__(self, N, MinParticlesInLeaf, TOL_POW, loc, kernel="log", kparam=None):
+        L = lib()
+        kid = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+        loc = np.ascontiguousarray(np.asarray(loc, dtype=np.float64).reshape(N, 2))
+        kp = np.array([kparam if kparam is not None else 0.01], dtype=np.float64)
+        h = ctypes.c_void_p()
+        st = L.afmm_create(int(N), int(MinParticlesInLeaf), int(TOL_POW), _ptr(loc), 1, kid, _ptr(kp),
+                           1 if kparam is not None else 0, ctypes.byref(h))
+        _check(st, None)
+        self._h = h
+        self.N = int(N)
+        self.MinParticlesInLeaf = int(MinParticlesInLeaf)
+        self.TOL_POW = int(TOL_POW)
+        self.kernel_id = kid
+        n = ctypes.c_int()
+        _check(L.afmm_get_nlevels(h, ctypes.byref(n)), h)
+        self.nLevels = n.value
+        self.assembled = False
+
+    # ------------------------------------------------------- reference API
+    def assemble(self):
+        """ACA skeletons, L2P and M2L blocks of every box (src/AFMM2D.cpp:41-44)."""
+        _check(lib().afmm_assemble(self._h), self._h)
+        self.assembled = True
+
+    def computeMatVecProduct(self, b, precision="fp64"):
+        """y = K b in the original point order (src/AFMM2D.cpp:46-65)."""
+        b = np.ascontiguousarray(np.asarray(b, dtype=np.float64))
+        nrhs = 1 if b.ndim == 1 else b.shape[1]
+        q = np.asfortranarray(b.reshape(self.N, nrhs))
+        y = np.zeros((self.N, nrhs), dtype=np.float64, order="F")
+        _check(lib().afmm_matvec(self._h, _ptr(q), _ptr(y), nrhs, self.N, PRECISIONS[precision], 0), self._h)
+        return y[:, 0] if b.ndim == 1 else y
+
+    def evaluateError(self, nsample=1, seed=0):
+        """Relative error of the last FP64 matvec against direct evaluation over
+        ``nsample`` seeded leaves (src/AFMM2D.cpp:67-74; all leaves if <= 0)."""
+        e = ctypes.c_double()
+        _check(lib().afmm_eval_error(self._h, int(nsample), int(seed), ctypes.byref(e)), self._h)
+        return e.value
+
+    @property
+    def sorted_Properties(self):
+        """Original index of each sorted point, as doubles (include/AFMM2D.hpp:25)."""
+        return self.permutation().astype(np.float64)
+
+    @property
+    def sorted_Locations(self):
+        """Sorted locations, interleaved x, y (include/AFMM2D.hpp:24)."""
+        xy = np.zeros(2 * self.N)
+        _check(lib().afmm_get_sorted_locations(self._h, _ptr(xy)), self._h)
+        return xy
+
+    # ------------------------------------------------------------- extras
+    def matvec_device(self, q_ptr, y_ptr, nrhs, ld, precision="fp64"):
+        """y = K q with device pointers (e.g. torch ``data_ptr()``), column-major N x nrhs."""
+        _check(lib().afmm_matvec(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(y_ptr), int(nrhs), int(ld),
+                                 PRECISIONS[precision], 1), self._h)
+
+    def matvec_host_ptr(self, q_ptr, y_ptr, nrhs, ld, precision="fp64"):
+        """y = K q with host pointers (e.g. pinned memory)."""
+        _check(lib().afmm_matvec(self._h, ctypes.c_void_p(q_ptr), ctypes.c_void_p(y_ptr), int(nrhs), int(ld),
+                                 PRECISIONS[precision], 0), self._h)
+
+    def permutation(self):
+        p = np.zeros(self.N, dtype=np.int64)
+        _check(lib().afmm_get_permutation(self._h, _ptr(p)), self._h)
+        return p
+
+    def leaves(self):
+        n = 4 ** self.nLevels
+        c = np.zeros(n, np.int32)
+        b = np.zeros(n, np.int32)
+        _check(lib().afmm_get_leaves(self._h, _ptr(c), _ptr(b)), self._h)
+        return c, b
+
+    def lists(self, level):
+        n = 4 ** level
+        a = [np.zeros(n * s, np.int32) for s in (8, 16, 24)]
+        _check(lib().afmm_get_lists(self._h, int(level), *[_ptr(x) for x in a]), self._h)
+        return a
+
+    def ranks(self, level):
+        r = np.zeros(4 ** level, np.int32)
+        _check(lib().afmm_get_ranks(self._h, int(level), _ptr(r)), self._h)
+        return r
+
+    def _ids(self, fn, level):
+        c = ctypes.c_int64()
+        _check(fn(self._h, int(level), None, ctypes.byref(c)), self._h)
+        ids = np.zeros(max(c.value, 1), np.int32)
+        _check(fn(self._h, int(level), _ptr(ids), ctypes.byref(c)), self._h)
+        return ids[: c.value]
+
+    def skeletons(self, level):
+        return self._ids(lib().afmm_get_skeletons, level)
+
+    def charge_points(self, level):
+        return self._ids(lib().afmm_get_charge_points, level)
+
+    def l2p(self, level, k):
+        r, c = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().afmm_get_l2p(self._h, int(level), int(k), ctypes.byref(r), ctypes.byref(c), None), self._h)
+        out = np.zeros((r.value, c.value))
+        if r.value * c.value:
+            _check(lib().afmm_get_l2p(self._h, int(level), int(k), ctypes.byref(r), ctypes.byref(c), _ptr(out)),
+                   self._h)
+        return out
+
+    def set_profiling(self, on=True):
+        _check(lib().afmm_set_profiling(self._h, 1 if on else 0), self._h)
+
+    def stage_times(self):
+        """Per-stage device milliseconds of the last matvec (profiling on)."""
+        n = ctypes.c_int()
+        names = (ctypes.c_char_p * 64)()
+        ms = (ctypes.c_double * 64)()
+        _check(lib().afmm_get_stage_times(self._h, 64, names, ms, ctypes.byref(n)), self._h)
+        return {names[i].decode(): ms[i] for i in range(min(n.value, 64))}
+
+    def setup_times(self):
+        t = np.zeros(2)
+        _check(lib().afmm_get_setup_times(self._h, _ptr(t)), self._h)
+        return {"create_s": t[0], "assemble_s": t[1]}
+
+    def counts(self):
+        c = np.zeros(7, np.int64)
+        _check(lib().afmm_get_counts(self._h, _ptr(c)), self._h)
+        keys = ["nlevels", "N", "sum_rank", "l2p_entries", "m2l_entries", "near_evals", "far_entries"]
+        return dict(zip(keys, c.tolist()))
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        _check(lib().afmm_get_launch_count(self._h, ctypes.byref(n)), self._h)
+        return n.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        _check(lib().afmm_get_stream(self._h, ctypes.byref(s)), self._h)
+        return s.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().afmm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

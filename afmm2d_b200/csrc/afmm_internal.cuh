@@ -1,0 +1,186 @@
+// Internal declarations shared by the AFMM2D B200 kernels and the C-ABI layer.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/afmm2d.h"
+
+namespace afmm {
+
+// ------------------------------------------------------------------ errors
+struct Error {
+  afmm_status status;
+  std::string msg;
+};
+
+#define AFMM_CUDA(call)                                                                      \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ::afmm::Error{AFMM_CUDA_ERR, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+  } while (0)
+
+#define AFMM_LAUNCH_CHECK() AFMM_CUDA(cudaGetLastError())
+
+// ----------------------------------------------------------------- kernels
+// User kernels of the reference are `double userkernel::getMatrixEntry(i, j)`
+// (include/kernel.hpp:58) reading particles_X[i], particles_X[j] and the
+// smallest box size `a` (src/AFMM2DTree.cpp:19).  Here a kernel is a functor
+// of the two points' coordinates.  `eval_exact` reproduces the reference's
+// double arithmetic operation by operation (no FMA contraction, IEEE sqrt and
+// division) and is used wherever results steer pivoting (ACA, L2P, M2L
+// blocks).  `eval` is the fast FP64 form for the matvec, `eval32` the FP32
+// form for the mixed-precision matvec: it receives dx, dy already reduced to
+// small numbers (coordinates relative to box anchors).
+struct KernelParams {
+  int id;
+  double a;      // 2^-L
+  double param;  // Gaussian: exp(-R2 / param)
+};
+
+__device__ __forceinline__ double r2_exact(double xi, double yi, double xj, double yj) {
+  double dx = __dsub_rn(xi, xj), dy = __dsub_rn(yi, yj);
+  return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+// One over r, scaled (examples/testAFMM2D.cpp:9-20): R < a ? R/a : a/R.
+struct KOneOverRScaled {
+  static constexpr int id = AFMM_KERNEL_ONE_OVER_R_SCALED;
+  __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
+    double R = __dsqrt_rn(R2);
+    return (R < p.a) ? __ddiv_rn(R, p.a) : __ddiv_rn(p.a, R);
+  }
+  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) {
+    double R = sqrt(R2);
+    return (R < p.a) ? R / p.a : p.a / R;
+  }
+  __device__ __forceinline__ static float eval32(float R2, float a, float) {
+    float R = sqrtf(R2);
+    return (R < a) ? R * (1.0f / a) : a * rsqrtf(R2);
+  }
+};
+
+// log(r) with the diagonal convention (examples/tutorial.cpp:22-35).
+struct KLog {
+  static constexpr int id = AFMM_KERNEL_LOG;
+  __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
+    if (R2 < 1e-10) return 0.0;
+    if (R2 < __dmul_rn(p.a, p.a)) return __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(0.5, R2), log(R2)), p.a), p.a);
+    return __dmul_rn(0.5, log(R2));
+  }
+  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return eval_exact(R2, p); }
+  __device__ __forceinline__ static float eval32(float R2, float a, float) {
+    if (R2 < 1e-10f) return 0.0f;
+    float l = __logf(R2);
+    if (R2 < a * a) return 0.5f * R2 * l / (a * a);
+    return 0.5f * l;
+  }
+};
+
+// 1/r with 0 at r = 0.
+struct KOneOverR {
+  static constexpr int id = AFMM_KERNEL_ONE_OVER_R;
+  __device__ __forceinline__ static double eval_exact(double R2, const KernelParams&) {
+    if (R2 == 0.0) return 0.0;
+    return __ddiv_rn(1.0, __dsqrt_rn(R2));
+  }
+  __device__ __forceinline__ static double eval(double R2, const KernelParams&) {
+    return R2 == 0.0 ? 0.0 : rsqrt(R2);
+  }
+  __device__ __forceinline__ static float eval32(float R2, float, float) {
+    return R2 == 0.0f ? 0.0f : rsqrtf(R2);
+  }
+};
+
+// Gaussian exp(-R2/param) (1 on the diagonal).
+struct KGaussian {
+  static constexpr int id = AFMM_KERNEL_GAUSSIAN;
+  __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
+    return exp(-__ddiv_rn(R2, p.param));
+  }
+  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return exp(-R2 / p.param); }
+  __device__ __forceinline__ static float eval32(float R2, float, float inv_param) {
+    return __expf(-R2 * inv_param);
+  }
+};
+
+// Calls F::template run<K>(args...) for the kernel id.
+template <template <class> class F, class... Args>
+void dispatch_kernel(int id, Args&&... args) {
+  switch (id) {
+    case AFMM_KERNEL_ONE_OVER_R_SCALED: F<KOneOverRScaled>::run(args...); break;
+    case AFMM_KERNEL_LOG: F<KLog>::run(args...); break;
+    case AFMM_KERNEL_ONE_OVER_R: F<KOneOverR>::run(args...); break;
+    case AFMM_KERNEL_GAUSSIAN: F<KGaussian>::run(args...); break;
+    default: throw Error{AFMM_BAD_ARG, "unknown kernel id"};
+  }
+}
+
+// ------------------------------------------------------------- allocation
+// Device allocations owned by a handle; freed together.
+struct DevArena {
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  template <class T>
+  T* alloc(size_t n) {
+    if (n == 0) n = 1;
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{AFMM_OOM, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed"};
+    }
+    ptrs.push_back(p);
+    bytes += n * sizeof(T);
+    return (T*)p;
+  }
+  void release(void* p) {
+    for (auto& q : ptrs)
+      if (q == p) {
+        cudaFree(q);
+        q = nullptr;
+      }
+  }
+  ~DevArena() {
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+  }
+};
+
+// ------------------------------------------------------------- tree layout
+// Per level j (4^j boxes, quadtree numbering k: parent k/4, children 4k+c).
+struct LevelDev {
+  long nbox = 0;
+  int32_t* il = nullptr;        // nbox*40: inner slots 0..15 then outer 0..23, -1 = none
+  int32_t* nbr = nullptr;       // nbox*8 neighbour slots (leaf level)
+  int32_t* node_off = nullptr;  // nbox+1 prefix over box node counts
+  int32_t* node_ids = nullptr;  // node lists (sorted-point ids)
+  int32_t* rank = nullptr;      // nbox
+  int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
+  int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
+  int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)
+  double2* skel_xy = nullptr;   // skeleton coordinates
+  int64_t* l2p_off = nullptr;   // nbox+1 prefix over n_b*r_b
+  double* l2p = nullptr;        // per box n_b x r_b, column-major (row index fastest)
+  float* l2p32 = nullptr;
+  double2* anchor = nullptr;    // per box reference point for FP32 relative coordinates
+  float2* skel_rel = nullptr;   // skeleton coordinates minus the box anchor (FP32)
+  int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c
+  double* m2l = nullptr;        // per box, per valid slot, block r_b x r_c column-major
+  double* qhat = nullptr;       // outgoing charges, skel_off layout
+  double* yhat = nullptr;       // incoming potentials, skel_off layout
+  float* qhat32 = nullptr;
+  float* yhat32 = nullptr;
+  // host copies
+  std::vector<int32_t> h_rank, h_skel_off;
+  std::vector<int32_t> h_node_off;
+  std::vector<int64_t> h_l2p_off, h_m2l_off;
+  int n1max = 0, rmax = 0;
+  long total_rank = 0;
+};
+
+}  // namespace afmm

@@ -1,0 +1,674 @@
+// C ABI of the AFMM2D B200 engine (include/afmm2d.h): handle, setup
+// orchestration and matvec dispatch.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "aca.cuh"
+#include "afmm_internal.cuh"
+#include "fmm.cuh"
+#include "kd_sort.cuh"
+#include "mixed.cuh"
+
+using namespace afmm;
+
+struct afmm_handle {
+  int N = 0, M = 0, tol_pow = 0, L = 0, kernel_id = 0;
+  KernelParams kp{};
+  cudaStream_t stream = nullptr;
+  DevArena arena;
+  double2* d_pts = nullptr;
+  int64_t* d_perm = nullptr;
+  std::vector<int32_t> h_counts, h_boxnum;          // DFS order
+  std::vector<int32_t> h_leaf_start, h_leaf_cnt;    // quadtree order
+  int32_t* d_leaf_start = nullptr;
+  int32_t* d_leaf_cnt = nullptr;
+  std::vector<LevelDev> lv;
+  std::vector<std::vector<int32_t>> h_il;
+  bool assembled = false;
+  double* d_qs = nullptr;
+  double* d_ys = nullptr;
+  double* d_q = nullptr;
+  double* d_y = nullptr;
+  MatvecPlan plan;
+  MixedState mixed;
+  StageTimer timer;
+  bool profiling = false;
+  std::vector<std::pair<std::string, double>> stage_ms;
+  double t_create = 0, t_assemble = 0;
+  int64_t launches = 0;
+  int64_t counts[7] = {0, 0, 0, 0, 0, 0, 0};
+  bool have_last = false;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <class F>
+afmm_status guard(afmm_handle* h, F&& f) {
+  try {
+    f();
+    return AFMM_OK;
+  } catch (const Error& e) {
+    (h ? h->err : g_err) = e.msg;
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    (h ? h->err : g_err) = "host allocation failed";
+    return AFMM_OOM;
+  } catch (const std::exception& e) {
+    (h ? h->err : g_err) = e.what();
+    return AFMM_CUDA_ERR;
+  }
+}
+
+// src/AFMM2D.cpp:7 -- nLevels = log(N/M)/log(4) with integer N/M, truncated.
+int n_levels(int N, int M) {
+  if (N <= 0 || M <= 0 || N / M < 1) return -1;
+  unsigned L = std::log(N / M) / std::log(4);
+  return (int)L;
+}
+
+void check_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    throw Error{AFMM_NO_DEVICE, "no CUDA device available"};
+  }
+  int dev = 0;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  cudaDeviceProp p;
+  AFMM_CUDA(cudaGetDeviceProperties(&p, dev));
+  if (p.major != 10) throw Error{AFMM_NO_DEVICE, std::string("device is not sm_100 (B200): ") + p.name};
+}
+
+// Splitmix64, for the seeded choice of leaves in afmm_eval_error.
+uint64_t splitmix(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ull);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+
+// Direct FP64 potentials at selected sorted points, Neumaier-compensated.
+template <class K>
+__global__ void k_dense_rows(const double2* __restrict__ pts, const double* __restrict__ qs, int N,
+                             const int32_t* __restrict__ rows, KernelParams kp, double* out) {
+  const int t = blockIdx.x;
+  const double2 xi = pts[rows[t]];
+  double s = 0.0, c = 0.0;
+  for (int j = threadIdx.x; j < N; j += blockDim.x) {
+    double v = K::eval_exact(r2_exact(xi.x, xi.y, pts[j].x, pts[j].y), kp) * qs[j];
+    double tt = s + v;
+    c += (fabs(s) >= fabs(v)) ? ((s - tt) + v) : ((v - tt) + s);
+    s = tt;
+  }
+  __shared__ double ss[256], sc[256];
+  ss[threadIdx.x] = s;
+  sc[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double S = 0.0, Cc = 0.0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      double v = ss[i];
+      double tt = S + v;
+      Cc += (fabs(S) >= fabs(v)) ? ((S - tt) + v) : ((v - tt) + S);
+      S = tt;
+      Cc += sc[i];
+    }
+    out[t] = S + Cc;
+  }
+}
+
+template <class K>
+struct DenseRun {
+  static void run(const double2* pts, const double* qs, int N, const int32_t* rows, int nrows, KernelParams kp,
+                  double* out, cudaStream_t s) {
+    k_dense_rows<K><<<nrows, 256, 0, s>>>(pts, qs, N, rows, kp, out);
+    AFMM_LAUNCH_CHECK();
+  }
+};
+
+void build_plan(afmm_handle* h) {
+  MatvecPlan& p = h->plan;
+  p.N = h->N;
+  p.L = h->L;
+  p.kp = h->kp;
+  p.perm = h->d_perm;
+  p.qs = h->d_qs;
+  p.ys = h->d_ys;
+  for (int j = 0; j <= h->L; ++j) {
+    LevelDev& d = h->lv[j];
+    LevelView& v = p.lv[j];
+    v = LevelView();
+    v.nbox = d.nbox;
+    v.il = d.il;
+    v.rank = d.rank;
+    v.skel_off = d.skel_off;
+    v.node_off = d.node_off;
+    v.leaf_start = (j == h->L) ? h->d_leaf_start : nullptr;
+    v.l2p_off = d.l2p_off;
+    v.l2p = d.l2p;
+    v.l2p32 = d.l2p32;
+    v.m2l_off = d.m2l_off;
+    v.m2l = d.m2l;
+    v.skel_xy = d.skel_xy;
+    v.skel_rel = d.skel_rel;
+    v.anchor = d.anchor;
+    v.qhat = d.qhat;
+    v.yhat = d.yhat;
+    v.qhat32 = d.qhat32;
+    v.yhat32 = d.yhat32;
+  }
+  p.levels.nlev = 0;
+  for (int j = 2; j <= h->L; ++j) p.levels.lv[p.levels.nlev++] = p.lv[j];
+  NearView& nv = p.near;
+  nv.nleaf = h->lv[h->L].nbox;
+  nv.nmax = *std::max_element(h->h_leaf_cnt.begin(), h->h_leaf_cnt.end());
+  nv.pts = h->d_pts;
+  nv.leaf_start = h->d_leaf_start;
+  nv.leaf_cnt = h->d_leaf_cnt;
+  nv.nbr = h->lv[h->L].nbr;
+}
+
+void do_create(afmm_handle* h, const double* loc, int layout) {
+  const int N = h->N, L = h->L;
+  std::vector<double> xy(2 * (size_t)N);
+  for (int i = 0; i < N; ++i) {
+    double x = layout == AFMM_LOC_COLMAJOR ? loc[i] : loc[2 * (size_t)i];
+    double y = layout == AFMM_LOC_COLMAJOR ? loc[(size_t)N + i] : loc[2 * (size_t)i + 1];
+    if (!std::isfinite(x) || !std::isfinite(y))
+      throw Error{AFMM_BAD_ARG, "point " + std::to_string(i) + " has a non-finite coordinate"};
+    xy[2 * (size_t)i] = x;
+    xy[2 * (size_t)i + 1] = y;
+  }
+  if ((int64_t)N >= (1LL << 28)) throw Error{AFMM_BAD_ARG, "N must be below 2^28"};
+  {
+    auto sz = kd_segment_sizes(N, L);
+    int64_t nmax = *std::max_element(sz[L].begin(), sz[L].end());
+    if (nmax > 1024) throw Error{AFMM_BAD_ARG, "leaf size " + std::to_string(nmax) + " exceeds 1024; use a smaller M"};
+  }
+  check_device();
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  cudaStream_t s = h->stream;
+  double* d_xy = h->arena.alloc<double>(2 * (size_t)N);
+  AFMM_CUDA(cudaMemcpyAsync(d_xy, xy.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
+  h->d_perm = h->arena.alloc<int64_t>(N);
+  h->d_pts = h->arena.alloc<double2>(N);
+  kd_sort_device(d_xy, N, L, h->d_perm, (double*)h->d_pts, s, &h->launches);
+  h->arena.release(d_xy);
+  // Leaf layout: DFS leaf d owns a contiguous sorted range; its quadtree box
+  // number follows src/KDTree.cpp:211-223 (children 4p+0, 4p+3, 4p+1, 4p+2).
+  auto sizes = kd_segment_sizes(N, L);
+  h->h_counts.assign(sizes[L].begin(), sizes[L].end());
+  std::vector<int32_t> bn(1, 0);
+  for (int j = 1; j <= L; ++j) {
+    std::vector<int32_t> nx;
+    nx.reserve(bn.size() * 4);
+    for (int32_t p : bn) {
+      nx.push_back(4 * p + 0);
+      nx.push_back(4 * p + 3);
+      nx.push_back(4 * p + 1);
+      nx.push_back(4 * p + 2);
+    }
+    bn.swap(nx);
+  }
+  h->h_boxnum = bn;
+  const long nleaf = (long)bn.size();
+  h->h_leaf_start.assign(nleaf, 0);
+  h->h_leaf_cnt.assign(nleaf, 0);
+  int64_t st = 0;
+  for (long d = 0; d < nleaf; ++d) {
+    h->h_leaf_start[bn[d]] = (int32_t)st;
+    h->h_leaf_cnt[bn[d]] = h->h_counts[d];
+    st += h->h_counts[d];
+  }
+  int nmax = *std::max_element(h->h_leaf_cnt.begin(), h->h_leaf_cnt.end());
+  if (nmax > 1024) throw Error{AFMM_BAD_ARG, "leaf size " + std::to_string(nmax) + " exceeds 1024; use a smaller M"};
+  h->d_leaf_start = h->arena.alloc<int32_t>(nleaf);
+  h->d_leaf_cnt = h->arena.alloc<int32_t>(nleaf);
+  AFMM_CUDA(cudaMemcpyAsync(h->d_leaf_start, h->h_leaf_start.data(), sizeof(int32_t) * nleaf, cudaMemcpyHostToDevice, s));
+  AFMM_CUDA(cudaMemcpyAsync(h->d_leaf_cnt, h->h_leaf_cnt.data(), sizeof(int32_t) * nleaf, cudaMemcpyHostToDevice, s));
+  // Interaction lists of every level (closed form on the device).
+  h->lv.resize(L + 1);
+  h->h_il.resize(L + 1);
+  for (int j = 0; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
+    v.nbox = 1L << (2 * j);
+    v.il = h->arena.alloc<int32_t>(v.nbox * 40);
+    v.nbr = h->arena.alloc<int32_t>(v.nbox * 8);
+    build_lists(j, v.nbox, v.nbr, v.il, s);
+    ++h->launches;
+    h->h_il[j].resize(v.nbox * 40);
+    AFMM_CUDA(cudaMemcpyAsync(h->h_il[j].data(), v.il, sizeof(int32_t) * v.nbox * 40, cudaMemcpyDeviceToHost, s));
+  }
+  // Leaf node lists (quadtree order): box k's nodes are its sorted range.
+  LevelDev& lf = h->lv[L];
+  lf.h_node_off.assign(nleaf + 1, 0);
+  for (long k = 0; k < nleaf; ++k) lf.h_node_off[k + 1] = lf.h_node_off[k] + h->h_leaf_cnt[k];
+  std::vector<int32_t> ids(N);
+  for (long k = 0; k < nleaf; ++k)
+    for (int i = 0; i < h->h_leaf_cnt[k]; ++i) ids[lf.h_node_off[k] + i] = h->h_leaf_start[k] + i;
+  lf.node_off = h->arena.alloc<int32_t>(nleaf + 1);
+  lf.node_ids = h->arena.alloc<int32_t>(N);
+  AFMM_CUDA(cudaMemcpyAsync(lf.node_off, lf.h_node_off.data(), sizeof(int32_t) * (nleaf + 1), cudaMemcpyHostToDevice, s));
+  AFMM_CUDA(cudaMemcpyAsync(lf.node_ids, ids.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
+  h->d_qs = h->arena.alloc<double>(N);
+  h->d_ys = h->arena.alloc<double>(N);
+  h->d_q = h->arena.alloc<double>(N);
+  h->d_y = h->arena.alloc<double>(N);
+  AFMM_CUDA(cudaStreamSynchronize(s));
+}
+
+void do_assemble(afmm_handle* h) {
+  cudaStream_t s = h->stream;
+  const int L = h->L;
+  double tol = std::pow(10, -1.0 * h->tol_pow);  // src/ACA.cpp:7
+  for (int j = L; j >= 2; --j) {
+    LevelDev& v = h->lv[j];
+    if (j < L) {
+      // a box's nodes are its children's skeletons (src/AFMM2DTree.cpp:997-1007)
+      LevelDev& c = h->lv[j + 1];
+      v.h_node_off.assign(v.nbox + 1, 0);
+      for (long b = 0; b <= v.nbox; ++b) v.h_node_off[b] = c.h_skel_off[4 * b];
+      v.node_off = h->arena.alloc<int32_t>(v.nbox + 1);
+      AFMM_CUDA(cudaMemcpyAsync(v.node_off, v.h_node_off.data(), sizeof(int32_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+      v.node_ids = c.skel_ids;
+    }
+    AcaLevelIn in;
+    in.nbox = v.nbox;
+    in.pts = h->d_pts;
+    in.node_off = v.node_off;
+    in.node_ids = v.node_ids;
+    in.il = v.il;
+    in.h_node_off = v.h_node_off;
+    in.tol = tol;
+    in.kp = h->kp;
+    int n1max = 0, n2max = 0;
+    const std::vector<int32_t>& il = h->h_il[j];
+    for (long b = 0; b < v.nbox; ++b) {
+      n1max = std::max(n1max, v.h_node_off[b + 1] - v.h_node_off[b]);
+      int n2 = 0;
+      for (int t = 0; t < 40; ++t) {
+        int c = il[b * 40 + t];
+        if (c >= 0) n2 += v.h_node_off[c + 1] - v.h_node_off[c];
+      }
+      n2max = std::max(n2max, n2);
+    }
+    in.n1max = n1max;
+    in.n2max = n2max;
+    v.rank = h->arena.alloc<int32_t>(v.nbox);
+    in.rank_out = v.rank;
+    AcaLevelOut out;
+    aca_level(in, out, h->arena, s, &h->launches);
+    v.skel_off = out.skel_off;
+    v.skel_ids = out.skel_ids;
+    v.cpiv_ids = out.cpiv_ids;
+    v.skel_xy = out.skel_xy;
+    v.l2p_off = out.l2p_off;
+    v.l2p = out.l2p;
+    v.h_rank = out.h_rank;
+    v.h_skel_off = out.h_skel_off;
+    v.h_l2p_off = out.h_l2p_off;
+    v.n1max = n1max;
+    v.rmax = out.rmax;
+    v.total_rank = out.h_skel_off[v.nbox];
+  }
+  // M2L blocks, levels 2..L
+  int64_t m2l_total = 0;
+  for (int j = 2; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
+    const std::vector<int32_t>& il = h->h_il[j];
+    v.h_m2l_off.assign(v.nbox + 1, 0);
+    for (long b = 0; b < v.nbox; ++b) {
+      int64_t e = 0;
+      for (int t = 0; t < 40; ++t) {
+        int c = il[b * 40 + t];
+        if (c >= 0) e += (int64_t)v.h_rank[b] * v.h_rank[c];
+      }
+      v.h_m2l_off[b + 1] = v.h_m2l_off[b] + e;
+    }
+    m2l_total += v.h_m2l_off[v.nbox];
+    v.m2l_off = h->arena.alloc<int64_t>(v.nbox + 1);
+    AFMM_CUDA(cudaMemcpyAsync(v.m2l_off, v.h_m2l_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+    v.m2l = h->arena.alloc<double>(v.h_m2l_off[v.nbox]);
+    v.qhat = h->arena.alloc<double>(v.total_rank);
+    v.yhat = h->arena.alloc<double>(v.total_rank);
+  }
+  build_plan(h);
+  for (int j = 2; j <= L; ++j) {
+    m2l_assemble(h->plan.lv[j], h->kp, s);
+    ++h->launches;
+  }
+  mixed_setup(h->plan, h->lv, h->mixed, h->arena, s, &h->launches);
+  build_plan(h);
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  // structure counts
+  int64_t sum_rank = 0, l2p_entries = 0;
+  for (int j = 2; j <= L; ++j) {
+    sum_rank += h->lv[j].total_rank;
+    l2p_entries += h->lv[j].h_l2p_off[h->lv[j].nbox];
+  }
+  int64_t near = 0;
+  const std::vector<int32_t>& il = h->h_il[L];
+  (void)il;
+  std::vector<int32_t> nbr(h->lv[L].nbox * 8);
+  AFMM_CUDA(cudaMemcpy(nbr.data(), h->lv[L].nbr, sizeof(int32_t) * nbr.size(), cudaMemcpyDeviceToHost));
+  for (long b = 0; b < h->lv[L].nbox; ++b) {
+    int64_t src = h->h_leaf_cnt[b];
+    for (int t = 0; t < 8; ++t)
+      if (nbr[b * 8 + t] >= 0) src += h->h_leaf_cnt[nbr[b * 8 + t]];
+    near += src * h->h_leaf_cnt[b];
+  }
+  h->counts[0] = L;
+  h->counts[1] = h->N;
+  h->counts[2] = sum_rank;
+  h->counts[3] = l2p_entries;
+  h->counts[4] = m2l_total;
+  h->counts[5] = near;
+  h->counts[6] = m2l_total;
+  h->assembled = true;
+}
+
+}  // namespace
+
+extern "C" {
+
+afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const double* loc, int loc_layout,
+                        int kernel_id, const double* kparams, int nkparams, afmm_handle** out) {
+  if (!out) {
+    g_err = "out is NULL";
+    return AFMM_BAD_ARG;
+  }
+  *out = nullptr;
+  afmm_handle* h = nullptr;
+  afmm_status st = guard(nullptr, [&] {
+    if (N < 1 || min_particles_in_leaf < 1) throw Error{AFMM_BAD_ARG, "N and MinParticlesInLeaf must be >= 1"};
+    if (!loc) throw Error{AFMM_BAD_ARG, "loc is NULL"};
+    if (loc_layout != AFMM_LOC_COLMAJOR && loc_layout != AFMM_LOC_INTERLEAVED) throw Error{AFMM_BAD_ARG, "bad loc_layout"};
+    if (kernel_id < 0 || kernel_id > AFMM_KERNEL_GAUSSIAN) throw Error{AFMM_BAD_ARG, "unknown kernel_id"};
+    int L = n_levels(N, min_particles_in_leaf);
+    if (L < 2)
+      throw Error{AFMM_BAD_ARG, "N/MinParticlesInLeaf gives nLevels = " + std::to_string(L) + " < 2"};
+    if (L >= kMaxLevels) throw Error{AFMM_BAD_ARG, "too many levels"};
+    double param = (kparams && nkparams > 0) ? kparams[0] : 0.01;
+    if (kernel_id == AFMM_KERNEL_GAUSSIAN && !(param > 0)) throw Error{AFMM_BAD_ARG, "Gaussian parameter must be > 0"};
+    h = new afmm_handle();
+    h->N = N;
+    h->M = min_particles_in_leaf;
+    h->tol_pow = tol_pow;
+    h->L = L;
+    h->kernel_id = kernel_id;
+    // a = boxRadius[L], halving from 1 (src/AFMM2DTree.cpp:14-19)
+    double a = 1.0;
+    for (int j = 0; j < L; ++j) a *= 0.5;
+    h->kp = KernelParams{kernel_id, a, param};
+    double t0 = now_s();
+    do_create(h, loc, loc_layout);
+    h->t_create = now_s() - t0;
+  });
+  if (st != AFMM_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return AFMM_OK;
+}
+
+afmm_status afmm_assemble(afmm_handle* h) {
+  if (!h) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    if (h->assembled) return;
+    double t0 = now_s();
+    do_assemble(h);
+    h->t_assemble = now_s() - t0;
+  });
+}
+
+afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int precision,
+                        int mem_device) {
+  if (!h) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_matvec before afmm_assemble"};
+    if (!q || !y || nrhs < 1 || ld < h->N) throw Error{AFMM_BAD_ARG, "bad q/y/nrhs/ld"};
+    if (precision != AFMM_PREC_FP64 && precision != AFMM_PREC_MIXED) throw Error{AFMM_BAD_ARG, "bad precision"};
+    cudaStream_t s = h->stream;
+    const size_t bytes = sizeof(double) * (size_t)h->N;
+    if (h->profiling) h->timer.reset();
+    StageTimer* tm = h->profiling ? &h->timer : nullptr;
+    if (precision == AFMM_PREC_MIXED) {
+      if (!mem_device) {
+        if (h->mixed.host_cap < (size_t)nrhs) mixed_reserve_io(h->mixed, h->N, nrhs, h->arena);
+        if (tm) tm->mark(s, "h2d");
+        for (int c = 0; c < nrhs; ++c)
+          AFMM_CUDA(cudaMemcpyAsync(h->mixed.d_qin + (size_t)c * h->N, q + (size_t)c * ld, bytes, cudaMemcpyHostToDevice, s));
+        matvec_mixed(h->plan, h->mixed, h->mixed.d_qin, h->N, h->mixed.d_yout, h->N, nrhs, s, tm, &h->launches);
+        if (tm) tm->mark(s, "d2h");
+        for (int c = 0; c < nrhs; ++c)
+          AFMM_CUDA(cudaMemcpyAsync(y + (size_t)c * ld, h->mixed.d_yout + (size_t)c * h->N, bytes, cudaMemcpyDeviceToHost, s));
+      } else {
+        matvec_mixed(h->plan, h->mixed, q, ld, y, ld, nrhs, s, tm, &h->launches);
+      }
+      if (tm) tm->mark(s, "end");
+    } else {
+      for (int c = 0; c < nrhs; ++c) {
+        const double* qc = q + (size_t)c * ld;
+        double* yc = y + (size_t)c * ld;
+        if (!mem_device) {
+          if (tm) tm->mark(s, "h2d");
+          AFMM_CUDA(cudaMemcpyAsync(h->d_q, qc, bytes, cudaMemcpyHostToDevice, s));
+          matvec_fp64(h->plan, h->d_q, h->d_y, s, tm, &h->launches);
+          if (tm) tm->mark(s, "d2h");
+          AFMM_CUDA(cudaMemcpyAsync(yc, h->d_y, bytes, cudaMemcpyDeviceToHost, s));
+          if (tm) tm->mark(s, "end");
+        } else {
+          matvec_fp64(h->plan, qc, yc, s, tm, &h->launches);
+        }
+      }
+      h->have_last = true;
+    }
+    AFMM_CUDA(cudaStreamSynchronize(s));
+    if (tm) tm->collect(h->stage_ms);
+  });
+}
+
+afmm_status afmm_eval_error(afmm_handle* h, int nsample, uint64_t seed, double* rel_err) {
+  if (!h || !rel_err) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    if (!h->have_last) throw Error{AFMM_BAD_ARG, "no FP64 matvec has been computed yet"};
+    const long nleaf = h->lv[h->L].nbox;
+    std::vector<long> leaves;
+    if (nsample <= 0 || nsample >= nleaf) {
+      for (long k = 0; k < nleaf; ++k) leaves.push_back(k);
+    } else {
+      std::vector<char> used(nleaf, 0);
+      uint64_t st = seed;
+      while ((int)leaves.size() < nsample) {
+        long k = (long)(splitmix(st) % (uint64_t)nleaf);
+        if (!used[k]) {
+          used[k] = 1;
+          leaves.push_back(k);
+        }
+      }
+    }
+    std::vector<int32_t> rows;
+    for (long k : leaves)
+      for (int i = 0; i < h->h_leaf_cnt[k]; ++i) rows.push_back(h->h_leaf_start[k] + i);
+    DevArena tmp;
+    int32_t* d_rows = tmp.alloc<int32_t>(rows.size());
+    double* d_out = tmp.alloc<double>(rows.size());
+    cudaStream_t s = h->stream;
+    AFMM_CUDA(cudaMemcpyAsync(d_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice, s));
+    dispatch_kernel<DenseRun>(h->kp.id, h->d_pts, h->d_qs, h->N, d_rows, (int)rows.size(), h->kp, d_out, s);
+    ++h->launches;
+    std::vector<double> dense(rows.size()), ys(h->N);
+    AFMM_CUDA(cudaMemcpyAsync(dense.data(), d_out, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, s));
+    AFMM_CUDA(cudaMemcpyAsync(ys.data(), h->d_ys, sizeof(double) * h->N, cudaMemcpyDeviceToHost, s));
+    AFMM_CUDA(cudaStreamSynchronize(s));
+    double num = 0, den = 0;
+    for (size_t t = 0; t < rows.size(); ++t) {
+      double d = ys[rows[t]] - dense[t];
+      num += d * d;
+      den += dense[t] * dense[t];
+    }
+    *rel_err = den > 0 ? std::sqrt(num / den) : std::sqrt(num);
+  });
+}
+
+afmm_status afmm_get_permutation(afmm_handle* h, int64_t* perm) {
+  if (!h || !perm) return AFMM_BAD_ARG;
+  return guard(h, [&] { AFMM_CUDA(cudaMemcpy(perm, h->d_perm, sizeof(int64_t) * h->N, cudaMemcpyDeviceToHost)); });
+}
+
+afmm_status afmm_get_sorted_locations(afmm_handle* h, double* xy) {
+  if (!h || !xy) return AFMM_BAD_ARG;
+  return guard(h, [&] { AFMM_CUDA(cudaMemcpy(xy, h->d_pts, sizeof(double) * 2 * h->N, cudaMemcpyDeviceToHost)); });
+}
+
+afmm_status afmm_get_nlevels(afmm_handle* h, int* nlevels) {
+  if (!h || !nlevels) return AFMM_BAD_ARG;
+  *nlevels = h->L;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_leaves(afmm_handle* h, int32_t* counts, int32_t* box_numbers) {
+  if (!h || !counts || !box_numbers) return AFMM_BAD_ARG;
+  std::copy(h->h_counts.begin(), h->h_counts.end(), counts);
+  std::copy(h->h_boxnum.begin(), h->h_boxnum.end(), box_numbers);
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_lists(afmm_handle* h, int level, int32_t* nbr, int32_t* inner, int32_t* outer) {
+  if (!h || level < 0 || level > h->L || !nbr || !inner || !outer) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    const LevelDev& v = h->lv[level];
+    AFMM_CUDA(cudaMemcpy(nbr, v.nbr, sizeof(int32_t) * v.nbox * 8, cudaMemcpyDeviceToHost));
+    const std::vector<int32_t>& il = h->h_il[level];
+    for (long b = 0; b < v.nbox; ++b) {
+      std::copy(il.begin() + b * 40, il.begin() + b * 40 + 16, inner + b * 16);
+      std::copy(il.begin() + b * 40 + 16, il.begin() + b * 40 + 40, outer + b * 24);
+    }
+  });
+}
+
+afmm_status afmm_get_ranks(afmm_handle* h, int level, int32_t* ranks) {
+  if (!h || !ranks || level < 2 || level > h->L) return AFMM_BAD_ARG;
+  if (!h->assembled) return AFMM_NOT_ASSEMBLED;
+  std::copy(h->lv[level].h_rank.begin(), h->lv[level].h_rank.end(), ranks);
+  return AFMM_OK;
+}
+
+static afmm_status get_ids(afmm_handle* h, int level, int32_t* ids, int64_t* count, bool skel) {
+  if (!h || !count || level < 2 || level > h->L) return AFMM_BAD_ARG;
+  if (!h->assembled) return AFMM_NOT_ASSEMBLED;
+  return guard(h, [&] {
+    const LevelDev& v = h->lv[level];
+    *count = v.total_rank;
+    if (ids && v.total_rank > 0)
+      AFMM_CUDA(cudaMemcpy(ids, skel ? v.skel_ids : v.cpiv_ids, sizeof(int32_t) * v.total_rank, cudaMemcpyDeviceToHost));
+  });
+}
+
+afmm_status afmm_get_skeletons(afmm_handle* h, int level, int32_t* ids, int64_t* count) {
+  return get_ids(h, level, ids, count, true);
+}
+
+afmm_status afmm_get_charge_points(afmm_handle* h, int level, int32_t* ids, int64_t* count) {
+  return get_ids(h, level, ids, count, false);
+}
+
+afmm_status afmm_get_l2p(afmm_handle* h, int level, int k, int32_t* rows, int32_t* cols, double* out) {
+  if (!h || !rows || !cols || level < 2 || level > h->L || k < 0 || k >= h->lv[level].nbox) return AFMM_BAD_ARG;
+  if (!h->assembled) return AFMM_NOT_ASSEMBLED;
+  return guard(h, [&] {
+    const LevelDev& v = h->lv[level];
+    int r = v.h_rank[k];
+    int n = v.h_node_off[k + 1] - v.h_node_off[k];
+    *rows = r ? n : 0;
+    *cols = r;
+    if (out && r) {
+      std::vector<double> cm((size_t)n * r);
+      AFMM_CUDA(cudaMemcpy(cm.data(), v.l2p + v.h_l2p_off[k], sizeof(double) * cm.size(), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < n; ++i)
+        for (int c = 0; c < r; ++c) out[(size_t)i * r + c] = cm[(size_t)c * n + i];
+    }
+  });
+}
+
+afmm_status afmm_set_profiling(afmm_handle* h, int on) {
+  if (!h) return AFMM_BAD_ARG;
+  h->profiling = on != 0;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_stage_times(afmm_handle* h, int cap, const char** names, double* ms, int* n) {
+  if (!h || !n) return AFMM_BAD_ARG;
+  *n = (int)h->stage_ms.size();
+  for (int i = 0; i < *n && i < cap; ++i) {
+    if (names) names[i] = h->stage_ms[i].first.c_str();
+    if (ms) ms[i] = h->stage_ms[i].second;
+  }
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_setup_times(afmm_handle* h, double* t2) {
+  if (!h || !t2) return AFMM_BAD_ARG;
+  t2[0] = h->t_create;
+  t2[1] = h->t_assemble;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_counts(afmm_handle* h, int64_t* c7) {
+  if (!h || !c7) return AFMM_BAD_ARG;
+  std::copy(h->counts, h->counts + 7, c7);
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_launch_count(afmm_handle* h, int64_t* n) {
+  if (!h || !n) return AFMM_BAD_ARG;
+  *n = h->launches;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_stream(afmm_handle* h, void** stream) {
+  if (!h || !stream) return AFMM_BAD_ARG;
+  *stream = (void*)h->stream;
+  return AFMM_OK;
+}
+
+afmm_status afmm_destroy(afmm_handle* h) {
+  if (!h) return AFMM_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  cudaStream_t s = h->stream;
+  delete h;
+  if (s) cudaStreamDestroy(s);
+  return AFMM_OK;
+}
+
+const char* afmm_status_string(afmm_status s) {
+  switch (s) {
+    case AFMM_OK: return "ok";
+    case AFMM_BAD_ARG: return "bad argument";
+    case AFMM_OOM: return "out of device memory";
+    case AFMM_CUDA_ERR: return "CUDA error";
+    case AFMM_TIMEOUT: return "device wait timed out";
+    case AFMM_NUMERIC: return "non-finite values";
+    case AFMM_NOT_ASSEMBLED: return "not assembled";
+    case AFMM_NO_DEVICE: return "no sm_100 device";
+  }
+  return "unknown status";
+}
+
+const char* afmm_last_error(afmm_handle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+const char* afmm_version(void) { return "afmm2d-b200 0.1"; }
+}

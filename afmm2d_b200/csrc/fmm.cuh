@@ -1,0 +1,104 @@
+// Tree views handed to the sweep kernels (see fmm.cu, mixed.cu).
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "afmm_internal.cuh"
+
+namespace afmm {
+
+constexpr int kMaxLevels = 16;
+
+// Device pointers of one level, passed by value to kernels.
+struct LevelView {
+  long nbox = 0;
+  const int32_t* il = nullptr;
+  const int32_t* rank = nullptr;
+  const int32_t* skel_off = nullptr;
+  const int32_t* node_off = nullptr;
+  const int32_t* leaf_start = nullptr;  // leaf level only (quadtree order)
+  const int64_t* l2p_off = nullptr;
+  const double* l2p = nullptr;
+  const float* l2p32 = nullptr;
+  const int64_t* m2l_off = nullptr;
+  double* m2l = nullptr;
+  const double2* skel_xy = nullptr;
+  const float2* skel_rel = nullptr;   // skeleton minus box anchor (FP32)
+  const double2* anchor = nullptr;    // box anchors (FP64)
+  double* qhat = nullptr;
+  double* yhat = nullptr;
+  float* qhat32 = nullptr;
+  float* yhat32 = nullptr;
+};
+
+struct LevelSet {
+  int nlev = 0;
+  LevelView lv[kMaxLevels];
+};
+
+// Leaf-level data for the near field.
+struct NearView {
+  long nleaf = 0;
+  int nmax = 0;
+  const double2* pts = nullptr;        // sorted points
+  const int32_t* leaf_start = nullptr; // quadtree order
+  const int32_t* leaf_cnt = nullptr;
+  const int32_t* nbr = nullptr;        // nleaf * 8
+  const double2* anchor = nullptr;     // leaf anchors (FP64)
+  const float2* rel = nullptr;         // point minus its leaf anchor (FP32), sorted order
+};
+
+// CUDA-event marks for per-stage device timing.
+struct StageTimer {
+  std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  size_t used = 0;
+  void reset() { used = 0; }
+  void mark(cudaStream_t s, const char* name) {
+    if (used == marks.size()) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      marks.push_back({name, e});
+    }
+    marks[used].first = name;
+    cudaEventRecord(marks[used].second, s);
+    ++used;
+  }
+  // durations between consecutive marks, accumulated by name
+  void collect(std::vector<std::pair<std::string, double>>& out) {
+    out.clear();
+    for (size_t i = 0; i + 1 < used; ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, marks[i].second, marks[i + 1].second);
+      bool found = false;
+      for (auto& o : out)
+        if (o.first == marks[i].first) {
+          o.second += ms;
+          found = true;
+        }
+      if (!found) out.push_back({marks[i].first, ms});
+    }
+  }
+  ~StageTimer() {
+    for (auto& m : marks) cudaEventDestroy(m.second);
+  }
+};
+
+struct MatvecPlan {
+  int N = 0, L = 0;
+  KernelParams kp;
+  const int64_t* perm = nullptr;
+  double* qs = nullptr;  // sorted charges
+  double* ys = nullptr;  // sorted potentials
+  float* qs32 = nullptr;
+  LevelView lv[kMaxLevels];
+  LevelSet levels;       // levels 2..L for the M2L launch
+  NearView near;
+};
+
+void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
+void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
+void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
+
+}  // namespace afmm

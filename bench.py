@@ -1,0 +1,292 @@
+#!/usr/bin/env python
+"""AFMM2D matvec benchmark on B200.
+
+One step = one matvec y = K q over the workload's N points (one right-hand
+side), with the assembled operators resident in HBM.  The default workload is
+the N = 4,194,304 Gaussian-mixture problem (16 components, sigma 0.02,
+kernel 1/r, M = 64, TOL_POW = 6); inputs are seeded synthetic data.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU: the path does not shard (one problem per GPU), so N ranks run N
+independent replicas; value = total points*RHS per second over all ranks,
+timed as the max over ranks.  --impl reference times the reference's own CPU
+code (compiled from its sources into oracle/_ref) on a bounded sample of the
+same workload on the host cores; under torchrun only rank 0 runs it.
+"""
+import argparse
+import csv
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "points*RHS/s per matvec at N=4M (mixture, 1/r, TOL 6)"
+UNIT = "points*RHS/s"
+CPU_SAMPLE_N = 65536
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="mixture4m")
+    ap.add_argument("--N", type=int, default=None, help="override N (same distribution)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
+    return ap.parse_args()
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r for r in csv.reader(self.f) if len(r) >= 9]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], d["bf16_tflops"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 1590.0, "fallback"
+
+
+def cpu_reference(name, n, steps, warmup):
+    """The reference's own OpenMP path (oracle/_ref) on a bounded sample."""
+    from afmm2d_b200 import workloads
+    from oracle_lib import RefLib
+    if not RefLib.available():
+        return None
+    pts, q, p = workloads.make(name, N=n)
+    t0 = time.perf_counter()
+    r = RefLib(pts, p["M"], p["tol"], p["kernel"])
+    r.assemble()
+    setup = time.perf_counter() - t0
+    for _ in range(warmup):
+        r.matvec(q)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r.matvec(q)
+    dt = (time.perf_counter() - t0) / steps
+    threads = r.lib.ref_num_threads()
+    return {"value": n / dt, "unit": UNIT, "cores": int(threads), "kind": "reference",
+            "sample": f"{name} at N={n} (same distribution, kernel, M, TOL), {steps} matvecs after {warmup} "
+                      f"warm-up, OpenMP {threads} threads; reference setup {setup:.1f} s",
+            "ms_per_step": dt * 1e3, "setup_s": setup}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    n = args.N or CPU_SAMPLE_N
+    res = cpu_reference(args.workload, n, max(args.steps, 1), max(args.warmup, 1))
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libafmm2d_ref.so was not built"}))
+        return
+    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": {"workload": args.workload, "N": n, "sample_of_N": 1 << 22},
+            "cpu_baseline": {k: res[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import afmm2d_b200 as A
+    from afmm2d_b200 import workloads
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    pts, q, p = workloads.make(args.workload, N=args.N)
+    N = len(pts)
+    t0 = time.perf_counter()
+    a = A.AFMM(N, p["M"], p["tol"], pts, kernel=p["kernel"])
+    a.assemble()
+    setup_s = time.perf_counter() - t0
+    st = a.setup_times()
+    counts = a.counts()
+    stream = torch.cuda.ExternalStream(a.stream())
+    dq = torch.from_numpy(q).to(f"cuda:{local}")
+    dy = torch.empty_like(dq)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
+
+    def timed(prec, steps, warm):
+        for _ in range(warm):
+            a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
+        ms = []
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return ms
+
+    if args.profile_once:
+        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "fp64")
+        torch.cuda.synchronize()
+        return
+    precs = ["fp64"]
+    try:
+        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "mixed")
+        precs.append("mixed")
+    except A.AFMMError:
+        pass
+    head = precs[-1]
+    # per-stage device times (separate, untimed pass)
+    a.set_profiling(True)
+    stages = {}
+    for prec in precs:
+        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
+        stages[prec] = a.stage_times()
+    a.set_profiling(False)
+    launches0 = a.launch_count()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = ClockSampler(local)
+    clk.start()
+    ms = {prec: timed(prec, args.steps, args.warmup) for prec in precs}
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = (a.launch_count() - launches0) // max(1, len(precs) * (args.steps + args.warmup))
+    y64 = np.empty(N)
+    a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "fp64")
+    y64[:] = dy.cpu().numpy()
+    err_dense = a.evaluateError(nsample=16, seed=1234)
+    err_mixed = None
+    if "mixed" in precs:
+        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "mixed")
+        ym = dy.cpu().numpy()
+        err_mixed = float(np.linalg.norm(ym - y64) / np.linalg.norm(y64))
+    # end to end through the C ABI with pinned host buffers
+    hq = torch.from_numpy(q).pin_memory()
+    hy = torch.empty(N, dtype=torch.float64).pin_memory()
+    for _ in range(args.warmup):
+        a.matvec_host_ptr(hq.data_ptr(), hy.data_ptr(), 1, N, head)
+    e2e = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        a.matvec_host_ptr(hq.data_ptr(), hy.data_ptr(), 1, N, head)
+        e2e.append(time.perf_counter() - t1)
+    t_dev = {prec: float(np.mean(v)) for prec, v in ms.items()}
+    t_e2e = float(np.mean(e2e))
+    if dist:
+        for prec in precs:
+            t = torch.tensor([t_dev[prec]], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_dev[prec] = float(t.item())
+        t = torch.tensor([t_e2e], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    value = world * N / (t_dev[head] * 1e-3)
+    hbm, bf16, peak_kind = load_peaks()
+    # roofline of the dominant stage of the headline path
+    sd = stages[head]
+    dom = max((k for k in sd if k not in ("end", "h2d", "d2h")), key=lambda k: sd[k])
+    w = 8 if head == "fp64" else 4
+    if dom == "m2l":
+        byts = counts["m2l_entries"] * w + 2 * counts["sum_rank"] * w
+        achieved = byts / (sd[dom] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": "m2l_apply", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes": byts, "ms": sd[dom]}
+    else:
+        evals = counts["near_evals"]
+        roof = {"bound": "compute", "kernel": dom, "achieved": evals / (sd[dom] * 1e-3) / 1e9,
+                "unit": "G kernel evals/s", "peak": None, "frac": None, "traffic": None,
+                "algorithmic_evals": evals, "ms": sd[dom]}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_dev[head], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "N": N, "kernel": p["kernel"], "M": p["M"], "TOL_POW": p["tol"],
+                       "nrhs": 1, "precision": head, "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "fp64_points_per_s": world * N / (t_dev["fp64"] * 1e-3), "fp64_ms": t_dev["fp64"],
+            "mixed_ms": t_dev.get("mixed"), "rel_err_mixed_vs_fp64": err_mixed,
+            "rel_err_fp64_vs_dense_16_leaves": err_dense,
+            "setup_s": setup_s, "setup": st, "stages_ms": stages, "counts": counts,
+            "roofline": roof, "clocks": clocks, "gpu_launches": int(launches),
+            "e2e": {"value": world * N / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N,
+                    "d2h_bytes_per_step": 8 * N, "ms_per_step": t_e2e * 1e3}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_reference(args.workload, CPU_SAMPLE_N, 5, 1)
+        if cb:
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    a.close()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

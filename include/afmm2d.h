@@ -1,0 +1,149 @@
+/*
+ * afmm2d.h -- C ABI of the B200 (sm_100a) AFMM2D engine.
+ *
+ * Drop-in replacement for the matvec path of the reference AFMM2D library
+ * (vaishna77/AFMM2D): y = K q for an N x N kernel matrix K(i,j) over 2-D
+ * points, through a uniform KD-tree, ACA skeletonisation of every
+ * interaction list, and M2M / M2L / L2L / near-field sweeps.  All compute
+ * runs on one GPU; there is no CPU fallback.  Plain pointers and sizes only.
+ *
+ * Reference interface each entry point replaces:
+ *   afmm_create           AFMM::AFMM(int N, int MinParticlesInLeaf, int TOL_POW,
+ *                         Eigen::MatrixXd& loc)       include/AFMM2D.hpp:28,
+ *                         src/AFMM2D.cpp:3-39 (KD sort, tree, lists)
+ *   afmm_assemble         AFMM::assemble()            include/AFMM2D.hpp:29,
+ *                         src/AFMM2D.cpp:41-44 (getNodes + assemble_M2L)
+ *   afmm_matvec           AFMM::computeMatVecProduct(Eigen::VectorXd)
+ *                         include/AFMM2D.hpp:30, src/AFMM2D.cpp:46-65
+ *   afmm_eval_error       AFMM::evaluateError()       include/AFMM2D.hpp:31,
+ *                         src/AFMM2D.cpp:67-74, src/AFMM2DTree.cpp:1227-1236
+ *   afmm_get_permutation  AFMM::sorted_Properties     include/AFMM2D.hpp:25
+ *   afmm_get_sorted_locations  AFMM::sorted_Locations include/AFMM2D.hpp:24
+ *   afmm_get_nlevels      AFMM::nLevels               include/AFMM2D.hpp:19
+ *   afmm_get_leaves       FMM2DTree::NumberOfParticlesInLeaves / boxNumbers
+ *                         include/AFMM2DTree.hpp:34-35
+ *   afmm_get_lists        FMM2DBox::neighborNumbers / innerNumbers /
+ *                         outerNumbers               include/AFMM2DBox.hpp:17-19
+ *   afmm_get_ranks, afmm_get_skeletons, afmm_get_charge_points, afmm_get_l2p
+ *                         FMM2DBox::incoming_checkPoints / incoming_chargePoints
+ *                         / L2P                      include/AFMM2DBox.hpp:25-35
+ *   afmm_destroy          AFMM::~AFMM()               include/AFMM2D.hpp:32
+ * The user kernel userkernel::getMatrixEntry (include/kernel.hpp:58) is
+ * selected by `kernel_id` (see afmm_kernel_id); new kernels are added as
+ * device functors.
+ *
+ * Errors: every call returns an afmm_status; afmm_last_error() gives a
+ * message.  Where the reference aborts or has undefined behaviour the engine
+ * returns an error instead (nLevels < 2, non-finite coordinates), and a box
+ * whose ACA rank is 0 contributes no far field (the reference crashes there).
+ *
+ * Threading: a handle owns one CUDA stream; calls on one handle must not
+ * overlap; distinct handles are independent.
+ */
+#ifndef AFMM2D_B200_H
+#define AFMM2D_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  AFMM_OK = 0,
+  AFMM_BAD_ARG = 1,       /* invalid argument, e.g. N/M giving fewer than 2 levels */
+  AFMM_OOM = 2,           /* device allocation failed */
+  AFMM_CUDA_ERR = 3,      /* a CUDA call failed */
+  AFMM_TIMEOUT = 4,       /* a bounded device wait gave up */
+  AFMM_NUMERIC = 5,       /* non-finite values where finite ones are required */
+  AFMM_NOT_ASSEMBLED = 6, /* matvec before assemble */
+  AFMM_NO_DEVICE = 7      /* no CUDA device of compute capability 10.x */
+} afmm_status;
+
+/* Built-in kernels (userkernel::getMatrixEntry variants). */
+typedef enum {
+  AFMM_KERNEL_ONE_OVER_R_SCALED = 0, /* R<a ? R/a : a/R  (examples/testAFMM2D.cpp:9-20) */
+  AFMM_KERNEL_LOG = 1,               /* log r with diagonal convention (examples/tutorial.cpp:22-35) */
+  AFMM_KERNEL_ONE_OVER_R = 2,        /* 1/r, 0 at r=0 */
+  AFMM_KERNEL_GAUSSIAN = 3           /* exp(-r^2/p), p = kparams[0] (default 0.01) */
+} afmm_kernel_id;
+
+typedef enum {
+  AFMM_PREC_FP64 = 0,  /* plain FP64 apply (stored operators) */
+  AFMM_PREC_MIXED = 1  /* FP32 apply with FP64 where it matters */
+} afmm_precision;
+
+/* Layout of the `loc` array given to afmm_create. */
+typedef enum {
+  AFMM_LOC_COLMAJOR = 0,   /* N x 2 column-major, as Eigen::MatrixXd loc(N,2) */
+  AFMM_LOC_INTERLEAVED = 1 /* x0,y0,x1,y1,... */
+} afmm_loc_layout;
+
+typedef struct afmm_handle afmm_handle;
+
+/* Builds the KD-tree permutation, leaf layout and interaction lists on the GPU.
+ * nLevels = (unsigned)(log(N/M)/log(4)) with integer N/M (src/AFMM2D.cpp:7);
+ * nLevels < 2 is rejected with AFMM_BAD_ARG.  kparams may be NULL. */
+afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const double* loc, int loc_layout,
+                        int kernel_id, const double* kparams, int nkparams, afmm_handle** out);
+
+/* ACA skeletonisation of every box (levels L..2), L2P, and M2L blocks. */
+afmm_status afmm_assemble(afmm_handle* h);
+
+/* y = K q for nrhs right-hand sides.  q and y are N x nrhs, column j at
+ * offset j*ld (ld >= N), in the caller's ORIGINAL point order.
+ * mem_device = 0: host pointers (copied in and out); 1: device pointers.
+ * precision: afmm_precision. */
+afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int precision,
+                        int mem_device);
+
+/* Relative 2-norm error of the last matvec (first RHS) against a direct FP64
+ * evaluation over `nsample` leaf boxes chosen with `seed` (all leaves when
+ * nsample <= 0).  Reproducible, unlike src/AFMM2D.cpp:68. */
+afmm_status afmm_eval_error(afmm_handle* h, int nsample, uint64_t seed, double* rel_err);
+
+/* perm[i] = original index of the i-th sorted point (sorted_Properties). */
+afmm_status afmm_get_permutation(afmm_handle* h, int64_t* perm);
+/* Sorted locations, interleaved x,y (sorted_Locations). */
+afmm_status afmm_get_sorted_locations(afmm_handle* h, double* xy);
+afmm_status afmm_get_nlevels(afmm_handle* h, int* nlevels);
+/* Leaf counts in KD (DFS) order and the DFS -> quadtree box-number map, 4^L each. */
+afmm_status afmm_get_leaves(afmm_handle* h, int32_t* counts, int32_t* box_numbers);
+/* Lists of one level (4^level boxes): nbr[8], inner[16], outer[24] per box, -1 = none. */
+afmm_status afmm_get_lists(afmm_handle* h, int level, int32_t* nbr, int32_t* inner, int32_t* outer);
+/* Ranks of the 4^level boxes of a level (after assemble). */
+afmm_status afmm_get_ranks(afmm_handle* h, int level, int32_t* ranks);
+/* Skeletons (incoming check points) of all boxes of a level, concatenated in box
+ * order; *count receives the total.  ids may be NULL to query the count. */
+afmm_status afmm_get_skeletons(afmm_handle* h, int level, int32_t* ids, int64_t* count);
+/* Pivot columns (incoming charge points) likewise. */
+afmm_status afmm_get_charge_points(afmm_handle* h, int level, int32_t* ids, int64_t* count);
+/* L2P of box k at a level: rows x cols, written row-major (out may be NULL). */
+afmm_status afmm_get_l2p(afmm_handle* h, int level, int k, int32_t* rows, int32_t* cols, double* out);
+
+/* Per-stage device times (ms) of the last matvec and setup, when profiling is
+ * on.  names/values arrays of capacity `cap`; *n receives the count. */
+afmm_status afmm_set_profiling(afmm_handle* h, int on);
+afmm_status afmm_get_stage_times(afmm_handle* h, int cap, const char** names, double* ms, int* n);
+/* Setup wall times in seconds: [create, assemble]. */
+afmm_status afmm_get_setup_times(afmm_handle* h, double* t2);
+/* Counts of the assembled structure: [nlevels, N, sum ranks, stored L2P entries,
+ * stored M2L entries, near-field kernel evaluations, far-field (M2L) entries]. */
+afmm_status afmm_get_counts(afmm_handle* h, int64_t* c7);
+/* Number of kernels this library launched since the handle was created. */
+afmm_status afmm_get_launch_count(afmm_handle* h, int64_t* n);
+/* The CUDA stream (cudaStream_t) the handle launches on. */
+afmm_status afmm_get_stream(afmm_handle* h, void** stream);
+
+afmm_status afmm_destroy(afmm_handle* h);
+const char* afmm_status_string(afmm_status s);
+const char* afmm_last_error(afmm_handle* h);
+/* Library version string. */
+const char* afmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* AFMM2D_B200_H */
