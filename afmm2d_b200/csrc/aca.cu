@@ -468,111 +468,123 @@ struct L2pArgs {
   int32_t* cpiv_ids;
   double2* skel_xy;
   double* l2p;
-  int xs;  // rows of L2P solved at once (one per thread)
+  int xs;            // rows of L2P solved at once (one per thread)
+  int rmax;          // largest rank of the level
+  double* gscratch;  // gridDim.x * rmax^2 when the factor lives in global memory
 };
 
-template <class K>
+// GA = true keeps the r x r factor in a per-CTA global scratch slot (ranks
+// whose factor does not fit in shared memory); the CTA then loops over boxes.
+template <class K, bool GA>
 __global__ void __launch_bounds__(L2P_T) k_l2p(L2pArgs P) {
-  const int b = blockIdx.x;
-  const int r = P.rank[b];
-  if (r == 0) return;
-  const int nb0 = P.node_off[b];
-  const int n = P.node_off[b + 1] - nb0;
   extern __shared__ __align__(16) unsigned char smem[];
-  const int rr2 = (r * r + 1) & ~1;  // keep the double2 array 16-byte aligned
-  double* Am = (double*)smem;        // r x r, row-major
-  double2* cxy = (double2*)(Am + rr2);  // r pivot-column points
-  double* X = (double*)(cxy + r);    // r x xs scratch, one column per solving thread
-  int* perm = (int*)(X + (size_t)r * P.xs);  // r
   __shared__ int s_piv;
-  const int so = P.skel_off[b];
-  for (int l = threadIdx.x; l < r; l += L2P_T) {
-    int rid = P.node_ids[nb0 + P.rowpiv[(size_t)b * P.rcap + l]];
-    int cid = P.colpiv[(size_t)b * P.rcap + l];
-    P.skel_ids[so + l] = rid;
-    P.cpiv_ids[so + l] = cid;
-    P.skel_xy[so + l] = P.pts[rid];
-    cxy[l] = P.pts[cid];
-    perm[l] = l;
-  }
-  __syncthreads();
-  // A(i,j) = D(j,i) = K(R_j, C_i)
-  for (int e = threadIdx.x; e < r * r; e += L2P_T) {
-    int i = e / r, j = e % r;
-    double2 rp = P.skel_xy[so + j];
-    Am[e] = K::eval_exact(r2_exact(rp.x, rp.y, cxy[i].x, cxy[i].y), P.kp);
-  }
-  __syncthreads();
-  for (int kk = 0; kk < r; ++kk) {
-    if (threadIdx.x < 32) {
-      double best = -1.0;
-      int bi = kk;
-      for (int i = kk + threadIdx.x; i < r; i += 32) {
-        double a = fabs(Am[(size_t)i * r + kk]);
-        if (a > best) { best = a; bi = i; }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        double ob = __shfl_down_sync(0xffffffffu, best, o);
-        int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-      }
-      if (threadIdx.x == 0) s_piv = bi;
+  for (int b = blockIdx.x; b < P.nbox; b += gridDim.x) {
+    const int r = P.rank[b];
+    if (r == 0) continue;
+    const int nb0 = P.node_off[b];
+    const int n = P.node_off[b + 1] - nb0;
+    const int rr2 = GA ? 0 : ((r * r + 1) & ~1);  // keep the double2 array 16-byte aligned
+    double* Am = GA ? P.gscratch + (size_t)blockIdx.x * P.rmax * P.rmax : (double*)smem;  // r x r, row-major
+    double2* cxy = (double2*)((double*)smem + rr2);  // r pivot-column points
+    double* X = (double*)(cxy + r);                  // r x xs scratch, one column per solving thread
+    int* perm = (int*)(X + (size_t)r * P.xs);        // r
+    const int so = P.skel_off[b];
+    __syncthreads();
+    for (int l = threadIdx.x; l < r; l += L2P_T) {
+      int rid = P.node_ids[nb0 + P.rowpiv[(size_t)b * P.rcap + l]];
+      int cid = P.colpiv[(size_t)b * P.rcap + l];
+      P.skel_ids[so + l] = rid;
+      P.cpiv_ids[so + l] = cid;
+      P.skel_xy[so + l] = P.pts[rid];
+      cxy[l] = P.pts[cid];
+      perm[l] = l;
     }
     __syncthreads();
-    const int pv = s_piv;
-    if (pv != kk) {
-      for (int j = threadIdx.x; j < r; j += L2P_T) {
-        double t = Am[(size_t)kk * r + j];
-        Am[(size_t)kk * r + j] = Am[(size_t)pv * r + j];
-        Am[(size_t)pv * r + j] = t;
-      }
-      if (threadIdx.x == 0) {
-        int t = perm[kk];
-        perm[kk] = perm[pv];
-        perm[pv] = t;
-      }
+    // A(i,j) = D(j,i) = K(R_j, C_i)
+    for (int e = threadIdx.x; e < r * r; e += L2P_T) {
+      int i = e / r, j = e % r;
+      double2 rp = P.pts[P.node_ids[nb0 + P.rowpiv[(size_t)b * P.rcap + j]]];
+      Am[e] = K::eval_exact(r2_exact(rp.x, rp.y, cxy[i].x, cxy[i].y), P.kp);
     }
     __syncthreads();
-    const double d = Am[(size_t)kk * r + kk];
-    if (d != 0.0) {
-      for (int i = kk + 1 + threadIdx.x; i < r; i += L2P_T) Am[(size_t)i * r + kk] /= d;
+    for (int kk = 0; kk < r; ++kk) {
+      if (threadIdx.x < 32) {
+        double best = -1.0;
+        int bi = kk;
+        for (int i = kk + threadIdx.x; i < r; i += 32) {
+          double a = fabs(Am[(size_t)i * r + kk]);
+          if (a > best) { best = a; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          double ob = __shfl_down_sync(0xffffffffu, best, o);
+          int oi = __shfl_down_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if (threadIdx.x == 0) s_piv = bi;
+      }
       __syncthreads();
-      const int m = r - kk - 1;
-      for (int e = threadIdx.x; e < m * m; e += L2P_T) {
-        int i = kk + 1 + e / m, j = kk + 1 + e % m;
-        Am[(size_t)i * r + j] -= Am[(size_t)i * r + kk] * Am[(size_t)kk * r + j];
+      const int pv = s_piv;
+      if (pv != kk) {
+        for (int j = threadIdx.x; j < r; j += L2P_T) {
+          double t = Am[(size_t)kk * r + j];
+          Am[(size_t)kk * r + j] = Am[(size_t)pv * r + j];
+          Am[(size_t)pv * r + j] = t;
+        }
+        if (threadIdx.x == 0) {
+          int t = perm[kk];
+          perm[kk] = perm[pv];
+          perm[pv] = t;
+        }
+      }
+      __syncthreads();
+      const double d = Am[(size_t)kk * r + kk];
+      if (d != 0.0) {
+        for (int i = kk + 1 + threadIdx.x; i < r; i += L2P_T) Am[(size_t)i * r + kk] /= d;
+        __syncthreads();
+        const int m = r - kk - 1;
+        for (int e = threadIdx.x; e < m * m; e += L2P_T) {
+          int i = kk + 1 + e / m, j = kk + 1 + e % m;
+          Am[(size_t)i * r + j] -= Am[(size_t)i * r + kk] * Am[(size_t)kk * r + j];
+        }
+      }
+      __syncthreads();
+    }
+    double* out = P.l2p + P.l2p_off[b];  // n x r column-major: (i, l) at l*n + i
+    const int xs = P.xs;
+    for (int i0 = 0; i0 < n; i0 += xs) {
+      const int i = i0 + threadIdx.x;
+      if (threadIdx.x < xs && i < n) {
+        double* x = X + threadIdx.x;  // x[l * xs]
+        double2 rp = P.pts[P.node_ids[nb0 + i]];
+        for (int l = 0; l < r; ++l) {
+          double2 c = cxy[perm[l]];
+          double s = K::eval_exact(r2_exact(rp.x, rp.y, c.x, c.y), P.kp);
+          for (int m = 0; m < l; ++m) s -= Am[(size_t)l * r + m] * x[m * xs];
+          x[l * xs] = s;
+        }
+        for (int l = r - 1; l >= 0; --l) {
+          double s = x[l * xs];
+          for (int m = l + 1; m < r; ++m) s -= Am[(size_t)l * r + m] * x[m * xs];
+          x[l * xs] = s / Am[(size_t)l * r + l];
+        }
+        for (int l = 0; l < r; ++l) out[(size_t)l * n + i] = x[l * xs];
       }
     }
     __syncthreads();
-  }
-  double* out = P.l2p + P.l2p_off[b];  // n x r column-major: (i, l) at l*n + i
-  const int xs = P.xs;
-  for (int i0 = 0; i0 < n; i0 += xs) {
-    const int i = i0 + threadIdx.x;
-    if (threadIdx.x < xs && i < n) {
-      double* x = X + threadIdx.x;  // x[l * xs]
-      double2 rp = P.pts[P.node_ids[nb0 + i]];
-      for (int l = 0; l < r; ++l) {
-        double2 c = cxy[perm[l]];
-        double s = K::eval_exact(r2_exact(rp.x, rp.y, c.x, c.y), P.kp);
-        for (int m = 0; m < l; ++m) s -= Am[(size_t)l * r + m] * x[m * xs];
-        x[l * xs] = s;
-      }
-      for (int l = r - 1; l >= 0; --l) {
-        double s = x[l * xs];
-        for (int m = l + 1; m < r; ++m) s -= Am[(size_t)l * r + m] * x[m * xs];
-        x[l * xs] = s / Am[(size_t)l * r + l];
-      }
-      for (int l = 0; l < r; ++l) out[(size_t)l * n + i] = x[l * xs];
-    }
   }
 }
 
 template <class K>
 struct L2pRun {
-  static void run(const L2pArgs& a, size_t smem, cudaStream_t s) {
-    AFMM_CUDA(cudaFuncSetAttribute(k_l2p<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_l2p<K><<<a.nbox, L2P_T, smem, s>>>(a);
+  static void run(const L2pArgs& a, size_t smem, bool global_factor, int grid, cudaStream_t s) {
+    if (global_factor) {
+      AFMM_CUDA(cudaFuncSetAttribute(k_l2p<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_l2p<K, true><<<grid, L2P_T, smem, s>>>(a);
+    } else {
+      AFMM_CUDA(cudaFuncSetAttribute(k_l2p<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_l2p<K, false><<<grid, L2P_T, smem, s>>>(a);
+    }
     AFMM_LAUNCH_CHECK();
   }
 };
@@ -676,13 +688,23 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     p.cpiv_ids = out.cpiv_ids;
     p.skel_xy = out.skel_xy;
     p.l2p = out.l2p;
-    const size_t budget2 = 220 * 1024;
-    size_t base = sizeof(double) * (size_t)((rmax * rmax + 1) & ~1) + sizeof(double2) * rmax + sizeof(int) * rmax + 64;
-    if (base + sizeof(double) * rmax > budget2)
-      throw Error{AFMM_BAD_ARG, "box rank " + std::to_string(rmax) + " too large for the L2P solve"};
+    const size_t budget2 = 200 * 1024;
+    // factor in shared memory when it leaves room for >= 32 solving threads
+    size_t fa = sizeof(double) * (size_t)((rmax * rmax + 1) & ~1);
+    size_t rest = sizeof(double2) * rmax + sizeof(int) * rmax + 64;
+    bool global_factor = fa + rest + sizeof(double) * (size_t)rmax * 32 > budget2;
+    size_t base = (global_factor ? 0 : fa) + rest;
     p.xs = (int)std::min<size_t>(L2P_T, (budget2 - base) / (sizeof(double) * rmax));
+    if (p.xs < 1) throw Error{AFMM_BAD_ARG, "box rank " + std::to_string(rmax) + " too large for the L2P solve"};
     size_t sm = base + sizeof(double) * (size_t)rmax * p.xs;
-    dispatch_kernel<L2pRun>(in.kp.id, p, sm, s);
+    p.rmax = rmax;
+    int grid = (int)in.nbox;
+    p.gscratch = nullptr;
+    if (global_factor) {
+      grid = (int)std::min<long>(in.nbox, 148 * 8);
+      p.gscratch = scratch.alloc<double>((size_t)grid * rmax * rmax);
+    }
+    dispatch_kernel<L2pRun>(in.kp.id, p, sm, global_factor, grid, s);
     *launches += 1;
   }
   AFMM_CUDA(cudaStreamSynchronize(s));
