@@ -37,6 +37,7 @@ namespace {
 
 constexpr int ACA_T = 256;
 constexpr int ACA_WARPS = ACA_T / 32;
+enum { AR_ROWS = 0, AR_COLS, AR_V, AR_U, AR_XDOT, AR_SMALL, AR_OK, AR_XARG, AR_N };
 
 struct AcaArgs {
   int nbox;
@@ -53,6 +54,12 @@ struct AcaArgs {
   int ucap;       // ranks of U held in shared memory
   double* vspill; // [cluster][C][rcap - vcap][chunk]
   double* uspill; // [cluster][C][rcap - ucap][n1max]
+  // Placement of the per-CTA arrays: byte offset into shared memory when the
+  // flag is set, else into this CTA's slot of `gscr` (gslot bytes per CTA).
+  unsigned char* gscr;
+  size_t gslot;
+  size_t off[8];
+  int in_smem[8];
   int32_t* rank_out;
   int32_t* rowpiv;  // nbox * rcap, local row index
   int32_t* colpiv;  // nbox * rcap, sorted point id
@@ -175,17 +182,25 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 
   extern __shared__ __align__(16) unsigned char smem[];
-  double2* rows_xy = (double2*)smem;                    // n1max
-  double2* cols_xy = rows_xy + A.n1max;                 // chunk
-  double* V = (double*)(cols_xy + A.chunk);             // vcap * chunk
-  double* U = V + (size_t)A.vcap * A.chunk;             // ucap * n1max
-  double* xbuf = U + (size_t)A.ucap * A.n1max;          // 2 * (rcap + 8)
-  double* vcol = xbuf + 2 * (A.rcap + 8);               // rcap
-  double* udot = vcol + A.rcap;                         // rcap
-  double* vdot = udot + A.rcap;                         // rcap
-  double* uri = vdot + A.rcap;                          // rcap: U_l(ri)
-  unsigned char* row_ok = (unsigned char*)(uri + A.rcap);   // n1max
-  unsigned char* col_ok = row_ok + A.n1max;                 // chunk
+  unsigned char* gbase = A.gscr ? A.gscr + ((size_t)cid * C + crank) * A.gslot : nullptr;
+  auto place = [&](int a) -> unsigned char* { return A.in_smem[a] ? smem + A.off[a] : gbase + A.off[a]; };
+  double2* rows_xy = (double2*)place(AR_ROWS);           // n1max
+  double2* cols_xy = (double2*)place(AR_COLS);           // chunk
+  double* V = (double*)place(AR_V);                      // vcap * chunk (shared memory)
+  double* U = (double*)place(AR_U);                      // ucap * n1max (shared memory)
+  double* xdot = (double*)place(AR_XDOT);                // 2 * (rcap + 8): V-dot exchange
+  double* vcol = (double*)place(AR_SMALL);               // rcap
+  double* udot = vcol + A.rcap;                          // rcap
+  double* vdot = udot + A.rcap;                          // rcap
+  double* uri = vdot + A.rcap;                           // rcap: U_l(ri)
+  unsigned char* row_ok = place(AR_OK);                  // n1max
+  unsigned char* col_ok = row_ok + A.n1max;              // chunk
+  double* xarg = (double*)place(AR_XARG);                // 2 * 8: argmax exchange (shared memory)
+  // the V-dot exchange of CTA c of this cluster (shared or global memory)
+  auto xdot_of = [&](int c) -> double* {
+    if (A.in_smem[AR_XDOT]) return cluster.map_shared_rank(xdot, c);
+    return (double*)(A.gscr + ((size_t)cid * C + c) * A.gslot + A.off[AR_XDOT]);
+  };
   __shared__ int s_pref[41];
   __shared__ int s_box[40];
   __shared__ ArgMax s_red[ACA_WARPS];
@@ -247,7 +262,7 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
           am_add(m, v, lo + j);
         }
         m = block_argmax(m, s_red);
-        piv = cluster_argmax(cluster, m, xbuf + xpar * (A.rcap + 8), &s_piv);
+        piv = cluster_argmax(cluster, m, xarg + xpar * 8, &s_piv);
         xpar ^= 1;
         if (piv.i < 0 || piv.i >= n2) break;  // cannot happen: every column is allowed here
         if (piv.a > A.tol) {
@@ -306,7 +321,7 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
             if (col_ok[j]) am_add(mm, v, lo + j);
           }
           mm = block_argmax(mm, s_red);
-          const ArgMax pv = cluster_argmax(cluster, mm, xbuf + xpar * (A.rcap + 8), &s_piv);
+          const ArgMax pv = cluster_argmax(cluster, mm, xarg + xpar * 8, &s_piv);
           xpar ^= 1;
           // Every CTA sees the same pv; an empty allowed set cannot occur
           // while rank < min(n1, n2), but stop rather than index out of range.
@@ -363,8 +378,8 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
             if (lane == 0) udot[l] = t;
           }
           __syncthreads();
-          double* xb2 = xbuf + xpar * (A.rcap + 8);
-          for (int l = tid; l <= k; l += ACA_T) xb2[l] = vdot[l];
+          const size_t xo = (size_t)xpar * (A.rcap + 8);
+          for (int l = tid; l <= k; l += ACA_T) xdot[xo + l] = vdot[l];
           if (tid == 0) {
             if (ownk == crank) col_ok[jok] = 0;
             row_ok[ri] = 0;
@@ -372,7 +387,7 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
           cluster.sync();
           for (int l = tid; l <= k; l += ACA_T) {
             double s = 0.0;
-            for (int c = 0; c < C; ++c) s += cluster.map_shared_rank(xb2, c)[l];
+            for (int c = 0; c < C; ++c) s += xdot_of(c)[xo + l];
             vdot[l] = s;
           }
           xpar ^= 1;
@@ -596,22 +611,51 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   const int n2max = std::max(in.n2max, 1);
   const int rcap = std::max(1, std::min(n1max, n2max));
   // Cluster size: smallest power of two (<= 16) whose column slice keeps at
-  // least min(rcap, 48) ranks of V in shared memory.
+  // least min(rcap, 48) ranks of V in shared memory.  The small per-CTA
+  // arrays go to shared memory first (argmax exchange, column and row
+  // coordinates, flags, per-rank vectors, V-dot exchange) while they fit in
+  // a quarter of the budget; whatever does not fit lives in a per-CTA slot
+  // of global memory.  U then takes up to a quarter and V the rest.
   const size_t budget = 200 * 1024;
-  int C = 1;
-  int chunk = 0, vcap = 0, ucap = 0;
-  size_t smem = 0;
+  int C = 1, chunk = 0, vcap = 0, ucap = 0;
+  size_t smem = 0, gslot = 0;
+  size_t off[AR_N] = {0};
+  int in_smem[AR_N] = {0};
   for (C = 1;; C *= 2) {
     chunk = (n2max + C - 1) / C;
-    size_t fixed = sizeof(double2) * ((size_t)n1max + chunk) + sizeof(double) * (2 * (size_t)(rcap + 8) + 4 * (size_t)rcap) +
-                   (size_t)n1max + chunk + 64;
-    ucap = std::min(rcap, (int)std::max<size_t>(1, (budget / 4) / (sizeof(double) * n1max)));
-    size_t left = budget > fixed + sizeof(double) * (size_t)ucap * n1max ? budget - fixed - sizeof(double) * (size_t)ucap * n1max : 0;
-    vcap = std::min(rcap, (int)(left / (sizeof(double) * chunk)));
+    size_t sz[AR_N];
+    sz[AR_ROWS] = sizeof(double2) * (size_t)n1max;
+    sz[AR_COLS] = sizeof(double2) * (size_t)chunk;
+    sz[AR_XDOT] = sizeof(double) * 2 * (size_t)(rcap + 8);
+    sz[AR_SMALL] = sizeof(double) * 4 * (size_t)rcap;
+    sz[AR_OK] = (size_t)n1max + chunk;
+    sz[AR_XARG] = sizeof(double) * 16;
+    auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    size_t used = 0, gused = 0;
+    const int order[] = {AR_XARG, AR_COLS, AR_ROWS, AR_SMALL, AR_XDOT, AR_OK};
+    for (int a : order) {
+      if (a == AR_XARG || used + al(sz[a]) <= budget / 4) {
+        in_smem[a] = 1;
+        off[a] = used;
+        used += al(sz[a]);
+      } else {
+        in_smem[a] = 0;
+        off[a] = gused;
+        gused += al(sz[a]);
+      }
+    }
+    ucap = std::min<long>(rcap, (long)((budget / 4) / (sizeof(double) * n1max)));
+    in_smem[AR_U] = 1;
+    off[AR_U] = used;
+    used += al(sizeof(double) * (size_t)ucap * n1max);
+    size_t left = budget > used ? budget - used : 0;
+    vcap = std::min<long>(rcap, (long)(left / (sizeof(double) * chunk)));
     if (vcap >= std::min(rcap, 48) || C == 16) {
-      vcap = std::max(vcap, 0);
-      smem = fixed + sizeof(double) * ((size_t)ucap * n1max + (size_t)vcap * chunk);
-      smem = (smem + 15) & ~(size_t)15;
+      in_smem[AR_V] = 1;
+      off[AR_V] = used;
+      used += al(sizeof(double) * (size_t)vcap * chunk);
+      smem = used;
+      gslot = gused;
       break;
     }
   }
@@ -633,7 +677,13 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   a.chunk = chunk;
   a.vcap = vcap;
   a.ucap = ucap;
+  for (int t = 0; t < AR_N; ++t) {
+    a.off[t] = off[t];
+    a.in_smem[t] = in_smem[t];
+  }
+  a.gslot = gslot;
   DevArena scratch;
+  a.gscr = gslot > 0 ? scratch.alloc<unsigned char>((size_t)ncl * C * gslot) : nullptr;
   a.vspill = vsp > 0 ? scratch.alloc<double>((size_t)ncl * C * vsp * chunk) : nullptr;
   a.uspill = usp > 0 ? scratch.alloc<double>((size_t)ncl * C * usp * n1max) : nullptr;
   out.rcap = rcap;

@@ -20,8 +20,10 @@ struct Error {
 #define AFMM_CUDA(call)                                                                      \
   do {                                                                                       \
     cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess)                                                                   \
+    if (e_ != cudaSuccess) {                                                                 \
+      cudaGetLastError(); /* clear a non-sticky error so later checks do not report it */    \
       throw ::afmm::Error{AFMM_CUDA_ERR, std::string(#call) + ": " + cudaGetErrorString(e_)}; \
+    }                                                                                        \
   } while (0)
 
 #define AFMM_LAUNCH_CHECK() AFMM_CUDA(cudaGetLastError())
@@ -166,7 +168,9 @@ struct LevelDev {
   double2* skel_xy = nullptr;   // skeleton coordinates
   int64_t* l2p_off = nullptr;   // nbox+1 prefix over n_b*r_b
   double* l2p = nullptr;        // per box n_b x r_b, column-major (row index fastest)
+  double* l2p_rm = nullptr;     // the same, row-major (rank index fastest)
   float* l2p32 = nullptr;
+  float* l2p32_rm = nullptr;
   double2* anchor = nullptr;    // per box reference point for FP32 relative coordinates
   float2* skel_rel = nullptr;   // skeleton coordinates minus the box anchor (FP32)
   int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c

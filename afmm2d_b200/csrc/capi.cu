@@ -158,7 +158,9 @@ void build_plan(afmm_handle* h) {
     v.leaf_start = (j == h->L) ? h->d_leaf_start : nullptr;
     v.l2p_off = d.l2p_off;
     v.l2p = d.l2p;
+    v.l2p_rm = d.l2p_rm;
     v.l2p32 = d.l2p32;
+    v.l2p32_rm = d.l2p32_rm;
     v.m2l_off = d.m2l_off;
     v.m2l = d.m2l;
     v.skel_xy = d.skel_xy;
@@ -344,10 +346,15 @@ void do_assemble(afmm_handle* h) {
     v.qhat = h->arena.alloc<double>(v.total_rank);
     v.yhat = h->arena.alloc<double>(v.total_rank);
   }
+  for (int j = 2; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
+    v.l2p_rm = h->arena.alloc<double>(v.h_l2p_off[v.nbox]);
+  }
   build_plan(h);
   for (int j = 2; j <= L; ++j) {
     m2l_assemble(h->plan.lv[j], h->kp, s);
-    ++h->launches;
+    l2p_transpose(h->plan.lv[j], h->lv[j].l2p, h->lv[j].l2p_rm, s);
+    h->launches += 2;
   }
   mixed_setup(h->plan, h->lv, h->mixed, h->arena, s, &h->launches);
   build_plan(h);

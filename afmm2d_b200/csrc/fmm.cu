@@ -120,7 +120,8 @@ __global__ void k_scatter(const double* __restrict__ ys, const int64_t* __restri
   if (i < n) y[perm[i]] = ys[i];
 }
 
-// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b, one warp per box.
+// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b, one warp per box,
+// lanes over the outputs c, reading the row-major copy of L2P (coalesced).
 // src_b = leaf charges, or the concatenated outgoing charges of children 0..3.
 __global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
   const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -130,14 +131,41 @@ __global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf)
   if (r == 0) return;
   const int n = v.node_off[b + 1] - v.node_off[b];
   const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
-  const double* P = v.l2p + v.l2p_off[b];
+  const double* P = v.l2p_rm + v.l2p_off[b];  // n x r, row-major
   double* out = v.qhat + v.skel_off[b];
-  for (int c = 0; c < r; ++c) {
-    double s = 0.0;
-    for (int i = lane; i < n; i += 32) s += P[(long)c * n + i] * src[i];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) out[c] = s;
+  for (int c0 = 0; c0 < r; c0 += 32) {
+    const int c = c0 + lane;
+    if (c < r) {
+      double s = 0.0;
+#pragma unroll 8
+      for (int i = 0; i < n; ++i) s += P[(long)i * r + c] * src[i];
+      out[c] = s;
+    }
   }
+}
+
+// Row-major copy of L2P (per box, r fastest) for the M2M sweep.
+template <class T>
+__global__ void k_l2p_transpose(LevelView v, const T* __restrict__ cm, T* rm) {
+  const long b = blockIdx.x;
+  const int r = v.rank[b];
+  if (r == 0) return;
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const long o = v.l2p_off[b];
+  for (int e = threadIdx.x; e < n * r; e += blockDim.x) {
+    int i = e / r, c = e - i * r;
+    rm[o + e] = cm[o + (long)c * n + i];
+  }
+}
+
+void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s) {
+  k_l2p_transpose<double><<<(int)v.nbox, 256, 0, s>>>(v, cm, rm);
+  AFMM_LAUNCH_CHECK();
+}
+
+void l2p_transpose32(const LevelView& v, const float* cm, float* rm, cudaStream_t s) {
+  k_l2p_transpose<float><<<(int)v.nbox, 256, 0, s>>>(v, cm, rm);
+  AFMM_LAUNCH_CHECK();
 }
 
 // M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch: one warp
@@ -163,8 +191,10 @@ __global__ void k_m2l_apply(LevelSet ls) {
       if (c < 0) continue;
       const int rc = v.rank[c];
       const double* qc = v.qhat + v.skel_off[c];
-      if (i < r)
+      if (i < r) {
+#pragma unroll 8
         for (int cc = 0; cc < rc; ++cc) acc += M[(long)cc * r + i] * qc[cc];
+      }
       M += (long)r * rc;
     }
     if (i < r) v.yhat[v.skel_off[b] + i] = acc;
@@ -183,6 +213,7 @@ __global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __re
   const double* yb = v.yhat + v.skel_off[b];
   for (int i = lane; i < n; i += 32) {
     double t = 0.0;
+#pragma unroll 8
     for (int c = 0; c < r; ++c) t += P[(long)c * n + i] * yb[c];
     if (leaf) ys[v.leaf_start[b] + i] = t;
     else child_yhat[v.node_off[b] + i] += t;

@@ -20,8 +20,10 @@ struct LevelView {
   const int32_t* node_off = nullptr;
   const int32_t* leaf_start = nullptr;  // leaf level only (quadtree order)
   const int64_t* l2p_off = nullptr;
-  const double* l2p = nullptr;
+  const double* l2p = nullptr;     // column-major (row index fastest)
+  const double* l2p_rm = nullptr;  // row-major copy (rank index fastest)
   const float* l2p32 = nullptr;
+  const float* l2p32_rm = nullptr;
   const int64_t* m2l_off = nullptr;
   double* m2l = nullptr;
   const double2* skel_xy = nullptr;
@@ -99,6 +101,8 @@ struct MatvecPlan {
 
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
+void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
+void l2p_transpose32(const LevelView& v, const float* cm, float* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
 
 }  // namespace afmm
