@@ -173,6 +173,7 @@ struct LevelDev {
   float* l2p32_rm = nullptr;
   double2* anchor = nullptr;    // per box reference point for FP32 relative coordinates
   float2* skel_rel = nullptr;   // skeleton coordinates minus the box anchor (FP32)
+  float* span = nullptr;        // per box max |skel_rel| component
   int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c
   double* m2l = nullptr;        // per box, per valid slot, block r_b x r_c column-major
   double* qhat = nullptr;       // outgoing charges, skel_off layout

@@ -166,6 +166,7 @@ void build_plan(afmm_handle* h) {
     v.skel_xy = d.skel_xy;
     v.skel_rel = d.skel_rel;
     v.anchor = d.anchor;
+    v.span = d.span;
     v.qhat = d.qhat;
     v.yhat = d.yhat;
     v.qhat32 = d.qhat32;
@@ -453,6 +454,7 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
     if (h->profiling) h->timer.reset();
     StageTimer* tm = h->profiling ? &h->timer : nullptr;
     if (precision == AFMM_PREC_MIXED) {
+      mixed_reserve(h->mixed, h->N, 1, h->arena);
       if (!mem_device) {
         if (h->mixed.host_cap < (size_t)nrhs) mixed_reserve_io(h->mixed, h->N, nrhs, h->arena);
         if (tm) tm->mark(s, "h2d");

@@ -29,6 +29,7 @@ struct LevelView {
   const double2* skel_xy = nullptr;
   const float2* skel_rel = nullptr;   // skeleton minus box anchor (FP32)
   const double2* anchor = nullptr;    // box anchors (FP64)
+  const float* span = nullptr;        // per box max |skel_rel| component
   double* qhat = nullptr;
   double* yhat = nullptr;
   float* qhat32 = nullptr;
@@ -50,6 +51,7 @@ struct NearView {
   const int32_t* nbr = nullptr;        // nleaf * 8
   const double2* anchor = nullptr;     // leaf anchors (FP64)
   const float2* rel = nullptr;         // point minus its leaf anchor (FP32), sorted order
+  const float* span = nullptr;         // per leaf max |rel| component
 };
 
 // CUDA-event marks for per-stage device timing.

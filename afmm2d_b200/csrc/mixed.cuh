@@ -14,12 +14,19 @@ struct MixedState {
   size_t host_cap = 0;      // RHS capacity of the staging buffers below
   double* d_qin = nullptr;  // N x host_cap staging for host inputs
   double* d_yout = nullptr; // N x host_cap staging for host outputs
+  int rhs_cap = 0;          // RHS capacity of qs32 / ys
+  float* qs32 = nullptr;    // sorted charges (FP32)
+  double* ys = nullptr;     // sorted potentials (FP64)
+  double2* leaf_anchor = nullptr;
+  float* leaf_span = nullptr;
+  float2* rel = nullptr;    // sorted point minus its leaf anchor (FP32)
 };
 
 // Builds the FP32 operators and anchors after assembly.
 void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevArena& arena, cudaStream_t s,
                  int64_t* launches);
 void mixed_reserve_io(MixedState& ms, int N, int nrhs, DevArena& arena);
+void mixed_reserve(MixedState& ms, int N, int nrhs, DevArena& arena);
 // y = K q for nrhs columns (q column c at q + c*ldq), original order, device pointers.
 void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t ldq, double* y, int64_t ldy, int nrhs,
                   cudaStream_t s, StageTimer* tm, int64_t* launches);

@@ -140,3 +140,43 @@ def test_full_size_properties_uniform1m():
     rows = np.random.default_rng(5).choice(N, 512, replace=False)
     yd = dense_rows(pts, q, p["kernel"], a.nLevels, rows)
     assert np.linalg.norm(y1[rows] - yd) / np.linalg.norm(yd) < 1e-6
+
+
+MIXED_TOL = 1e-6  # relative 2-norm of the mixed-precision result vs the FP64 path
+
+
+@pytest.mark.parametrize("name,N,kernel,tol,M", [("mixture4m", 65536, "one_over_r", 6, 64),
+                                                 ("uniform1m", 65536, "log", 10, 64),
+                                                 ("gauss1m", 65536, "gaussian", 8, 64),
+                                                 ("uniform4k", 4096, "one_over_r_scaled", 8, 32)])
+def test_mixed_vs_fp64(name, N, kernel, tol, M):
+    pts, q, _ = workloads.make(name, N=N, nrhs=1)
+    a = A.AFMM(N, M, tol, pts, kernel=kernel)
+    a.assemble()
+    y64 = a.computeMatVecProduct(q)
+    ym = a.computeMatVecProduct(q, precision="mixed")
+    rel = np.linalg.norm(ym - y64) / np.linalg.norm(y64)
+    assert rel <= MIXED_TOL, rel
+
+
+def test_mixed_spiral_close_pairs():
+    """Spiral points with 1e-4 jitter: close pairs take the FP64 fallback and
+    the log kernel's R2 < 1e-10 convention is decided in FP64."""
+    pts, q, p = workloads.make("spiral16m", N=131072)
+    a = A.AFMM(len(pts), 64, 12, pts, kernel="log")
+    a.assemble()
+    y64 = a.computeMatVecProduct(q)
+    ym = a.computeMatVecProduct(q, precision="mixed")
+    assert np.linalg.norm(ym - y64) / np.linalg.norm(y64) <= MIXED_TOL
+
+
+def test_mixed_host_and_device_agree():
+    torch = pytest.importorskip("torch")
+    pts, q, _ = workloads.make("mixture4m", N=65536)
+    a = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
+    a.assemble()
+    yh = a.computeMatVecProduct(q, precision="mixed")
+    dq = torch.tensor(q, device="cuda")
+    dy = torch.zeros_like(dq)
+    a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, 65536, precision="mixed")
+    np.testing.assert_array_equal(dy.cpu().numpy(), yh)
