@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 
-__all__ = ["AFMM", "AFMMError", "KERNELS", "PRECISIONS", "lib", "nlevels"]
+__all__ = ["AFMM", "AFMMError", "KERNELS", "PRECISIONS", "kernel_eval", "lib", "nlevels"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafmm2d.so")
@@ -49,6 +49,7 @@ _SIGS = {
     "afmm_get_counts": [_vp, _vp],
     "afmm_get_launch_count": [_vp, _vp],
     "afmm_get_stream": [_vp, _vp],
+    "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
     "afmm_destroy": [_vp],
 }
 _lib = None
@@ -87,6 +88,18 @@ def _check(st, h=None):
 
 def _ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
+
+
+def kernel_eval(kernel, a, xy1, xy2, mode="exact", param=0.01):
+    """K(xy1[t], xy2[t]) for point pairs on the GPU.  mode: "exact" (setup
+    arithmetic), "fp64" (matvec form) or "fp32"."""
+    kid = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
+    xy1 = np.ascontiguousarray(xy1, dtype=np.float64).reshape(-1, 2)
+    xy2 = np.ascontiguousarray(xy2, dtype=np.float64).reshape(-1, 2)
+    out = np.zeros(len(xy1))
+    m = {"exact": 0, "fp64": 1, "fp32": 2}[mode]
+    _check(lib().afmm_kernel_eval(kid, float(a), float(param), len(xy1), _ptr(xy1), _ptr(xy2), _ptr(out), m))
+    return out
 
 
 def nlevels(N, M):

@@ -8,6 +8,7 @@
 #include <vector>
 
 #include "../../include/afmm2d.h"
+#include "exact_math.cuh"
 
 namespace afmm {
 
@@ -34,10 +35,10 @@ struct Error {
 // smallest box size `a` (src/AFMM2DTree.cpp:19).  Here a kernel is a functor
 // of the two points' coordinates.  `eval_exact` reproduces the reference's
 // double arithmetic operation by operation (no FMA contraction, IEEE sqrt and
-// division) and is used wherever results steer pivoting (ACA, L2P, M2L
-// blocks).  `eval` is the fast FP64 form for the matvec, `eval32` the FP32
-// form for the mixed-precision matvec: it receives dx, dy already reduced to
-// small numbers (coordinates relative to box anchors).
+// division, correctly rounded log/exp from exact_math.cuh) and is used
+// wherever results steer pivoting (ACA, L2P, M2L blocks).  `eval` is the fast FP64 form for the matvec, `eval32` the FP32
+// form for the mixed-precision matvec (R2 formed from coordinates relative to
+// box anchors; the third argument is the Gaussian parameter).
 struct KernelParams {
   int id;
   double a;      // 2^-L
@@ -62,7 +63,7 @@ struct KOneOverRScaled {
   }
   __device__ __forceinline__ static float eval32(float R2, float a, float) {
     float R = sqrtf(R2);
-    return (R < a) ? R * (1.0f / a) : a * rsqrtf(R2);
+    return (R < a) ? __fdiv_rn(R, a) : __fdiv_rn(a, R);
   }
 };
 
@@ -71,14 +72,19 @@ struct KLog {
   static constexpr int id = AFMM_KERNEL_LOG;
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     if (R2 < 1e-10) return 0.0;
-    if (R2 < __dmul_rn(p.a, p.a)) return __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(0.5, R2), log(R2)), p.a), p.a);
-    return __dmul_rn(0.5, log(R2));
+    const double l = log_cr(R2);
+    if (R2 < __dmul_rn(p.a, p.a)) return __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(0.5, R2), l), p.a), p.a);
+    return __dmul_rn(0.5, l);
   }
-  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return eval_exact(R2, p); }
+  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) {
+    if (R2 < 1e-10) return 0.0;
+    if (R2 < p.a * p.a) return 0.5 * R2 * log(R2) / p.a / p.a;
+    return 0.5 * log(R2);
+  }
   __device__ __forceinline__ static float eval32(float R2, float a, float) {
     if (R2 < 1e-10f) return 0.0f;
-    float l = __logf(R2);
-    if (R2 < a * a) return 0.5f * R2 * l / (a * a);
+    float l = logf(R2);
+    if (R2 < a * a) return __fdiv_rn(0.5f * R2 * l, a * a);
     return 0.5f * l;
   }
 };
@@ -93,8 +99,12 @@ struct KOneOverR {
   __device__ __forceinline__ static double eval(double R2, const KernelParams&) {
     return R2 == 0.0 ? 0.0 : rsqrt(R2);
   }
+  // rsqrtf refined by one Newton-Raphson step y += y/2 (1 - R2 y^2)
   __device__ __forceinline__ static float eval32(float R2, float, float) {
-    return R2 == 0.0f ? 0.0f : rsqrtf(R2);
+    if (R2 == 0.0f) return 0.0f;
+    float y = rsqrtf(R2);
+    float e = fmaf(-R2 * y, y, 1.0f);
+    return fmaf(0.5f * y, e, y);
   }
 };
 
@@ -102,11 +112,11 @@ struct KOneOverR {
 struct KGaussian {
   static constexpr int id = AFMM_KERNEL_GAUSSIAN;
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
-    return exp(-__ddiv_rn(R2, p.param));
+    return exp_cr(-__ddiv_rn(R2, p.param));
   }
   __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return exp(-R2 / p.param); }
-  __device__ __forceinline__ static float eval32(float R2, float, float inv_param) {
-    return __expf(-R2 * inv_param);
+  __device__ __forceinline__ static float eval32(float R2, float, float param) {
+    return expf(-__fdiv_rn(R2, param));
   }
 };
 
@@ -173,6 +183,7 @@ struct LevelDev {
   float* l2p32_rm = nullptr;
   double2* anchor = nullptr;    // per box reference point for FP32 relative coordinates
   float2* skel_rel = nullptr;   // skeleton coordinates minus the box anchor (FP32)
+  float* qlo32 = nullptr;       // low FP32 part of the outgoing charges (qhat = qhat32 + qlo32)
   float* span = nullptr;        // per box max |skel_rel| component
   int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c
   double* m2l = nullptr;        // per box, per valid slot, block r_b x r_c column-major

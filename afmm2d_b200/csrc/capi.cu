@@ -107,7 +107,7 @@ __global__ void k_dense_rows(const double2* __restrict__ pts, const double* __re
   const double2 xi = pts[rows[t]];
   double s = 0.0, c = 0.0;
   for (int j = threadIdx.x; j < N; j += blockDim.x) {
-    double v = K::eval_exact(r2_exact(xi.x, xi.y, pts[j].x, pts[j].y), kp) * qs[j];
+    double v = K::eval(r2_exact(xi.x, xi.y, pts[j].x, pts[j].y), kp) * qs[j];
     double tt = s + v;
     c += (fabs(s) >= fabs(v)) ? ((s - tt) + v) : ((v - tt) + s);
     s = tt;
@@ -134,6 +134,31 @@ struct DenseRun {
   static void run(const double2* pts, const double* qs, int N, const int32_t* rows, int nrows, KernelParams kp,
                   double* out, cudaStream_t s) {
     k_dense_rows<K><<<nrows, 256, 0, s>>>(pts, qs, N, rows, kp, out);
+    AFMM_LAUNCH_CHECK();
+  }
+};
+
+template <class K>
+__global__ void k_kernel_pairs(const double2* __restrict__ a, const double2* __restrict__ b, long n, KernelParams kp,
+                               int mode, double* out) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double2 p = a[t], q = b[t];
+  if (mode == 0) {
+    out[t] = K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
+  } else if (mode == 1) {
+    double dx = p.x - q.x, dy = p.y - q.y;
+    out[t] = K::eval(dx * dx + dy * dy, kp);
+  } else {
+    float dx = (float)(p.x - q.x), dy = (float)(p.y - q.y);
+    out[t] = (double)K::eval32(fmaf(dx, dx, dy * dy), (float)kp.a, (float)kp.param);
+  }
+}
+
+template <class K>
+struct PairsRun {
+  static void run(const double2* a, const double2* b, long n, KernelParams kp, int mode, double* out) {
+    k_kernel_pairs<K><<<(int)((n + 255) / 256), 256>>>(a, b, n, kp, mode, out);
     AFMM_LAUNCH_CHECK();
   }
 };
@@ -170,10 +195,15 @@ void build_plan(afmm_handle* h) {
     v.qhat = d.qhat;
     v.yhat = d.yhat;
     v.qhat32 = d.qhat32;
+    v.qlo32 = d.qlo32;
     v.yhat32 = d.yhat32;
   }
   p.levels.nlev = 0;
   for (int j = 2; j <= h->L; ++j) p.levels.lv[p.levels.nlev++] = p.lv[j];
+  for (int j = 0; j <= h->L; ++j) {
+    p.rmax[j] = h->lv[j].rmax;
+    p.n1max[j] = h->lv[j].n1max;
+  }
   NearView& nv = p.near;
   nv.nleaf = h->lv[h->L].nbox;
   nv.nmax = *std::max_element(h->h_leaf_cnt.begin(), h->h_leaf_cnt.end());
@@ -652,6 +682,24 @@ afmm_status afmm_get_stream(afmm_handle* h, void** stream) {
   if (!h || !stream) return AFMM_BAD_ARG;
   *stream = (void*)h->stream;
   return AFMM_OK;
+}
+
+afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, const double* xy1, const double* xy2,
+                             double* out, int mode) {
+  if (!xy1 || !xy2 || !out || n < 0 || mode < 0 || mode > 2 || kernel_id < 0 || kernel_id > AFMM_KERNEL_GAUSSIAN)
+    return AFMM_BAD_ARG;
+  if (n == 0) return AFMM_OK;
+  return guard(nullptr, [&] {
+    check_device();
+    DevArena tmp;
+    double2* da = tmp.alloc<double2>(n);
+    double2* db = tmp.alloc<double2>(n);
+    double* dout = tmp.alloc<double>(n);
+    AFMM_CUDA(cudaMemcpy(da, xy1, sizeof(double2) * n, cudaMemcpyHostToDevice));
+    AFMM_CUDA(cudaMemcpy(db, xy2, sizeof(double2) * n, cudaMemcpyHostToDevice));
+    dispatch_kernel<PairsRun>(kernel_id, da, db, (long)n, KernelParams{kernel_id, a, param}, mode, dout);
+    AFMM_CUDA(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  });
 }
 
 afmm_status afmm_destroy(afmm_handle* h) {

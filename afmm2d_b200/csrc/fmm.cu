@@ -120,27 +120,35 @@ __global__ void k_scatter(const double* __restrict__ ys, const int64_t* __restri
   if (i < n) y[perm[i]] = ys[i];
 }
 
-// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b, one warp per box,
-// lanes over the outputs c, reading the row-major copy of L2P (coalesced).
-// src_b = leaf charges, or the concatenated outgoing charges of children 0..3.
-__global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
-  const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= v.nbox) return;
+// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b.  One CTA per
+// box: the rows are split into SW_WARPS contiguous ranges, one per warp, lanes
+// run over the outputs c on the row-major copy of L2P (coalesced); the warps'
+// partial sums are added in warp order.  src_b = leaf charges, or the
+// concatenated outgoing charges of children 0..3.
+__global__ void __launch_bounds__(SW_T) k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
+  extern __shared__ double part[];  // SW_WARPS x r
+  const long b = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r = v.rank[b];
   if (r == 0) return;
   const int n = v.node_off[b + 1] - v.node_off[b];
   const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
   const double* P = v.l2p_rm + v.l2p_off[b];  // n x r, row-major
-  double* out = v.qhat + v.skel_off[b];
+  const int i0 = (int)((long)n * warp / SW_WARPS), i1 = (int)((long)n * (warp + 1) / SW_WARPS);
   for (int c0 = 0; c0 < r; c0 += 32) {
     const int c = c0 + lane;
     if (c < r) {
       double s = 0.0;
-#pragma unroll 8
-      for (int i = 0; i < n; ++i) s += P[(long)i * r + c] * src[i];
-      out[c] = s;
+#pragma unroll 4
+      for (int i = i0; i < i1; ++i) s += P[(long)i * r + c] * src[i];
+      part[warp * r + c] = s;
     }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < r; c += SW_T) {
+    double s = 0.0;
+    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + c];
+    v.qhat[v.skel_off[b] + c] = s;
   }
 }
 
@@ -168,50 +176,72 @@ void l2p_transpose32(const LevelView& v, const float* cm, float* rm, cudaStream_
   AFMM_LAUNCH_CHECK();
 }
 
-// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch: one warp
-// per box, lanes over the box's skeleton rows, slots in order inner 0..15,
-// outer 0..23.
-__global__ void k_m2l_apply(LevelSet ls) {
-  long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch.  One CTA
+// per box (upper levels first, so the large boxes start early): warp w takes
+// the box's valid interaction-list slots w, w + SW_WARPS, ... in slot order,
+// lanes run over the box's skeleton rows on column-major blocks (coalesced);
+// the warps' partial sums are added in warp order.
+__global__ void __launch_bounds__(SW_T) k_m2l_apply(LevelSet ls) {
+  extern __shared__ double part[];  // SW_WARPS x r
+  __shared__ int s_slot[40], s_nvalid;
+  __shared__ long s_off[41];
+  long gb = blockIdx.x;
   int j = 0;
-  while (j < ls.nlev && gw >= ls.lv[j].nbox) gw -= ls.lv[j++].nbox;
+  while (j < ls.nlev && gb >= ls.lv[j].nbox) gb -= ls.lv[j++].nbox;
   if (j >= ls.nlev) return;
   const LevelView& v = ls.lv[j];
-  const long b = gw;
+  const long b = gb;
   const int r = v.rank[b];
   if (r == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    int m = 0;
+    long off = 0;
+    for (int s = 0; s < 40; ++s) {
+      int c = v.il[b * 40 + s];
+      if (c < 0) continue;
+      s_slot[m] = c;
+      s_off[m] = off;
+      off += (long)r * v.rank[c];
+      ++m;
+    }
+    s_nvalid = m;
+  }
+  __syncthreads();
   const double* M0 = v.m2l + v.m2l_off[b];
   for (int i0 = 0; i0 < r; i0 += 32) {
     const int i = i0 + lane;
     double acc = 0.0;
-    const double* M = M0;
-    for (int s = 0; s < 40; ++s) {
-      int c = v.il[b * 40 + s];
-      if (c < 0) continue;
-      const int rc = v.rank[c];
-      const double* qc = v.qhat + v.skel_off[c];
-      if (i < r) {
+    if (i < r)
+      for (int t = warp; t < s_nvalid; t += SW_WARPS) {
+        const int c = s_slot[t];
+        const int rc = v.rank[c];
+        const double* qc = v.qhat + v.skel_off[c];
+        const double* M = M0 + s_off[t];
 #pragma unroll 8
         for (int cc = 0; cc < rc; ++cc) acc += M[(long)cc * r + i] * qc[cc];
       }
-      M += (long)r * rc;
-    }
-    if (i < r) v.yhat[v.skel_off[b] + i] = acc;
+    if (i < r) part[warp * r + i] = acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < r; i += SW_T) {
+    double s = 0.0;
+    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + i];
+    v.yhat[v.skel_off[b] + i] = s;
   }
 }
 
 // L2L (src/AFMM2DTree.cpp:1180-1197): t = L2P_b yhat_b; added to the children's
-// incoming potentials, or written as the leaf potential.
-__global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
-  const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= v.nbox) return;
+// incoming potentials, or written as the leaf potential.  One CTA per box,
+// threads over rows (column-major L2P: coalesced).
+__global__ void __launch_bounds__(SW_T) k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys,
+                                              int leaf) {
+  const long b = blockIdx.x;
   const int r = v.rank[b];
   const int n = v.node_off[b + 1] - v.node_off[b];
   const double* P = v.l2p + v.l2p_off[b];
   const double* yb = v.yhat + v.skel_off[b];
-  for (int i = lane; i < n; i += 32) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
     double t = 0.0;
 #pragma unroll 8
     for (int c = 0; c < r; ++c) t += P[(long)c * n + i] * yb[c];
@@ -292,25 +322,25 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   if (tm) tm->mark(s, "m2m");
   for (int j = p.L; j >= 2; --j) {
     const LevelView& v = p.lv[j];
-    long thr = v.nbox * 32;
-    k_m2m<<<(int)((thr + 255) / 256), 256, 0, s>>>(v, j == p.L ? p.qs : p.lv[j + 1].qhat, j == p.L);
+    k_m2m<<<(int)v.nbox, SW_T, sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1), s>>>(
+        v, j == p.L ? p.qs : p.lv[j + 1].qhat, j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
   if (tm) tm->mark(s, "m2l");
   {
     long boxes = 0;
+    int rm = 1;
     for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
-    long thr = boxes * 32;
-    k_m2l_apply<<<(int)((thr + 255) / 256), 256, 0, s>>>(p.levels);
+    for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
+    k_m2l_apply<<<(int)boxes, SW_T, sizeof(double) * SW_WARPS * rm, s>>>(p.levels);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
   if (tm) tm->mark(s, "l2l");
   for (int j = 2; j <= p.L; ++j) {
     const LevelView& v = p.lv[j];
-    long thr = v.nbox * 32;
-    k_l2l<<<(int)((thr + 255) / 256), 256, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, p.ys, j == p.L);
+    k_l2l<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, p.ys, j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }

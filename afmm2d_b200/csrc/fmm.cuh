@@ -10,6 +10,11 @@
 namespace afmm {
 
 constexpr int kMaxLevels = 16;
+// CTA shape of the per-box sweep kernels.
+constexpr int SW_T = 256;
+constexpr int SW_WARPS = SW_T / 32;
+// threads for a per-box kernel whose work runs over up to n rows
+inline int sweep_threads(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 256); }
 
 // Device pointers of one level, passed by value to kernels.
 struct LevelView {
@@ -32,7 +37,8 @@ struct LevelView {
   const float* span = nullptr;        // per box max |skel_rel| component
   double* qhat = nullptr;
   double* yhat = nullptr;
-  float* qhat32 = nullptr;
+  float* qhat32 = nullptr;   // high FP32 part of qhat
+  float* qlo32 = nullptr;    // low FP32 part of qhat
   float* yhat32 = nullptr;
 };
 
@@ -97,6 +103,8 @@ struct MatvecPlan {
   double* ys = nullptr;  // sorted potentials
   float* qs32 = nullptr;
   LevelView lv[kMaxLevels];
+  int rmax[kMaxLevels] = {0};   // largest rank per level
+  int n1max[kMaxLevels] = {0};  // largest node count per level
   LevelSet levels;       // levels 2..L for the M2L launch
   NearView near;
 };

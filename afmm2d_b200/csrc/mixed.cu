@@ -1,8 +1,8 @@
 // Mixed-precision matvec: FP32 apply with FP64 where it matters.
 //
 // Same sweeps as the FP64 path (src/AFMM2DTree.cpp:1129-1213), with
-//  * L2P stored in FP32 (both layouts) for M2M and L2L, FP32 outgoing and
-//    incoming vectors;
+//  * L2P stored in FP32 (both layouts) and applied with FP64 accumulation to
+//    FP64 outgoing / incoming vectors (those vectors are small);
 //  * M2L evaluated on the fly from skeleton coordinates instead of reading
 //    stored blocks: K(R_b, R_c) entries are the kernel between skeleton points
 //    (src/AFMM2DTree.cpp:1080);
@@ -15,8 +15,11 @@
 //    coordinates lose more than ~2^-17 relative precision), and for the log
 //    kernel every pair with R2 near its 1e-10 diagonal convention, are
 //    re-evaluated in FP64 from the exact coordinates;
-//  * FP32 partial sums cover one interaction-list box (M2L) or one source leaf
-//    (near field) and are accumulated in FP64; outputs are FP64.
+//  * M2L: the outgoing charges are split into FP32 high and low parts, the
+//    products with the high part are summed with Kahan compensation per
+//    interaction-list box, and the per-box sums are accumulated in FP64;
+//  * near field: FP32 partial sums per source leaf, accumulated in FP64;
+//    outputs are FP64.
 #include <algorithm>
 
 #include "mixed.cuh"
@@ -74,13 +77,14 @@ __global__ void k_to_f32(const double* __restrict__ src, long n, float* dst) {
   if (i < n) dst[i] = (float)src[i];
 }
 
-// qs32[i] = q[perm[i]] for nrhs columns (column c of q at q + c*ldq; of qs32 at c*N)
-__global__ void k_gather32(const double* __restrict__ q, int64_t ldq, const int64_t* __restrict__ perm, int N,
-                           int nrhs, float* qs32) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)N * nrhs) return;
-  int c = (int)(t / N), i = (int)(t - (long)c * N);
-  qs32[t] = (float)q[(long)c * ldq + perm[i]];
+// qs[i] = q[perm[i]] in FP64 and FP32
+__global__ void k_gather_mixed(const double* __restrict__ q, const int64_t* __restrict__ perm, int N, double* qs,
+                               float* qs32) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  double v = q[perm[i]];
+  qs[i] = v;
+  qs32[i] = (float)v;
 }
 
 __global__ void k_scatter64(const double* __restrict__ ys, const int64_t* __restrict__ perm, int N, int nrhs,
@@ -91,25 +95,37 @@ __global__ void k_scatter64(const double* __restrict__ ys, const int64_t* __rest
   y[(long)c * ldy + perm[i]] = ys[t];
 }
 
-// M2M in FP32: one warp per box, lanes over outputs, row-major FP32 L2P.
-__global__ void k_m2m32(LevelView v, const float* __restrict__ src_all, int leaf) {
-  const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= v.nbox) return;
+// M2M with FP32 L2P (row-major) and FP64 accumulation: one CTA per box, rows
+// split across warps, lanes over outputs.  Writes qhat (FP64) and its FP32
+// high/low split.
+__global__ void __launch_bounds__(SW_T) k_m2m_mixed(LevelView v, const double* __restrict__ src_all, int leaf) {
+  extern __shared__ double part[];  // SW_WARPS x r
+  const long b = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int r = v.rank[b];
   if (r == 0) return;
   const int n = v.node_off[b + 1] - v.node_off[b];
-  const float* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
+  const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
   const float* P = v.l2p32_rm + v.l2p_off[b];
-  float* out = v.qhat32 + v.skel_off[b];
+  const int i0 = (int)((long)n * warp / SW_WARPS), i1 = (int)((long)n * (warp + 1) / SW_WARPS);
   for (int c0 = 0; c0 < r; c0 += 32) {
     const int c = c0 + lane;
     if (c < r) {
-      float s = 0.0f;
-#pragma unroll 8
-      for (int i = 0; i < n; ++i) s = fmaf(P[(long)i * r + c], src[i], s);
-      out[c] = s;
+      double s = 0.0;
+#pragma unroll 4
+      for (int i = i0; i < i1; ++i) s += (double)P[(long)i * r + c] * src[i];
+      part[warp * r + c] = s;
     }
+  }
+  __syncthreads();
+  const int so = v.skel_off[b];
+  for (int c = threadIdx.x; c < r; c += SW_T) {
+    double s = 0.0;
+    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + c];
+    v.qhat[so + c] = s;
+    float hi = (float)s;
+    v.qhat32[so + c] = hi;
+    v.qlo32[so + c] = (float)(s - (double)hi);
   }
 }
 
@@ -122,81 +138,102 @@ __device__ __forceinline__ float fallback_r2(float span_b, float span_c) {
   return t;
 }
 
-// M2L on the fly for every level: one warp per box, lanes over skeleton rows.
+// M2L on the fly for every level: one CTA per box (upper levels first), warp
+// w takes the valid interaction-list slots w, w + SW_WARPS, ...; lanes run
+// over the box's skeleton rows; partial sums are added in warp order.
 template <class K>
-__global__ void k_m2l32(LevelSet ls, KernelParams kp) {
-  long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
+__global__ void __launch_bounds__(SW_T) k_m2l32(LevelSet ls, KernelParams kp) {
+  extern __shared__ double part[];  // SW_WARPS x r
+  __shared__ int s_slot[40], s_nvalid;
+  long gb = blockIdx.x;
   int j = 0;
-  while (j < ls.nlev && gw >= ls.lv[j].nbox) gw -= ls.lv[j++].nbox;
+  while (j < ls.nlev && gb >= ls.lv[j].nbox) gb -= ls.lv[j++].nbox;
   if (j >= ls.nlev) return;
   const LevelView& v = ls.lv[j];
-  const long b = gw;
+  const long b = gb;
   const int r = v.rank[b];
   if (r == 0) return;
-  const float a32 = (float)kp.a, ip32 = (float)(1.0 / kp.param);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) {
+    int m = 0;
+    for (int s = 0; s < 40; ++s) {
+      int c = v.il[b * 40 + s];
+      if (c >= 0 && v.rank[c] > 0) s_slot[m++] = c;
+    }
+    s_nvalid = m;
+  }
+  __syncthreads();
+  const float a32 = (float)kp.a, p32 = (float)kp.param;
   const double2 ab = v.anchor[b];
   const float sb = v.span[b];
   const int so = v.skel_off[b];
   for (int i0 = 0; i0 < r; i0 += 32) {
     const int i = i0 + lane;
-    const bool act = i < r;
-    const float2 xi = act ? v.skel_rel[so + i] : make_float2(0.f, 0.f);
     double acc = 0.0;
-    for (int s = 0; s < 40; ++s) {
-      const int c = v.il[b * 40 + s];
-      if (c < 0) continue;
-      const int rc = v.rank[c];
-      const int sc = v.skel_off[c];
-      const double2 ac = v.anchor[c];
-      const float dxa = (float)(ab.x - ac.x), dya = (float)(ab.y - ac.y);
-      const float thr = fallback_r2<K>(sb, v.span[c]);
-      float part = 0.0f;
-      if (act) {
+    if (i < r) {
+      const float2 xi = v.skel_rel[so + i];
+      for (int t = warp; t < s_nvalid; t += SW_WARPS) {
+        const int c = s_slot[t];
+        const int rc = v.rank[c];
+        const int sc = v.skel_off[c];
+        const double2 ac = v.anchor[c];
+        const float ox = xi.x + (float)(ab.x - ac.x), oy = xi.y + (float)(ab.y - ac.y);
+        const float thr = fallback_r2<K>(sb, v.span[c]);
+        float sum = 0.0f, comp = 0.0f, lo = 0.0f;
 #pragma unroll 4
         for (int cc = 0; cc < rc; ++cc) {
           const float2 xc = v.skel_rel[sc + cc];
-          const float dx = (xi.x - xc.x) + dxa, dy = (xi.y - xc.y) + dya;
+          const float dx = ox - xc.x, dy = oy - xc.y;
           const float R2 = fmaf(dx, dx, dy * dy);
           float kv;
           if (R2 < thr) {
             const double2 p = v.skel_xy[so + i], q = v.skel_xy[sc + cc];
             kv = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
           } else {
-            kv = K::eval32(R2, a32, ip32);
+            kv = K::eval32(R2, a32, p32);
           }
-          part = fmaf(kv, v.qhat32[sc + cc], part);
+          // Kahan-compensated sum of kv * qhi; plain sum of kv * qlo
+          const float yk = fmaf(kv, v.qhat32[sc + cc], -comp);
+          const float tk = sum + yk;
+          comp = (tk - sum) - yk;
+          sum = tk;
+          lo = fmaf(kv, v.qlo32[sc + cc], lo);
         }
+        acc += (double)sum - (double)comp + (double)lo;
       }
-      acc += (double)part;
+      part[warp * r + i] = acc;
     }
-    if (act) v.yhat32[so + i] = (float)acc;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < r; i += SW_T) {
+    double s = 0.0;
+    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + i];
+    v.yhat[so + i] = s;
   }
 }
 
 template <class K>
 struct M2l32Run {
-  static void run(const LevelSet& ls, const KernelParams& kp, long boxes, cudaStream_t s) {
-    long thr = boxes * 32;
-    k_m2l32<K><<<(int)((thr + 255) / 256), 256, 0, s>>>(ls, kp);
+  static void run(const LevelSet& ls, const KernelParams& kp, long boxes, int rmax, cudaStream_t s) {
+    k_m2l32<K><<<(int)boxes, SW_T, sizeof(double) * SW_WARPS * std::max(rmax, 1), s>>>(ls, kp);
     AFMM_LAUNCH_CHECK();
   }
 };
 
-// L2L in FP32: lanes over rows; leaf potentials are written in FP64.
-__global__ void k_l2l32(LevelView v, float* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
-  const long b = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (b >= v.nbox) return;
+// L2L with FP32 L2P (column-major) and FP64 accumulation: one CTA per box,
+// threads over rows.
+__global__ void __launch_bounds__(SW_T) k_l2l_mixed(LevelView v, double* __restrict__ child_yhat,
+                                                    double* __restrict__ ys, int leaf) {
+  const long b = blockIdx.x;
   const int r = v.rank[b];
   const int n = v.node_off[b + 1] - v.node_off[b];
   const float* P = v.l2p32 + v.l2p_off[b];
-  const float* yb = v.yhat32 + v.skel_off[b];
-  for (int i = lane; i < n; i += 32) {
-    float t = 0.0f;
+  const double* yb = v.yhat + v.skel_off[b];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double t = 0.0;
 #pragma unroll 8
-    for (int c = 0; c < r; ++c) t = fmaf(P[(long)c * n + i], yb[c], t);
-    if (leaf) ys[v.leaf_start[b] + i] = (double)t;
+    for (int c = 0; c < r; ++c) t += (double)P[(long)c * n + i] * yb[c];
+    if (leaf) ys[v.leaf_start[b] + i] = t;
     else child_yhat[v.node_off[b] + i] += t;
   }
 }
@@ -213,7 +250,7 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const int T = blockDim.x;
-  const float a32 = (float)kp.a, ip32 = (float)(1.0 / kp.param);
+  const float a32 = (float)kp.a, p32 = (float)kp.param;
   const double2 ab = nv.anchor[b];
   const float sb = nv.span[b];
   constexpr int MAXT = 4;
@@ -254,7 +291,7 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
             const double2 p = nv.pts[s0 + i], q = nv.pts[c0 + t];
             kv = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
           } else {
-            kv = K::eval32(R2, a32, ip32);
+            kv = K::eval32(R2, a32, p32);
           }
           acc = fmaf(kv, sq[t], acc);
         }
@@ -297,7 +334,7 @@ void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevAr
     d.l2p32 = arena.alloc<float>(ne);
     d.l2p32_rm = arena.alloc<float>(ne);
     d.qhat32 = arena.alloc<float>(tr);
-    d.yhat32 = arena.alloc<float>(tr);
+    d.qlo32 = arena.alloc<float>(tr);
     k_anchor_level<<<nb(d.nbox, 128), 128, 0, s>>>(d.nbox, d.rank, d.skel_off, d.skel_xy, d.anchor, d.skel_rel, d.span);
     k_to_f32<<<nb(ne, 256), 256, 0, s>>>(d.l2p, d.h_l2p_off[d.nbox], d.l2p32);
     k_to_f32<<<nb(ne, 256), 256, 0, s>>>(d.l2p_rm, d.h_l2p_off[d.nbox], d.l2p32_rm);
@@ -318,6 +355,7 @@ void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevAr
 void mixed_reserve(MixedState& ms, int N, int nrhs, DevArena& arena) {
   if (ms.rhs_cap >= nrhs) return;
   ms.qs32 = arena.alloc<float>((size_t)N * nrhs);
+  ms.qs = arena.alloc<double>((size_t)N * nrhs);
   ms.ys = arena.alloc<double>((size_t)N * nrhs);
   ms.rhs_cap = nrhs;
 }
@@ -332,29 +370,32 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
                   cudaStream_t s, StageTimer* tm, int64_t* launches) {
   if (!ms.ready) throw Error{AFMM_BAD_ARG, "mixed precision operators are not set up"};
   const int N = p.N;
+  long boxes = 0;
+  int rm = 1;
+  for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
+  for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
   for (int c = 0; c < nrhs; ++c) {
-    const float* qs32 = ms.qs32;
     double* ys = ms.ys;
     if (tm) tm->mark(s, "gather");
-    k_gather32<<<nb(N, 256), 256, 0, s>>>(q + (long)c * ldq, ldq, p.perm, N, 1, ms.qs32);
+    k_gather_mixed<<<nb(N, 256), 256, 0, s>>>(q + (long)c * ldq, p.perm, N, ms.qs, ms.qs32);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
     for (int j = p.L; j >= 2; --j) {
       const LevelView& v = p.lv[j];
-      k_m2m32<<<nb(v.nbox * 32, 256), 256, 0, s>>>(v, j == p.L ? qs32 : p.lv[j + 1].qhat32, j == p.L);
+      k_m2m_mixed<<<(int)v.nbox, SW_T, sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1), s>>>(
+          v, j == p.L ? ms.qs : p.lv[j + 1].qhat, j == p.L);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
     if (tm) tm->mark(s, "m2l");
-    long boxes = 0;
-    for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
-    dispatch_kernel<M2l32Run>(p.kp.id, p.levels, p.kp, boxes, s);
+    dispatch_kernel<M2l32Run>(p.kp.id, p.levels, p.kp, boxes, rm, s);
     ++*launches;
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];
-      k_l2l32<<<nb(v.nbox * 32, 256), 256, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat32 : nullptr, ys, j == p.L);
+      k_l2l_mixed<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys,
+                                                                    j == p.L);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
@@ -363,7 +404,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     nv.anchor = ms.leaf_anchor;
     nv.rel = ms.rel;
     nv.span = ms.leaf_span;
-    dispatch_kernel<P2p32Run>(p.kp.id, nv, p.kp, qs32, ys, s);
+    dispatch_kernel<P2p32Run>(p.kp.id, nv, p.kp, ms.qs32, ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
     k_scatter64<<<nb(N, 256), 256, 0, s>>>(ys, p.perm, N, 1, y + (long)c * ldy, ldy);

@@ -16,6 +16,7 @@ struct MixedState {
   double* d_yout = nullptr; // N x host_cap staging for host outputs
   int rhs_cap = 0;          // RHS capacity of qs32 / ys
   float* qs32 = nullptr;    // sorted charges (FP32)
+  double* qs = nullptr;     // sorted charges (FP64)
   double* ys = nullptr;     // sorted potentials (FP64)
   double2* leaf_anchor = nullptr;
   float* leaf_span = nullptr;

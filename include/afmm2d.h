@@ -98,7 +98,7 @@ afmm_status afmm_assemble(afmm_handle* h);
 afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int precision,
                         int mem_device);
 
-/* Relative 2-norm error of the last matvec (first RHS) against a direct FP64
+/* Relative 2-norm error of the last FP64 matvec (its last RHS) against a direct FP64
  * evaluation over `nsample` leaf boxes chosen with `seed` (all leaves when
  * nsample <= 0).  Reproducible, unlike src/AFMM2D.cpp:68. */
 afmm_status afmm_eval_error(afmm_handle* h, int nsample, uint64_t seed, double* rel_err);
@@ -135,6 +135,15 @@ afmm_status afmm_get_counts(afmm_handle* h, int64_t* c7);
 afmm_status afmm_get_launch_count(afmm_handle* h, int64_t* n);
 /* The CUDA stream (cudaStream_t) the handle launches on. */
 afmm_status afmm_get_stream(afmm_handle* h, void** stream);
+
+/* Evaluates the kernel on n point pairs (host arrays, interleaved x,y):
+ * out[t] = K(xy1[t], xy2[t]) with box-size parameter a (2^-nLevels) and
+ * kernel parameter `param`.  mode 0: the setup arithmetic (operation order of
+ * the reference, correctly rounded log/exp); 1: the FP64 matvec form; 2: the
+ * FP32 form.  Replaces no reference interface (a diagnostic of
+ * userkernel::getMatrixEntry, include/kernel.hpp:58). */
+afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, const double* xy1, const double* xy2,
+                             double* out, int mode);
 
 afmm_status afmm_destroy(afmm_handle* h);
 const char* afmm_status_string(afmm_status s);

@@ -787,5 +787,12 @@ void afo_kd_total_order(int N, int L, const double* xy, int64_t* perm) {
   for (int i = 0; i < N; ++i) perm[i] = p[i];
 }
 
+// K(xy1[t], xy2[t]) with the restated kernels (host libm).
+void afo_kernel_pairs(int kernel_id, double a, double param, long n, const double* xy1, const double* xy2,
+                      double* out) {
+  Kern K{kernel_id, a, param};
+  for (long t = 0; t < n; ++t) out[t] = K(xy1[2 * t], xy1[2 * t + 1], xy2[2 * t], xy2[2 * t + 1]);
+}
+
 int afo_num_threads(void) { return omp_get_max_threads(); }
 }

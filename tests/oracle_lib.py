@@ -177,6 +177,19 @@ def dense_rows(pts, q, kernel, L, rows, kparam=0.01):
     return y
 
 
+def kernel_pairs(kernel, a, xy1, xy2, param=0.01):
+    """K(xy1[t], xy2[t]) with the oracle's kernels (host libm)."""
+    lib = oracle_lib()
+    lib.afo_kernel_pairs.argtypes = [I, D, D, L, vp, vp, vp]
+    lib.afo_kernel_pairs.restype = None
+    xy1 = np.ascontiguousarray(xy1, dtype=np.float64)
+    xy2 = np.ascontiguousarray(xy2, dtype=np.float64)
+    out = np.zeros(len(xy1))
+    kid = KERNEL_IDS[kernel] if isinstance(kernel, str) else kernel
+    lib.afo_kernel_pairs(kid, a, param, len(xy1), xy1.ctypes.data, xy2.ctypes.data, out.ctypes.data)
+    return out
+
+
 def kd_total_order(pts, L):
     lib = oracle_lib()
     pts = np.ascontiguousarray(pts, dtype=np.float64)
