@@ -179,18 +179,10 @@ struct LevelDev {
   int64_t* l2p_off = nullptr;   // nbox+1 prefix over n_b*r_b
   double* l2p = nullptr;        // per box n_b x r_b, column-major (row index fastest)
   double* l2p_rm = nullptr;     // the same, row-major (rank index fastest)
-  float* l2p32 = nullptr;
-  float* l2p32_rm = nullptr;
-  double2* anchor = nullptr;    // per box reference point for FP32 relative coordinates
-  float2* skel_rel = nullptr;   // skeleton coordinates minus the box anchor (FP32)
-  float* qlo32 = nullptr;       // low FP32 part of the outgoing charges (qhat = qhat32 + qlo32)
-  float* span = nullptr;        // per box max |skel_rel| component
   int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c
   double* m2l = nullptr;        // per box, per valid slot, block r_b x r_c column-major
   double* qhat = nullptr;       // outgoing charges, skel_off layout
   double* yhat = nullptr;       // incoming potentials, skel_off layout
-  float* qhat32 = nullptr;
-  float* yhat32 = nullptr;
   // host copies
   std::vector<int32_t> h_rank, h_skel_off;
   std::vector<int32_t> h_node_off;

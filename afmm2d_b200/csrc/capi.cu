@@ -184,19 +184,11 @@ void build_plan(afmm_handle* h) {
     v.l2p_off = d.l2p_off;
     v.l2p = d.l2p;
     v.l2p_rm = d.l2p_rm;
-    v.l2p32 = d.l2p32;
-    v.l2p32_rm = d.l2p32_rm;
     v.m2l_off = d.m2l_off;
     v.m2l = d.m2l;
     v.skel_xy = d.skel_xy;
-    v.skel_rel = d.skel_rel;
-    v.anchor = d.anchor;
-    v.span = d.span;
     v.qhat = d.qhat;
     v.yhat = d.yhat;
-    v.qhat32 = d.qhat32;
-    v.qlo32 = d.qlo32;
-    v.yhat32 = d.yhat32;
   }
   p.levels.nlev = 0;
   for (int j = 2; j <= h->L; ++j) p.levels.lv[p.levels.nlev++] = p.lv[j];

@@ -171,11 +171,6 @@ void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_
   AFMM_LAUNCH_CHECK();
 }
 
-void l2p_transpose32(const LevelView& v, const float* cm, float* rm, cudaStream_t s) {
-  k_l2p_transpose<float><<<(int)v.nbox, 256, 0, s>>>(v, cm, rm);
-  AFMM_LAUNCH_CHECK();
-}
-
 // M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch.  One CTA
 // per box (upper levels first, so the large boxes start early): warp w takes
 // the box's valid interaction-list slots w, w + SW_WARPS, ... in slot order,
@@ -312,6 +307,26 @@ struct P2p64Run {
   }
 };
 
+void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches) {
+  for (int j = p.L; j >= 2; --j) {
+    const LevelView& v = p.lv[j];
+    size_t sm = sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1);
+    allow_smem(k_m2m, sm);
+    k_m2m<<<(int)v.nbox, SW_T, sm, s>>>(v, j == p.L ? qs : p.lv[j + 1].qhat, j == p.L);
+    AFMM_LAUNCH_CHECK();
+    ++*launches;
+  }
+}
+
+void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches) {
+  for (int j = 2; j <= p.L; ++j) {
+    const LevelView& v = p.lv[j];
+    k_l2l<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys, j == p.L);
+    AFMM_LAUNCH_CHECK();
+    ++*launches;
+  }
+}
+
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches) {
   const int N = p.N;
   const int gb = (N + 255) / 256;
@@ -320,30 +335,21 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   AFMM_LAUNCH_CHECK();
   ++*launches;
   if (tm) tm->mark(s, "m2m");
-  for (int j = p.L; j >= 2; --j) {
-    const LevelView& v = p.lv[j];
-    k_m2m<<<(int)v.nbox, SW_T, sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1), s>>>(
-        v, j == p.L ? p.qs : p.lv[j + 1].qhat, j == p.L);
-    AFMM_LAUNCH_CHECK();
-    ++*launches;
-  }
+  sweep_m2m(p, p.qs, s, launches);
   if (tm) tm->mark(s, "m2l");
   {
     long boxes = 0;
     int rm = 1;
     for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
     for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
-    k_m2l_apply<<<(int)boxes, SW_T, sizeof(double) * SW_WARPS * rm, s>>>(p.levels);
+    size_t sm = sizeof(double) * SW_WARPS * rm;
+    allow_smem(k_m2l_apply, sm);
+    k_m2l_apply<<<(int)boxes, SW_T, sm, s>>>(p.levels);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
   if (tm) tm->mark(s, "l2l");
-  for (int j = 2; j <= p.L; ++j) {
-    const LevelView& v = p.lv[j];
-    k_l2l<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, p.ys, j == p.L);
-    AFMM_LAUNCH_CHECK();
-    ++*launches;
-  }
+  sweep_l2l(p, p.ys, s, launches);
   if (tm) tm->mark(s, "p2p");
   dispatch_kernel<P2p64Run>(p.kp.id, p.near, p.kp, p.qs, p.ys, s);
   ++*launches;

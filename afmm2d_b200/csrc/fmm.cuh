@@ -16,6 +16,15 @@ constexpr int SW_WARPS = SW_T / 32;
 // threads for a per-box kernel whose work runs over up to n rows
 inline int sweep_threads(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 256); }
 
+// Allows `bytes` of dynamic shared memory for kernel `fn` (needed above 48 KB).
+template <class F>
+inline void allow_smem(F* fn, size_t bytes) {
+  if (bytes > 48 * 1024) {
+    if (bytes > 227 * 1024) throw Error{AFMM_BAD_ARG, "per-box rank too large for the sweep kernels"};
+    AFMM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  }
+}
+
 // Device pointers of one level, passed by value to kernels.
 struct LevelView {
   long nbox = 0;
@@ -27,19 +36,11 @@ struct LevelView {
   const int64_t* l2p_off = nullptr;
   const double* l2p = nullptr;     // column-major (row index fastest)
   const double* l2p_rm = nullptr;  // row-major copy (rank index fastest)
-  const float* l2p32 = nullptr;
-  const float* l2p32_rm = nullptr;
   const int64_t* m2l_off = nullptr;
   double* m2l = nullptr;
   const double2* skel_xy = nullptr;
-  const float2* skel_rel = nullptr;   // skeleton minus box anchor (FP32)
-  const double2* anchor = nullptr;    // box anchors (FP64)
-  const float* span = nullptr;        // per box max |skel_rel| component
   double* qhat = nullptr;
   double* yhat = nullptr;
-  float* qhat32 = nullptr;   // high FP32 part of qhat
-  float* qlo32 = nullptr;    // low FP32 part of qhat
-  float* yhat32 = nullptr;
 };
 
 struct LevelSet {
@@ -101,7 +102,6 @@ struct MatvecPlan {
   const int64_t* perm = nullptr;
   double* qs = nullptr;  // sorted charges
   double* ys = nullptr;  // sorted potentials
-  float* qs32 = nullptr;
   LevelView lv[kMaxLevels];
   int rmax[kMaxLevels] = {0};   // largest rank per level
   int n1max[kMaxLevels] = {0};  // largest node count per level
@@ -112,7 +112,9 @@ struct MatvecPlan {
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
 void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
-void l2p_transpose32(const LevelView& v, const float* cm, float* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
+// The FP64 sweeps shared by both precisions (leaf charges qs in FP64).
+void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches);
+void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches);
 
 }  // namespace afmm

@@ -1,25 +1,23 @@
-// Mixed-precision matvec: FP32 apply with FP64 where it matters.
+// Mixed-precision matvec: FP32 where the work is and the error is small, FP64
+// where cancellation would amplify rounding.
 //
-// Same sweeps as the FP64 path (src/AFMM2DTree.cpp:1129-1213), with
-//  * L2P stored in FP32 (both layouts) and applied with FP64 accumulation to
-//    FP64 outgoing / incoming vectors (those vectors are small);
-//  * M2L evaluated on the fly from skeleton coordinates instead of reading
-//    stored blocks: K(R_b, R_c) entries are the kernel between skeleton points
-//    (src/AFMM2DTree.cpp:1080);
-//  * near field evaluated on the fly in FP32.
-// Precision safeguards:
-//  * coordinates are kept relative to a per-box anchor point in FP32, and the
-//    anchor difference of a box pair is formed in FP64 before rounding, so dx
-//    keeps ~2^-24 relative precision however clustered the points are;
-//  * pairs closer than 2^-7 of the two boxes' extents (where the FP32 relative
-//    coordinates lose more than ~2^-17 relative precision), and for the log
-//    kernel every pair with R2 near its 1e-10 diagonal convention, are
-//    re-evaluated in FP64 from the exact coordinates;
-//  * M2L: the outgoing charges are split into FP32 high and low parts, the
-//    products with the high part are summed with Kahan compensation per
-//    interaction-list box, and the per-box sums are accumulated in FP64;
-//  * near field: FP32 partial sums per source leaf, accumulated in FP64;
-//    outputs are FP64.
+// Same sweeps as the FP64 path (src/AFMM2DTree.cpp:1129-1213), changed in two
+// places:
+//  * M2L is evaluated on the fly from the skeleton coordinates instead of
+//    streaming stored blocks: the blocks are plain kernel entries between
+//    skeleton points (src/AFMM2DTree.cpp:1080), so the 8-byte-per-entry read
+//    becomes one FP64 kernel evaluation per entry.  It stays in FP64 because
+//    the outgoing charges are combinations with large, mixed-sign weights
+//    (ACA interpolation matrices) and FP32 entries lose ~10x to cancellation.
+//  * The near field is evaluated in FP32 from coordinates relative to a
+//    per-leaf anchor point (anchor differences formed in FP64 before
+//    rounding, so dx keeps ~2^-24 relative precision however clustered the
+//    points are); pairs closer than 2^-7 of the two leaves' extents, and for
+//    the log kernel every pair with R2 near its 1e-10 diagonal convention,
+//    are re-evaluated in FP64 from the exact coordinates.  FP32 partial sums
+//    cover one source leaf and are accumulated in FP64.
+// M2M / L2L keep FP64 operators (they move ~2 GB at N = 4M and carry the same
+// cancellation); inputs and outputs are FP64.
 #include <algorithm>
 
 #include "mixed.cuh"
@@ -28,26 +26,8 @@ namespace afmm {
 
 namespace {
 
-// Per box: anchor = first skeleton point; rel = skeleton - anchor (FP32);
+// Leaves: anchor = first point of the leaf; rel for every sorted point;
 // span = max |rel| component.
-__global__ void k_anchor_level(long nbox, const int32_t* __restrict__ rank, const int32_t* __restrict__ skel_off,
-                               const double2* __restrict__ skel_xy, double2* anchor, float2* rel, float* span) {
-  const long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nbox) return;
-  const int r = rank[b], so = skel_off[b];
-  double2 a = r > 0 ? skel_xy[so] : make_double2(0.0, 0.0);
-  float sp = 0.0f;
-  for (int l = 0; l < r; ++l) {
-    double2 p = skel_xy[so + l];
-    float2 d = make_float2((float)(p.x - a.x), (float)(p.y - a.y));
-    rel[so + l] = d;
-    sp = fmaxf(sp, fmaxf(fabsf(d.x), fabsf(d.y)));
-  }
-  anchor[b] = a;
-  span[b] = sp;
-}
-
-// Leaves: anchor = first point of the leaf; rel for every sorted point.
 __global__ void k_anchor_leaf(long nleaf, const int32_t* __restrict__ start, const int32_t* __restrict__ cnt,
                               const double2* __restrict__ pts, double2* anchor, float2* rel, float* span) {
   const long b = blockIdx.x;
@@ -72,11 +52,6 @@ __global__ void k_anchor_leaf(long nleaf, const int32_t* __restrict__ start, con
   }
 }
 
-__global__ void k_to_f32(const double* __restrict__ src, long n, float* dst) {
-  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) dst[i] = (float)src[i];
-}
-
 // qs[i] = q[perm[i]] in FP64 and FP32
 __global__ void k_gather_mixed(const double* __restrict__ q, const int64_t* __restrict__ perm, int N, double* qs,
                                float* qs32) {
@@ -87,49 +62,12 @@ __global__ void k_gather_mixed(const double* __restrict__ q, const int64_t* __re
   qs32[i] = (float)v;
 }
 
-__global__ void k_scatter64(const double* __restrict__ ys, const int64_t* __restrict__ perm, int N, int nrhs,
-                            double* y, int64_t ldy) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)N * nrhs) return;
-  int c = (int)(t / N), i = (int)(t - (long)c * N);
-  y[(long)c * ldy + perm[i]] = ys[t];
+__global__ void k_scatter64(const double* __restrict__ ys, const int64_t* __restrict__ perm, int N, double* y) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < N) y[perm[i]] = ys[i];
 }
 
-// M2M with FP32 L2P (row-major) and FP64 accumulation: one CTA per box, rows
-// split across warps, lanes over outputs.  Writes qhat (FP64) and its FP32
-// high/low split.
-__global__ void __launch_bounds__(SW_T) k_m2m_mixed(LevelView v, const double* __restrict__ src_all, int leaf) {
-  extern __shared__ double part[];  // SW_WARPS x r
-  const long b = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int r = v.rank[b];
-  if (r == 0) return;
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
-  const float* P = v.l2p32_rm + v.l2p_off[b];
-  const int i0 = (int)((long)n * warp / SW_WARPS), i1 = (int)((long)n * (warp + 1) / SW_WARPS);
-  for (int c0 = 0; c0 < r; c0 += 32) {
-    const int c = c0 + lane;
-    if (c < r) {
-      double s = 0.0;
-#pragma unroll 4
-      for (int i = i0; i < i1; ++i) s += (double)P[(long)i * r + c] * src[i];
-      part[warp * r + c] = s;
-    }
-  }
-  __syncthreads();
-  const int so = v.skel_off[b];
-  for (int c = threadIdx.x; c < r; c += SW_T) {
-    double s = 0.0;
-    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + c];
-    v.qhat[so + c] = s;
-    float hi = (float)s;
-    v.qhat32[so + c] = hi;
-    v.qlo32[so + c] = (float)(s - (double)hi);
-  }
-}
-
-// Threshold below which a pair is re-evaluated in FP64.
+// Threshold below which a near-field pair is re-evaluated in FP64.
 template <class K>
 __device__ __forceinline__ float fallback_r2(float span_b, float span_c) {
   float e = (span_b + span_c) * 0.0078125f;  // 2^-7 of the combined extent
@@ -138,11 +76,11 @@ __device__ __forceinline__ float fallback_r2(float span_b, float span_c) {
   return t;
 }
 
-// M2L on the fly for every level: one CTA per box (upper levels first), warp
-// w takes the valid interaction-list slots w, w + SW_WARPS, ...; lanes run
-// over the box's skeleton rows; partial sums are added in warp order.
+// M2L on the fly in FP64 for every level: one CTA per box (upper levels
+// first), warp w takes the valid interaction-list slots w, w + SW_WARPS, ...;
+// lanes run over the box's skeleton rows; partial sums are added in warp order.
 template <class K>
-__global__ void __launch_bounds__(SW_T) k_m2l32(LevelSet ls, KernelParams kp) {
+__global__ void __launch_bounds__(SW_T) k_m2l_otf(LevelSet ls, KernelParams kp) {
   extern __shared__ double part[];  // SW_WARPS x r
   __shared__ int s_slot[40], s_nvalid;
   long gb = blockIdx.x;
@@ -163,45 +101,32 @@ __global__ void __launch_bounds__(SW_T) k_m2l32(LevelSet ls, KernelParams kp) {
     s_nvalid = m;
   }
   __syncthreads();
-  const float a32 = (float)kp.a, p32 = (float)kp.param;
-  const double2 ab = v.anchor[b];
-  const float sb = v.span[b];
   const int so = v.skel_off[b];
   for (int i0 = 0; i0 < r; i0 += 32) {
     const int i = i0 + lane;
-    double acc = 0.0;
     if (i < r) {
-      const float2 xi = v.skel_rel[so + i];
+      const double2 xi = v.skel_xy[so + i];
+      double acc0 = 0.0, acc1 = 0.0;
       for (int t = warp; t < s_nvalid; t += SW_WARPS) {
         const int c = s_slot[t];
         const int rc = v.rank[c];
-        const int sc = v.skel_off[c];
-        const double2 ac = v.anchor[c];
-        const float ox = xi.x + (float)(ab.x - ac.x), oy = xi.y + (float)(ab.y - ac.y);
-        const float thr = fallback_r2<K>(sb, v.span[c]);
-        float sum = 0.0f, comp = 0.0f, lo = 0.0f;
-#pragma unroll 4
-        for (int cc = 0; cc < rc; ++cc) {
-          const float2 xc = v.skel_rel[sc + cc];
-          const float dx = ox - xc.x, dy = oy - xc.y;
-          const float R2 = fmaf(dx, dx, dy * dy);
-          float kv;
-          if (R2 < thr) {
-            const double2 p = v.skel_xy[so + i], q = v.skel_xy[sc + cc];
-            kv = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-          } else {
-            kv = K::eval32(R2, a32, p32);
-          }
-          // Kahan-compensated sum of kv * qhi; plain sum of kv * qlo
-          const float yk = fmaf(kv, v.qhat32[sc + cc], -comp);
-          const float tk = sum + yk;
-          comp = (tk - sum) - yk;
-          sum = tk;
-          lo = fmaf(kv, v.qlo32[sc + cc], lo);
+        const double2* xc = v.skel_xy + v.skel_off[c];
+        const double* qc = v.qhat + v.skel_off[c];
+        int cc = 0;
+        for (; cc + 1 < rc; cc += 2) {
+          const double2 p0 = xc[cc], p1 = xc[cc + 1];
+          const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+          const double dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
+          acc0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+          acc1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * qc[cc + 1];
         }
-        acc += (double)sum - (double)comp + (double)lo;
+        if (cc < rc) {
+          const double2 p0 = xc[cc];
+          const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+          acc0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+        }
       }
-      part[warp * r + i] = acc;
+      part[warp * r + i] = acc0 + acc1;
     }
   }
   __syncthreads();
@@ -213,30 +138,14 @@ __global__ void __launch_bounds__(SW_T) k_m2l32(LevelSet ls, KernelParams kp) {
 }
 
 template <class K>
-struct M2l32Run {
+struct M2lOtfRun {
   static void run(const LevelSet& ls, const KernelParams& kp, long boxes, int rmax, cudaStream_t s) {
-    k_m2l32<K><<<(int)boxes, SW_T, sizeof(double) * SW_WARPS * std::max(rmax, 1), s>>>(ls, kp);
+    size_t sm = sizeof(double) * SW_WARPS * std::max(rmax, 1);
+    allow_smem(k_m2l_otf<K>, sm);
+    k_m2l_otf<K><<<(int)boxes, SW_T, sm, s>>>(ls, kp);
     AFMM_LAUNCH_CHECK();
   }
 };
-
-// L2L with FP32 L2P (column-major) and FP64 accumulation: one CTA per box,
-// threads over rows.
-__global__ void __launch_bounds__(SW_T) k_l2l_mixed(LevelView v, double* __restrict__ child_yhat,
-                                                    double* __restrict__ ys, int leaf) {
-  const long b = blockIdx.x;
-  const int r = v.rank[b];
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const float* P = v.l2p32 + v.l2p_off[b];
-  const double* yb = v.yhat + v.skel_off[b];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double t = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < r; ++c) t += (double)P[(long)c * n + i] * yb[c];
-    if (leaf) ys[v.leaf_start[b] + i] = t;
-    else child_yhat[v.node_off[b] + i] += t;
-  }
-}
 
 // Near field in FP32 from leaf-relative coordinates: CTA per leaf, threads
 // over targets, source leaves (neighbours 0..7, then self) staged in
@@ -321,26 +230,8 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevArena& arena, cudaStream_t s,
+void mixed_setup(MatvecPlan& p, std::vector<LevelDev>&, MixedState& ms, DevArena& arena, cudaStream_t s,
                  int64_t* launches) {
-  const int L = p.L;
-  for (int j = 2; j <= L; ++j) {
-    LevelDev& d = lv[j];
-    const long tr = std::max<long>(d.total_rank, 1);
-    const long ne = std::max<long>(d.h_l2p_off[d.nbox], 1);
-    d.anchor = arena.alloc<double2>(d.nbox);
-    d.skel_rel = arena.alloc<float2>(tr);
-    d.span = arena.alloc<float>(d.nbox);
-    d.l2p32 = arena.alloc<float>(ne);
-    d.l2p32_rm = arena.alloc<float>(ne);
-    d.qhat32 = arena.alloc<float>(tr);
-    d.qlo32 = arena.alloc<float>(tr);
-    k_anchor_level<<<nb(d.nbox, 128), 128, 0, s>>>(d.nbox, d.rank, d.skel_off, d.skel_xy, d.anchor, d.skel_rel, d.span);
-    k_to_f32<<<nb(ne, 256), 256, 0, s>>>(d.l2p, d.h_l2p_off[d.nbox], d.l2p32);
-    k_to_f32<<<nb(ne, 256), 256, 0, s>>>(d.l2p_rm, d.h_l2p_off[d.nbox], d.l2p32_rm);
-    AFMM_LAUNCH_CHECK();
-    *launches += 3;
-  }
   NearView& nv = p.near;
   ms.leaf_anchor = arena.alloc<double2>(nv.nleaf);
   ms.leaf_span = arena.alloc<float>(nv.nleaf);
@@ -374,40 +265,27 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
   int rm = 1;
   for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
   for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
+  NearView nv = p.near;
+  nv.anchor = ms.leaf_anchor;
+  nv.rel = ms.rel;
+  nv.span = ms.leaf_span;
   for (int c = 0; c < nrhs; ++c) {
-    double* ys = ms.ys;
     if (tm) tm->mark(s, "gather");
     k_gather_mixed<<<nb(N, 256), 256, 0, s>>>(q + (long)c * ldq, p.perm, N, ms.qs, ms.qs32);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
-    for (int j = p.L; j >= 2; --j) {
-      const LevelView& v = p.lv[j];
-      k_m2m_mixed<<<(int)v.nbox, SW_T, sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1), s>>>(
-          v, j == p.L ? ms.qs : p.lv[j + 1].qhat, j == p.L);
-      AFMM_LAUNCH_CHECK();
-      ++*launches;
-    }
+    sweep_m2m(p, ms.qs, s, launches);
     if (tm) tm->mark(s, "m2l");
-    dispatch_kernel<M2l32Run>(p.kp.id, p.levels, p.kp, boxes, rm, s);
+    dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, boxes, rm, s);
     ++*launches;
     if (tm) tm->mark(s, "l2l");
-    for (int j = 2; j <= p.L; ++j) {
-      const LevelView& v = p.lv[j];
-      k_l2l_mixed<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys,
-                                                                    j == p.L);
-      AFMM_LAUNCH_CHECK();
-      ++*launches;
-    }
+    sweep_l2l(p, ms.ys, s, launches);
     if (tm) tm->mark(s, "p2p");
-    NearView nv = p.near;
-    nv.anchor = ms.leaf_anchor;
-    nv.rel = ms.rel;
-    nv.span = ms.leaf_span;
-    dispatch_kernel<P2p32Run>(p.kp.id, nv, p.kp, ms.qs32, ys, s);
+    dispatch_kernel<P2p32Run>(p.kp.id, nv, p.kp, ms.qs32, ms.ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
-    k_scatter64<<<nb(N, 256), 256, 0, s>>>(ys, p.perm, N, 1, y + (long)c * ldy, ldy);
+    k_scatter64<<<nb(N, 256), 256, 0, s>>>(ms.ys, p.perm, N, y + (long)c * ldy);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }

@@ -44,6 +44,7 @@ def cases():
     base[128:160, 1] = -0.0
     dup = np.concatenate([base, base[rng.permutation(1024)]])
     out["dups2k_log"] = (dup, rng.standard_normal(2048), 16, 8, "log")
+    out["dups2k_oneoverr"] = (dup, rng.standard_normal(2048), 16, 8, "one_over_r")
     return out
 
 
