@@ -18,9 +18,9 @@
 // identically in every CTA, so all CTAs take the same control flow.
 //
 // Arithmetic follows the reference operation by operation (no FMA, IEEE
-// division), so residuals, pivots and ranks equal the reference's wherever
-// the kernel entries are equal; only the dot-product summation order of the
-// stopping test differs.
+// division), and the dot products of the stopping test are correctly rounded
+// (double-double accumulation), so residuals, pivots, ranks and L2P equal the
+// reference's wherever the kernel entries are equal.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -188,11 +188,12 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
   double2* cols_xy = (double2*)place(AR_COLS);           // chunk
   double* V = (double*)place(AR_V);                      // vcap * chunk (shared memory)
   double* U = (double*)place(AR_U);                      // ucap * n1max (shared memory)
-  double* xdot = (double*)place(AR_XDOT);                // 2 * (rcap + 8): V-dot exchange
+  double* xdot = (double*)place(AR_XDOT);                // 2 parities x 2 x (rcap + 8): V-dot exchange (hi, lo)
   double* vcol = (double*)place(AR_SMALL);               // rcap
   double* udot = vcol + A.rcap;                          // rcap
   double* vdot = udot + A.rcap;                          // rcap
   double* uri = vdot + A.rcap;                           // rcap: U_l(ri)
+  double* vdlo = uri + A.rcap;                           // rcap: low part of this CTA's V-dots
   unsigned char* row_ok = place(AR_OK);                  // n1max
   unsigned char* col_ok = row_ok + A.n1max;              // chunk
   double* xarg = (double*)place(AR_XARG);                // 2 * 8: argmax exchange (shared memory)
@@ -364,31 +365,53 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
             Uk[i] = u;
           }
           __syncthreads();
-          // partial V_l . v over this CTA's columns, and U_l . u (redundant)
+          // Partial V_l . v over this CTA's columns and U_l . u (redundant in every
+          // CTA), accumulated in double-double: the cluster-wide sums are then
+          // rounded once, so they are the correctly rounded dot products
+          // whatever the summation order (the stopping test depends on them).
           for (int l = warp; l <= k; l += ACA_WARPS) {
             const double* Vl = Vrow(l);
-            double s = 0.0;
-            for (int j = lane; j < nloc; j += 32) s += Vl[j] * Vk[j];
-            for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-            if (lane == 0) vdot[l] = s;
+            dd sv{0.0, 0.0};
+            for (int j = lane; j < nloc; j += 32) {
+              const double a = Vl[j], c = Vk[j];
+              const double p = __dmul_rn(a, c);
+              sv = dd_add(sv, dd{p, __fma_rn(a, c, -p)});
+            }
+            for (int o = 16; o > 0; o >>= 1)
+              sv = dd_add(sv, dd{__shfl_down_sync(0xffffffffu, sv.hi, o), __shfl_down_sync(0xffffffffu, sv.lo, o)});
+            if (lane == 0) {
+              vdot[l] = sv.hi;
+              vdlo[l] = sv.lo;
+            }
             const double* Ul = Urow(l);
-            double t = 0.0;
-            for (int i = lane; i < n1; i += 32) t += Ul[i] * Uk[i];
-            for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
-            if (lane == 0) udot[l] = t;
+            dd su{0.0, 0.0};
+            for (int i = lane; i < n1; i += 32) {
+              const double a = Ul[i], c = Uk[i];
+              const double p = __dmul_rn(a, c);
+              su = dd_add(su, dd{p, __fma_rn(a, c, -p)});
+            }
+            for (int o = 16; o > 0; o >>= 1)
+              su = dd_add(su, dd{__shfl_down_sync(0xffffffffu, su.hi, o), __shfl_down_sync(0xffffffffu, su.lo, o)});
+            if (lane == 0) udot[l] = __dadd_rn(su.hi, su.lo);
           }
           __syncthreads();
-          const size_t xo = (size_t)xpar * (A.rcap + 8);
-          for (int l = tid; l <= k; l += ACA_T) xdot[xo + l] = vdot[l];
+          const size_t xo = (size_t)xpar * 2 * (A.rcap + 8);
+          for (int l = tid; l <= k; l += ACA_T) {
+            xdot[xo + 2 * l] = vdot[l];
+            xdot[xo + 2 * l + 1] = vdlo[l];
+          }
           if (tid == 0) {
             if (ownk == crank) col_ok[jok] = 0;
             row_ok[ri] = 0;
           }
           cluster.sync();
           for (int l = tid; l <= k; l += ACA_T) {
-            double s = 0.0;
-            for (int c = 0; c < C; ++c) s += xdot_of(c)[xo + l];
-            vdot[l] = s;
+            dd s{0.0, 0.0};
+            for (int c = 0; c < C; ++c) {
+              const double* xc = xdot_of(c) + xo;
+              s = dd_add(s, dd{xc[2 * l], xc[2 * l + 1]});
+            }
+            vdot[l] = __dadd_rn(s.hi, s.lo);
           }
           xpar ^= 1;
           __syncthreads();
@@ -555,12 +578,12 @@ __global__ void __launch_bounds__(L2P_T) k_l2p(L2pArgs P) {
       __syncthreads();
       const double d = Am[(size_t)kk * r + kk];
       if (d != 0.0) {
-        for (int i = kk + 1 + threadIdx.x; i < r; i += L2P_T) Am[(size_t)i * r + kk] /= d;
+        for (int i = kk + 1 + threadIdx.x; i < r; i += L2P_T) Am[(size_t)i * r + kk] = __ddiv_rn(Am[(size_t)i * r + kk], d);
         __syncthreads();
         const int m = r - kk - 1;
         for (int e = threadIdx.x; e < m * m; e += L2P_T) {
           int i = kk + 1 + e / m, j = kk + 1 + e % m;
-          Am[(size_t)i * r + j] -= Am[(size_t)i * r + kk] * Am[(size_t)kk * r + j];
+          Am[(size_t)i * r + j] = __dsub_rn(Am[(size_t)i * r + j], __dmul_rn(Am[(size_t)i * r + kk], Am[(size_t)kk * r + j]));
         }
       }
       __syncthreads();
@@ -626,8 +649,8 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     size_t sz[AR_N];
     sz[AR_ROWS] = sizeof(double2) * (size_t)n1max;
     sz[AR_COLS] = sizeof(double2) * (size_t)chunk;
-    sz[AR_XDOT] = sizeof(double) * 2 * (size_t)(rcap + 8);
-    sz[AR_SMALL] = sizeof(double) * 4 * (size_t)rcap;
+    sz[AR_XDOT] = sizeof(double) * 4 * (size_t)(rcap + 8);
+    sz[AR_SMALL] = sizeof(double) * 5 * (size_t)rcap;
     sz[AR_OK] = (size_t)n1max + chunk;
     sz[AR_XARG] = sizeof(double) * 16;
     auto al = [](size_t x) { return (x + 15) & ~(size_t)15; };

@@ -10,6 +10,8 @@
 //
 // Arithmetic: compiled with -ffp-contract=off (no FMA), like the reference's
 // own build flags, so kernel entries and ACA residuals round the same way.
+// log/exp and the ACA dot products are correctly rounded (cr_math.h), as in
+// the reference build here (its Eigen shim and user kernels) and on the GPU.
 // The reference's unqualified abs(double) is taken as the double overload
 // (the behaviour its published benchmarks imply).
 #include <omp.h>
@@ -20,6 +22,8 @@
 #include <cstdint>
 #include <cstring>
 #include <vector>
+
+#include "cr_math.h"
 
 namespace {
 
@@ -40,13 +44,13 @@ struct Kern {
       }
       case 1:  // examples/tutorial.cpp:22-35 (log with diagonal convention)
         if (R2 < 1e-10) return 0.0;
-        if (R2 < a * a) return 0.5 * R2 * std::log(R2) / a / a;
-        return 0.5 * std::log(R2);
+        if (R2 < a * a) return 0.5 * R2 * crm::log_cr(R2) / a / a;
+        return 0.5 * crm::log_cr(R2);
       case 2:  // 1/r, 0 at r = 0
         if (R2 == 0.0) return 0.0;
         return 1.0 / std::sqrt(R2);
       default:  // Gaussian exp(-R2/param)
-        return std::exp(-R2 / param);
+        return crm::exp_cr(-R2 / param);
     }
   }
 };
@@ -314,10 +318,9 @@ int argmax_abs(const std::vector<double>& v, const std::vector<char>& allowed) {
   return idx < 0 ? 0 : idx;  // an empty set yields index 0 (never used)
 }
 
+// Correctly rounded dot product (the shim's VectorXd::dot and squaredNorm).
 double dotp(const std::vector<double>& a, const std::vector<double>& b) {
-  double s = 0;
-  for (size_t i = 0; i < a.size(); ++i) s += a[i] * b[i];
-  return s;
+  return crm::dot_cr(a.data(), b.data(), (long)a.size());
 }
 
 // src/ACA.cpp:27-133 -- partially pivoted ACA returning row/col pivots.

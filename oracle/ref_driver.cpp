@@ -13,6 +13,8 @@
 //        R2 < 1e-10 -> 0;  R2 < a^2 -> 0.5*R2*log(R2)/a/a;  else 0.5*log(R2)
 //   2  1/r with 0 at r = 0
 //   3  Gaussian exp(-R2/p), p = kernel parameter (0.01 by default)
+// log and exp are correctly rounded (cr_math.h), so the entries are a
+// function of the coordinates alone, as on the device.
 #include <omp.h>
 
 #include <chrono>
@@ -20,6 +22,7 @@
 #include <cstring>
 
 #include "AFMM2D.hpp"
+#include "cr_math.h"
 
 static int g_kernel_id = 1;
 static double g_kparam = 0.01;
@@ -37,15 +40,15 @@ double userkernel::getMatrixEntry(const unsigned i, const unsigned j) {
     }
     case 1:
       if (R2 < 1e-10) return 0.0;
-      if (R2 < a * a) return 0.5 * R2 * log(R2) / a / a;
-      return 0.5 * log(R2);
+      if (R2 < a * a) return 0.5 * R2 * crm::log_cr(R2) / a / a;
+      return 0.5 * crm::log_cr(R2);
     case 2: {
       if (R2 == 0.0) return 0.0;
       double R = sqrt(R2);
       return 1.0 / R;
     }
     default:
-      return exp(-R2 / g_kparam);
+      return crm::exp_cr(-R2 / g_kparam);
   }
 }
 

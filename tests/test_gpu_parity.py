@@ -37,17 +37,9 @@ def test_assemble_and_matvec_golden(golden):
     a = make(golden)
     a.assemble()
     exact_kernel = golden["kernel"] in ("one_over_r", "one_over_r_scaled")
-    if golden["name"] == "dups2k_log":
-        # Exact duplicate points make the skeleton systems exactly singular;
-        # whether the reference's output ends up NaN then hinges on last-bit
-        # rounding of log, where the host libm is not correctly rounded in a
-        # few cases in 10^4 and this engine is (see the exact-kernel test).
-        # The tree and lists of this case are checked bit-exactly above; the
-        # duplicate-point matvec is checked with the 1/r kernel
-        # (dups2k_oneoverr), whose entries are bit-identical.
-        return
     if np.isnan(golden["y"]).any():
-        # singular skeleton systems: only the NaN pattern is comparable
+        # exact duplicate points make the skeleton systems singular and the
+        # reference's output NaN; only the NaN pattern is comparable
         y = a.computeMatVecProduct(golden["q"])
         np.testing.assert_array_equal(np.isnan(y), np.isnan(golden["y"]))
         return
