@@ -171,58 +171,76 @@ void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_
   AFMM_LAUNCH_CHECK();
 }
 
-// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch.  One CTA
-// per box (upper levels first, so the large boxes start early): warp w takes
-// the box's valid interaction-list slots w, w + SW_WARPS, ... in slot order,
-// lanes run over the box's skeleton rows on column-major blocks (coalesced);
-// the warps' partial sums are added in warp order.
-__global__ void __launch_bounds__(SW_T) k_m2l_apply(LevelSet ls) {
-  extern __shared__ double part[];  // SW_WARPS x r
-  __shared__ int s_slot[40], s_nvalid;
-  __shared__ long s_off[41];
-  long gb = blockIdx.x;
+// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch: one CTA
+// per box, upper levels first so the large boxes start early.  The work is
+// split into (slot, row) items over all threads: item (t, i) is row i of the
+// t-th valid interaction-list block times that box's outgoing charges
+// (column-major blocks: a warp's consecutive rows read contiguously); the
+// per-slot partial sums are then added per row in slot order, as the
+// reference adds M2L[k][c] * q_c slot by slot.
+__device__ __forceinline__ void stage_slots(const LevelView& v, long b, int r, SlotTable& st) {
+  int m = 0;
+  long off = 0;
+  for (int s = 0; s < 40; ++s) {
+    int c = v.il[b * 40 + s];
+    if (c < 0) continue;
+    const int rc = v.rank[c];
+    st.box[m] = c;
+    st.rank[m] = rc;
+    st.skel[m] = v.skel_off[c];
+    st.off[m] = off;
+    off += (long)r * rc;
+    ++m;
+  }
+  st.n = m;
+}
+
+__device__ __forceinline__ const LevelView* level_of_block(const LevelSet& ls, long& b) {
+  b = blockIdx.x;
   int j = 0;
-  while (j < ls.nlev && gb >= ls.lv[j].nbox) gb -= ls.lv[j++].nbox;
-  if (j >= ls.nlev) return;
-  const LevelView& v = ls.lv[j];
-  const long b = gb;
+  while (j < ls.nlev && b >= ls.lv[j].nbox) b -= ls.lv[j++].nbox;
+  return j < ls.nlev ? &ls.lv[j] : nullptr;
+}
+
+__global__ void __launch_bounds__(SW_T) k_m2l_apply(LevelSet ls) {
+  extern __shared__ double part[];  // nslots x rch
+  __shared__ SlotTable st;
+  long b;
+  const LevelView* vp = level_of_block(ls, b);
+  if (!vp) return;
+  const LevelView& v = *vp;
   const int r = v.rank[b];
   if (r == 0) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (threadIdx.x == 0) {
-    int m = 0;
-    long off = 0;
-    for (int s = 0; s < 40; ++s) {
-      int c = v.il[b * 40 + s];
-      if (c < 0) continue;
-      s_slot[m] = c;
-      s_off[m] = off;
-      off += (long)r * v.rank[c];
-      ++m;
-    }
-    s_nvalid = m;
-  }
+  if (threadIdx.x == 0) stage_slots(v, b, r, st);
   __syncthreads();
   const double* M0 = v.m2l + v.m2l_off[b];
-  for (int i0 = 0; i0 < r; i0 += 32) {
-    const int i = i0 + lane;
-    double acc = 0.0;
-    if (i < r)
-      for (int t = warp; t < s_nvalid; t += SW_WARPS) {
-        const int c = s_slot[t];
-        const int rc = v.rank[c];
-        const double* qc = v.qhat + v.skel_off[c];
-        const double* M = M0 + s_off[t];
-#pragma unroll 8
-        for (int cc = 0; cc < rc; ++cc) acc += M[(long)cc * r + i] * qc[cc];
+  const int so = v.skel_off[b];
+  for (int i0 = 0; i0 < r; i0 += M2L_RCH) {
+    const int rch = min(M2L_RCH, r - i0);
+    const int items = st.n * rch;
+    for (int it = threadIdx.x; it < items; it += SW_T) {
+      const int t = it / rch, i = i0 + (it - t * rch);
+      const int rc = st.rank[t];
+      const double* M = M0 + st.off[t] + i;
+      const double* qc = v.qhat + st.skel[t];
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      int cc = 0;
+      for (; cc + 3 < rc; cc += 4) {
+        a0 += M[(long)cc * r] * qc[cc];
+        a1 += M[(long)(cc + 1) * r] * qc[cc + 1];
+        a2 += M[(long)(cc + 2) * r] * qc[cc + 2];
+        a3 += M[(long)(cc + 3) * r] * qc[cc + 3];
       }
-    if (i < r) part[warp * r + i] = acc;
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < r; i += SW_T) {
-    double s = 0.0;
-    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + i];
-    v.yhat[v.skel_off[b] + i] = s;
+      for (; cc < rc; ++cc) a0 += M[(long)cc * r] * qc[cc];
+      part[it] = (a0 + a1) + (a2 + a3);
+    }
+    __syncthreads();
+    for (int ii = threadIdx.x; ii < rch; ii += SW_T) {
+      double s = 0.0;
+      for (int t = 0; t < st.n; ++t) s += part[t * rch + ii];
+      v.yhat[so + i0 + ii] = s;
+    }
+    __syncthreads();
   }
 }
 
@@ -245,64 +263,83 @@ __global__ void __launch_bounds__(SW_T) k_l2l(LevelView v, double* __restrict__ 
   }
 }
 
-// Near field (src/AFMM2DTree.cpp:1199-1213): per leaf, neighbours 0..7 then
-// the leaf itself, kernel evaluated on the fly from shared-memory tiles.
+// Near field (src/AFMM2DTree.cpp:1199-1213): per leaf, neighbours 0..7 and
+// the leaf itself, kernel evaluated on the fly.  One CTA per leaf; all source
+// leaves are staged in shared memory at once; G groups of NT threads split
+// the source leaves (group g takes leaves g, g+G, ...), each thread owns one
+// target, and the groups' sums are added in group order.
 template <class K>
-__global__ void k_p2p64(NearView nv, KernelParams kp, const double* __restrict__ qs, double* __restrict__ ys) {
+__global__ void k_p2p64(NearView nv, KernelParams kp, const double* __restrict__ qs, double* __restrict__ ys, int NT,
+                        int G) {
   extern __shared__ __align__(16) unsigned char smem[];
-  double2* sx = (double2*)smem;
-  double* sq = (double*)(sx + nv.nmax);
+  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
   const long b = blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
-  const int T = blockDim.x;
-  constexpr int MAXT = 4;
-  double2 xi[MAXT];
-  double pot[MAXT];
-  for (int u = 0; u < MAXT; ++u) {
-    int i = threadIdx.x + u * T;
-    if (i < n) {
-      xi[u] = nv.pts[s0 + i];
-      pot[u] = ys[s0 + i];
+  if (threadIdx.x == 0) {
+    int m = 0, off = 0;
+    for (int slot = 0; slot < 9; ++slot) {
+      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
+      if (c < 0) continue;
+      s_src[m] = nv.leaf_start[c];
+      s_cnt[m] = nv.leaf_cnt[c];
+      s_off[m] = off;
+      off += nv.leaf_cnt[c];
+      ++m;
     }
+    s_off[m] = off;
+    s_ns = m;
   }
-  for (int slot = 0; slot < 9; ++slot) {
-    const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-    if (c < 0) continue;
-    const int nc = nv.leaf_cnt[c];
-    const int c0 = nv.leaf_start[c];
-    __syncthreads();
-    for (int t = threadIdx.x; t < nc; t += T) {
-      sx[t] = nv.pts[c0 + t];
-      sq[t] = qs[c0 + t];
+  __syncthreads();
+  const int ns = s_ns, tot = s_off[ns];
+  double2* sx = (double2*)smem;
+  double* sq = (double*)(sx + 9 * nv.nmax);
+  double* red = sq + 9 * nv.nmax;  // G x NT
+  for (int m = 0; m < ns; ++m)
+    for (int t = threadIdx.x; t < s_cnt[m]; t += blockDim.x) {
+      sx[s_off[m] + t] = nv.pts[s_src[m] + t];
+      sq[s_off[m] + t] = qs[s_src[m] + t];
     }
-    __syncthreads();
-    for (int u = 0; u < MAXT; ++u) {
-      int i = threadIdx.x + u * T;
-      if (i < n) {
-        double acc = 0.0;
-        for (int t = 0; t < nc; ++t) {
-          double dx = xi[u].x - sx[t].x, dy = xi[u].y - sx[t].y;
-          acc += K::eval(dx * dx + dy * dy, kp) * sq[t];
-        }
-        pot[u] += acc;
+  __syncthreads();
+  (void)tot;
+  const int i = threadIdx.x % NT, g = threadIdx.x / NT;
+  double acc = 0.0;
+  if (i < n) {
+    const double2 xi = nv.pts[s0 + i];
+    for (int m = g; m < ns; m += G) {
+      const int o = s_off[m], nc = s_cnt[m];
+      double a0 = 0.0, a1 = 0.0;
+      int t = 0;
+      for (; t + 1 < nc; t += 2) {
+        const double2 p0 = sx[o + t], p1 = sx[o + t + 1];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y, dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
+        a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * sq[o + t + 1];
       }
+      if (t < nc) {
+        const double2 p0 = sx[o + t];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
+      }
+      acc += a0 + a1;
     }
   }
-  for (int u = 0; u < MAXT; ++u) {
-    int i = threadIdx.x + u * T;
-    if (i < n) ys[s0 + i] = pot[u];
+  red[g * NT + i] = acc;
+  __syncthreads();
+  if (g == 0 && i < n) {
+    double s = ys[s0 + i];
+    for (int h = 0; h < G; ++h) s += red[h * NT + i];
+    ys[s0 + i] = s;
   }
 }
 
 template <class K>
 struct P2p64Run {
   static void run(const NearView& nv, const KernelParams& kp, const double* qs, double* ys, cudaStream_t s) {
-    int T = std::min(256, ((nv.nmax + 3) / 4 + 31) / 32 * 32);
-    T = std::max(T, 64);
-    size_t smem = (size_t)nv.nmax * (sizeof(double2) + sizeof(double));
-    if (smem > 48 * 1024) AFMM_CUDA(cudaFuncSetAttribute(k_p2p64<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_p2p64<K><<<(int)nv.nleaf, T, smem, s>>>(nv, kp, qs, ys);
+    P2pShape sh = p2p_shape(nv.nmax);
+    size_t smem = (size_t)9 * nv.nmax * (sizeof(double2) + sizeof(double)) + sizeof(double) * sh.threads;
+    allow_smem(k_p2p64<K>, smem);
+    k_p2p64<K><<<(int)nv.nleaf, sh.threads, smem, s>>>(nv, kp, qs, ys, sh.nt, sh.g);
     AFMM_LAUNCH_CHECK();
   }
 };
@@ -342,7 +379,7 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
     int rm = 1;
     for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
     for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
-    size_t sm = sizeof(double) * SW_WARPS * rm;
+    size_t sm = sizeof(double) * 40 * std::min(rm, M2L_RCH);
     allow_smem(k_m2l_apply, sm);
     k_m2l_apply<<<(int)boxes, SW_T, sm, s>>>(p.levels);
     AFMM_LAUNCH_CHECK();

@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -108,6 +109,33 @@ struct MatvecPlan {
   LevelSet levels;       // levels 2..L for the M2L launch
   NearView near;
 };
+
+// M2L kernels work on (slot, row) items; rows are processed in chunks of at
+// most M2L_RCH so that the per-slot partial sums (40 x M2L_RCH doubles) fit
+// in shared memory.
+constexpr int M2L_RCH = 256;
+
+// Valid interaction-list slots of a box, staged by one thread.
+struct SlotTable {
+  int n;
+  int box[40];
+  int rank[40];
+  int skel[40];
+  long off[40];  // block offset within the box's M2L data (stored form)
+};
+
+// Near-field launch shape: NT threads per target group (targets rounded up to
+// a warp multiple), G groups splitting the (up to 9) source leaves.
+struct P2pShape {
+  int nt, g, threads;
+};
+inline P2pShape p2p_shape(int nmax) {
+  P2pShape p;
+  p.nt = (nmax + 31) / 32 * 32;
+  p.g = std::max(1, std::min(9, 256 / p.nt));
+  p.threads = p.nt * p.g;
+  return p;
+}
 
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);

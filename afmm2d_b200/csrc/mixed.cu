@@ -77,151 +77,187 @@ __device__ __forceinline__ float fallback_r2(float span_b, float span_c) {
 }
 
 // M2L on the fly in FP64 for every level: one CTA per box (upper levels
-// first), warp w takes the valid interaction-list slots w, w + SW_WARPS, ...;
-// lanes run over the box's skeleton rows; partial sums are added in warp order.
+// first), (slot, row) items over all threads, each item the dot product of
+// row i of K(R_b, R_c) -- evaluated from the skeleton coordinates -- with the
+// outgoing charges of slot box c; per-row sums in slot order.
 template <class K>
 __global__ void __launch_bounds__(SW_T) k_m2l_otf(LevelSet ls, KernelParams kp) {
-  extern __shared__ double part[];  // SW_WARPS x r
-  __shared__ int s_slot[40], s_nvalid;
-  long gb = blockIdx.x;
+  extern __shared__ double part[];  // nslots x rch
+  __shared__ SlotTable st;
+  long b = blockIdx.x;
   int j = 0;
-  while (j < ls.nlev && gb >= ls.lv[j].nbox) gb -= ls.lv[j++].nbox;
+  while (j < ls.nlev && b >= ls.lv[j].nbox) b -= ls.lv[j++].nbox;
   if (j >= ls.nlev) return;
   const LevelView& v = ls.lv[j];
-  const long b = gb;
   const int r = v.rank[b];
   if (r == 0) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (threadIdx.x == 0) {
     int m = 0;
     for (int s = 0; s < 40; ++s) {
       int c = v.il[b * 40 + s];
-      if (c >= 0 && v.rank[c] > 0) s_slot[m++] = c;
+      if (c < 0 || v.rank[c] == 0) continue;
+      st.box[m] = c;
+      st.rank[m] = v.rank[c];
+      st.skel[m] = v.skel_off[c];
+      ++m;
     }
-    s_nvalid = m;
+    st.n = m;
   }
   __syncthreads();
   const int so = v.skel_off[b];
-  for (int i0 = 0; i0 < r; i0 += 32) {
-    const int i = i0 + lane;
-    if (i < r) {
+  for (int i0 = 0; i0 < r; i0 += M2L_RCH) {
+    const int rch = min(M2L_RCH, r - i0);
+    const int items = st.n * rch;
+    for (int it = threadIdx.x; it < items; it += SW_T) {
+      const int t = it / rch, i = i0 + (it - t * rch);
+      const int rc = st.rank[t];
       const double2 xi = v.skel_xy[so + i];
-      double acc0 = 0.0, acc1 = 0.0;
-      for (int t = warp; t < s_nvalid; t += SW_WARPS) {
-        const int c = s_slot[t];
-        const int rc = v.rank[c];
-        const double2* xc = v.skel_xy + v.skel_off[c];
-        const double* qc = v.qhat + v.skel_off[c];
-        int cc = 0;
-        for (; cc + 1 < rc; cc += 2) {
-          const double2 p0 = xc[cc], p1 = xc[cc + 1];
-          const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
-          const double dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
-          acc0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
-          acc1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * qc[cc + 1];
-        }
-        if (cc < rc) {
-          const double2 p0 = xc[cc];
-          const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
-          acc0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
-        }
+      const double2* xc = v.skel_xy + st.skel[t];
+      const double* qc = v.qhat + st.skel[t];
+      double a0 = 0.0, a1 = 0.0;
+      int cc = 0;
+      for (; cc + 1 < rc; cc += 2) {
+        const double2 p0 = xc[cc], p1 = xc[cc + 1];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+        const double dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+        a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * qc[cc + 1];
       }
-      part[warp * r + i] = acc0 + acc1;
+      if (cc < rc) {
+        const double2 p0 = xc[cc];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+      }
+      part[it] = a0 + a1;
     }
-  }
-  __syncthreads();
-  for (int i = threadIdx.x; i < r; i += SW_T) {
-    double s = 0.0;
-    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + i];
-    v.yhat[so + i] = s;
+    __syncthreads();
+    for (int ii = threadIdx.x; ii < rch; ii += SW_T) {
+      double s = 0.0;
+      for (int t = 0; t < st.n; ++t) s += part[t * rch + ii];
+      v.yhat[so + i0 + ii] = s;
+    }
+    __syncthreads();
   }
 }
 
 template <class K>
 struct M2lOtfRun {
   static void run(const LevelSet& ls, const KernelParams& kp, long boxes, int rmax, cudaStream_t s) {
-    size_t sm = sizeof(double) * SW_WARPS * std::max(rmax, 1);
+    size_t sm = sizeof(double) * 40 * std::min(std::max(rmax, 1), M2L_RCH);
     allow_smem(k_m2l_otf<K>, sm);
     k_m2l_otf<K><<<(int)boxes, SW_T, sm, s>>>(ls, kp);
     AFMM_LAUNCH_CHECK();
   }
 };
 
-// Near field in FP32 from leaf-relative coordinates: CTA per leaf, threads
-// over targets, source leaves (neighbours 0..7, then self) staged in
-// shared memory.
+// Near field in FP32 from leaf-relative coordinates.  One CTA per leaf; all
+// source leaves (neighbours 0..7, then the leaf) are staged in shared memory
+// at once, with each source leaf's anchor offset folded in FP64; G groups of
+// NT threads split the source leaves, each thread owns one target, FP32
+// partial sums per source leaf are added in FP64, and the groups' sums are
+// added in group order.
 template <class K>
-__global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ qs32, double* __restrict__ ys) {
+__global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ qs32, double* __restrict__ ys, int NT,
+                        int G) {
   extern __shared__ __align__(16) unsigned char smem[];
-  float2* sx = (float2*)smem;
-  float* sq = (float*)(sx + nv.nmax);
+  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
+  __shared__ float s_dx[9], s_dy[9], s_thr[9];
   const long b = blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
-  const int T = blockDim.x;
   const float a32 = (float)kp.a, p32 = (float)kp.param;
-  const double2 ab = nv.anchor[b];
-  const float sb = nv.span[b];
-  constexpr int MAXT = 4;
-  float2 xi[MAXT];
-  double pot[MAXT];
-#pragma unroll
-  for (int u = 0; u < MAXT; ++u) {
-    int i = threadIdx.x + u * T;
-    xi[u] = i < n ? nv.rel[s0 + i] : make_float2(0.f, 0.f);
-    pot[u] = i < n ? ys[s0 + i] : 0.0;
-  }
-  for (int slot = 0; slot < 9; ++slot) {
-    const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-    if (c < 0) continue;
-    const int nc = nv.leaf_cnt[c];
-    const int c0 = nv.leaf_start[c];
-    const double2 ac = nv.anchor[c];
-    const float dxa = (float)(ab.x - ac.x), dya = (float)(ab.y - ac.y);
-    const float thr = fallback_r2<K>(sb, nv.span[c]);
-    __syncthreads();
-    for (int t = threadIdx.x; t < nc; t += T) {
-      sx[t] = nv.rel[c0 + t];
-      sq[t] = qs32[c0 + t];
+  if (threadIdx.x == 0) {
+    const double2 ab = nv.anchor[b];
+    const float sb = nv.span[b];
+    int m = 0, off = 0;
+    for (int slot = 0; slot < 9; ++slot) {
+      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
+      if (c < 0) continue;
+      const double2 ac = nv.anchor[c];
+      s_src[m] = nv.leaf_start[c];
+      s_cnt[m] = nv.leaf_cnt[c];
+      s_off[m] = off;
+      s_dx[m] = (float)(ab.x - ac.x);
+      s_dy[m] = (float)(ab.y - ac.y);
+      s_thr[m] = fallback_r2<K>(sb, nv.span[c]);
+      off += nv.leaf_cnt[c];
+      ++m;
     }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < MAXT; ++u) {
-      const int i = threadIdx.x + u * T;
-      if (i < n) {
-        float acc = 0.0f;
-        const float ox = xi[u].x + dxa, oy = xi[u].y + dya;
-#pragma unroll 4
-        for (int t = 0; t < nc; ++t) {
-          const float dx = ox - sx[t].x, dy = oy - sx[t].y;
-          const float R2 = fmaf(dx, dx, dy * dy);
-          float kv;
-          if (R2 < thr) {
-            const double2 p = nv.pts[s0 + i], q = nv.pts[c0 + t];
-            kv = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-          } else {
-            kv = K::eval32(R2, a32, p32);
-          }
-          acc = fmaf(kv, sq[t], acc);
+    s_off[m] = off;
+    s_ns = m;
+  }
+  __syncthreads();
+  const int ns = s_ns;
+  float2* sx = (float2*)smem;
+  float* sq = (float*)(sx + 9 * nv.nmax);
+  double* red = (double*)(((uintptr_t)(sq + 9 * nv.nmax) + 15) & ~(uintptr_t)15);  // G x NT
+  for (int m = 0; m < ns; ++m)
+    for (int t = threadIdx.x; t < s_cnt[m]; t += blockDim.x) {
+      sx[s_off[m] + t] = nv.rel[s_src[m] + t];
+      sq[s_off[m] + t] = qs32[s_src[m] + t];
+    }
+  __syncthreads();
+  const int i = threadIdx.x % NT, g = threadIdx.x / NT;
+  double acc = 0.0;
+  if (i < n) {
+    const float2 xi = nv.rel[s0 + i];
+    for (int m = g; m < ns; m += G) {
+      const int o = s_off[m], nc = s_cnt[m];
+      const float ox = xi.x + s_dx[m], oy = xi.y + s_dy[m], thr = s_thr[m];
+      float a0 = 0.0f, a1 = 0.0f;
+      int t = 0;
+      for (; t + 1 < nc; t += 2) {
+        const float2 p0 = sx[o + t], p1 = sx[o + t + 1];
+        const float dx0 = ox - p0.x, dy0 = oy - p0.y, dx1 = ox - p1.x, dy1 = oy - p1.y;
+        const float R0 = fmaf(dx0, dx0, dy0 * dy0), R1 = fmaf(dx1, dx1, dy1 * dy1);
+        float k0, k1;
+        if (R0 < thr) {
+          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t];
+          k0 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
+        } else {
+          k0 = K::eval32(R0, a32, p32);
         }
-        pot[u] += (double)acc;
+        if (R1 < thr) {
+          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t + 1];
+          k1 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
+        } else {
+          k1 = K::eval32(R1, a32, p32);
+        }
+        a0 = fmaf(k0, sq[o + t], a0);
+        a1 = fmaf(k1, sq[o + t + 1], a1);
       }
+      if (t < nc) {
+        const float2 p0 = sx[o + t];
+        const float dx0 = ox - p0.x, dy0 = oy - p0.y;
+        const float R0 = fmaf(dx0, dx0, dy0 * dy0);
+        float k0;
+        if (R0 < thr) {
+          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t];
+          k0 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
+        } else {
+          k0 = K::eval32(R0, a32, p32);
+        }
+        a0 = fmaf(k0, sq[o + t], a0);
+      }
+      acc += (double)a0 + (double)a1;
     }
   }
-#pragma unroll
-  for (int u = 0; u < MAXT; ++u) {
-    int i = threadIdx.x + u * T;
-    if (i < n) ys[s0 + i] = pot[u];
+  red[g * NT + i] = acc;
+  __syncthreads();
+  if (g == 0 && i < n) {
+    double s = ys[s0 + i];
+    for (int h = 0; h < G; ++h) s += red[h * NT + i];
+    ys[s0 + i] = s;
   }
 }
 
 template <class K>
 struct P2p32Run {
   static void run(const NearView& nv, const KernelParams& kp, const float* qs32, double* ys, cudaStream_t s) {
-    int T = std::min(256, ((nv.nmax + 3) / 4 + 31) / 32 * 32);
-    T = std::max(T, 64);
-    size_t smem = (size_t)nv.nmax * (sizeof(float2) + sizeof(float));
-    k_p2p32<K><<<(int)nv.nleaf, T, smem, s>>>(nv, kp, qs32, ys);
+    P2pShape sh = p2p_shape(nv.nmax);
+    size_t smem = (size_t)9 * nv.nmax * (sizeof(float2) + sizeof(float)) + 16 + sizeof(double) * sh.threads;
+    allow_smem(k_p2p32<K>, smem);
+    k_p2p32<K><<<(int)nv.nleaf, sh.threads, smem, s>>>(nv, kp, qs32, ys, sh.nt, sh.g);
     AFMM_LAUNCH_CHECK();
   }
 };
