@@ -53,6 +53,7 @@ __device__ __forceinline__ double r2_exact(double xi, double yi, double xj, doub
 // One over r, scaled (examples/testAFMM2D.cpp:9-20): R < a ? R/a : a/R.
 struct KOneOverRScaled {
   static constexpr int id = AFMM_KERNEL_ONE_OVER_R_SCALED;
+  __device__ __forceinline__ static double at_zero() { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     double R = __dsqrt_rn(R2);
     return (R < p.a) ? __ddiv_rn(R, p.a) : __ddiv_rn(p.a, R);
@@ -70,6 +71,7 @@ struct KOneOverRScaled {
 // log(r) with the diagonal convention (examples/tutorial.cpp:22-35).
 struct KLog {
   static constexpr int id = AFMM_KERNEL_LOG;
+  __device__ __forceinline__ static double at_zero() { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     if (R2 < 1e-10) return 0.0;
     const double l = log_cr(R2);
@@ -92,6 +94,7 @@ struct KLog {
 // 1/r with 0 at r = 0.
 struct KOneOverR {
   static constexpr int id = AFMM_KERNEL_ONE_OVER_R;
+  __device__ __forceinline__ static double at_zero() { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams&) {
     if (R2 == 0.0) return 0.0;
     return __ddiv_rn(1.0, __dsqrt_rn(R2));
@@ -111,6 +114,7 @@ struct KOneOverR {
 // Gaussian exp(-R2/param) (1 on the diagonal).
 struct KGaussian {
   static constexpr int id = AFMM_KERNEL_GAUSSIAN;
+  __device__ __forceinline__ static double at_zero() { return 1.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     return exp_cr(-__ddiv_rn(R2, p.param));
   }
@@ -172,6 +176,8 @@ struct LevelDev {
   int32_t* node_off = nullptr;  // nbox+1 prefix over box node counts
   int32_t* node_ids = nullptr;  // node lists (sorted-point ids)
   int32_t* rank = nullptr;      // nbox
+  int32_t* skel_box = nullptr;  // skeleton row -> box
+  int32_t* node_box = nullptr;  // node row -> box
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)

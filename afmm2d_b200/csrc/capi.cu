@@ -189,9 +189,18 @@ void build_plan(afmm_handle* h) {
     v.skel_xy = d.skel_xy;
     v.qhat = d.qhat;
     v.yhat = d.yhat;
+    v.skel_box = d.skel_box;
+    v.node_box = d.node_box;
+    v.nrows = d.total_rank;
+    v.nnodes = d.h_node_off.empty() ? 0 : d.h_node_off[d.nbox];
   }
   p.levels.nlev = 0;
-  for (int j = 2; j <= h->L; ++j) p.levels.lv[p.levels.nlev++] = p.lv[j];
+  p.levels.row0[0] = 0;
+  for (int j = 2; j <= h->L; ++j) {
+    p.levels.lv[p.levels.nlev] = p.lv[j];
+    p.levels.row0[p.levels.nlev + 1] = p.levels.row0[p.levels.nlev] + p.lv[j].nrows;
+    ++p.levels.nlev;
+  }
   for (int j = 0; j <= h->L; ++j) {
     p.rmax[j] = h->lv[j].rmax;
     p.n1max[j] = h->lv[j].n1max;
@@ -368,6 +377,12 @@ void do_assemble(afmm_handle* h) {
     v.m2l = h->arena.alloc<double>(v.h_m2l_off[v.nbox]);
     v.qhat = h->arena.alloc<double>(v.total_rank);
     v.yhat = h->arena.alloc<double>(v.total_rank);
+    // row -> box maps for the thread-per-row sweeps
+    v.skel_box = h->arena.alloc<int32_t>(v.total_rank);
+    v.node_box = h->arena.alloc<int32_t>(v.h_node_off[v.nbox]);
+    fill_box_map(v.skel_off, v.nbox, v.skel_box, s);
+    fill_box_map(v.node_off, v.nbox, v.node_box, s);
+    h->launches += 2;
   }
   for (int j = 2; j <= L; ++j) {
     LevelDev& v = h->lv[j];

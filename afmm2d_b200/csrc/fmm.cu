@@ -71,6 +71,17 @@ void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s) {
   AFMM_LAUNCH_CHECK();
 }
 
+__global__ void k_fill_box_map(const int32_t* __restrict__ off, long nbox, int32_t* map) {
+  long b = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbox) return;
+  for (int32_t t = off[b]; t < off[b + 1]; ++t) map[t] = (int32_t)b;
+}
+
+void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s) {
+  k_fill_box_map<<<(int)((nbox + 255) / 256), 256, 0, s>>>(off, nbox, map);
+  AFMM_LAUNCH_CHECK();
+}
+
 // ------------------------------------------------------------ M2L blocks
 // M2L[b][c] = K(R_b, R_c) for every valid inner/outer slot of b, in slot
 // order (src/AFMM2DTree.cpp:1070-1097), stored column-major r_b x r_c.
@@ -120,36 +131,29 @@ __global__ void k_scatter(const double* __restrict__ ys, const int64_t* __restri
   if (i < n) y[perm[i]] = ys[i];
 }
 
-// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b.  One CTA per
-// box: the rows are split into SW_WARPS contiguous ranges, one per warp, lanes
-// run over the outputs c on the row-major copy of L2P (coalesced); the warps'
-// partial sums are added in warp order.  src_b = leaf charges, or the
-// concatenated outgoing charges of children 0..3.
-__global__ void __launch_bounds__(SW_T) k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
-  extern __shared__ double part[];  // SW_WARPS x r
-  const long b = blockIdx.x;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b.  One thread per
+// output (skeleton row of the level), summing over the box's node rows on
+// the row-major copy of L2P (a warp's consecutive outputs read contiguously).
+// src_b = leaf charges, or the concatenated outgoing charges of children 0..3.
+__global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
+  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= v.nrows) return;
+  const int b = v.skel_box[row];
   const int r = v.rank[b];
-  if (r == 0) return;
+  const int c = (int)(row - v.skel_off[b]);
   const int n = v.node_off[b + 1] - v.node_off[b];
   const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
-  const double* P = v.l2p_rm + v.l2p_off[b];  // n x r, row-major
-  const int i0 = (int)((long)n * warp / SW_WARPS), i1 = (int)((long)n * (warp + 1) / SW_WARPS);
-  for (int c0 = 0; c0 < r; c0 += 32) {
-    const int c = c0 + lane;
-    if (c < r) {
-      double s = 0.0;
-#pragma unroll 4
-      for (int i = i0; i < i1; ++i) s += P[(long)i * r + c] * src[i];
-      part[warp * r + c] = s;
-    }
+  const double* P = v.l2p_rm + v.l2p_off[b] + c;  // (i, c) at i*r + c
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int i = 0;
+  for (; i + 3 < n; i += 4) {
+    a0 += P[(long)i * r] * src[i];
+    a1 += P[(long)(i + 1) * r] * src[i + 1];
+    a2 += P[(long)(i + 2) * r] * src[i + 2];
+    a3 += P[(long)(i + 3) * r] * src[i + 3];
   }
-  __syncthreads();
-  for (int c = threadIdx.x; c < r; c += SW_T) {
-    double s = 0.0;
-    for (int w = 0; w < SW_WARPS; ++w) s += part[w * r + c];
-    v.qhat[v.skel_off[b] + c] = s;
-  }
+  for (; i < n; ++i) a0 += P[(long)i * r] * src[i];
+  v.qhat[row] = (a0 + a1) + (a2 + a3);
 }
 
 // Row-major copy of L2P (per box, r fastest) for the M2M sweep.
@@ -171,96 +175,73 @@ void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_
   AFMM_LAUNCH_CHECK();
 }
 
-// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch: one CTA
-// per box, upper levels first so the large boxes start early.  The work is
-// split into (slot, row) items over all threads: item (t, i) is row i of the
-// t-th valid interaction-list block times that box's outgoing charges
-// (column-major blocks: a warp's consecutive rows read contiguously); the
-// per-slot partial sums are then added per row in slot order, as the
-// reference adds M2L[k][c] * q_c slot by slot.
-__device__ __forceinline__ void stage_slots(const LevelView& v, long b, int r, SlotTable& st) {
-  int m = 0;
-  long off = 0;
+// Level of flat row g of a LevelSet (row0 is its prefix of row counts).
+__device__ __forceinline__ int level_of_row(const LevelSet& ls, long g) {
+  int j = 0;
+  while (j + 1 < ls.nlev && g >= ls.row0[j + 1]) ++j;
+  return j;
+}
+
+// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch, one thread
+// per skeleton row (upper levels first): row i of box b sums, slot by slot in
+// the reference's order (inner 0..15, outer 0..23), row i of the stored block
+// M2L[b][c] (column-major: a warp's consecutive rows read contiguously) times
+// the outgoing charges of c.
+__global__ void k_m2l_apply(LevelSet ls) {
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ls.row0[ls.nlev]) return;
+  const LevelView& v = ls.lv[level_of_row(ls, g)];
+  const long row = g - ls.row0[level_of_row(ls, g)];
+  const int b = v.skel_box[row];
+  const int r = v.rank[b];
+  const int i = (int)(row - v.skel_off[b]);
+  const double* M = v.m2l + v.m2l_off[b] + i;
+  double acc = 0.0;
   for (int s = 0; s < 40; ++s) {
-    int c = v.il[b * 40 + s];
+    const int c = v.il[(long)b * 40 + s];
     if (c < 0) continue;
     const int rc = v.rank[c];
-    st.box[m] = c;
-    st.rank[m] = rc;
-    st.skel[m] = v.skel_off[c];
-    st.off[m] = off;
-    off += (long)r * rc;
-    ++m;
-  }
-  st.n = m;
-}
-
-__device__ __forceinline__ const LevelView* level_of_block(const LevelSet& ls, long& b) {
-  b = blockIdx.x;
-  int j = 0;
-  while (j < ls.nlev && b >= ls.lv[j].nbox) b -= ls.lv[j++].nbox;
-  return j < ls.nlev ? &ls.lv[j] : nullptr;
-}
-
-__global__ void __launch_bounds__(SW_T) k_m2l_apply(LevelSet ls) {
-  extern __shared__ double part[];  // nslots x rch
-  __shared__ SlotTable st;
-  long b;
-  const LevelView* vp = level_of_block(ls, b);
-  if (!vp) return;
-  const LevelView& v = *vp;
-  const int r = v.rank[b];
-  if (r == 0) return;
-  if (threadIdx.x == 0) stage_slots(v, b, r, st);
-  __syncthreads();
-  const double* M0 = v.m2l + v.m2l_off[b];
-  const int so = v.skel_off[b];
-  for (int i0 = 0; i0 < r; i0 += M2L_RCH) {
-    const int rch = min(M2L_RCH, r - i0);
-    const int items = st.n * rch;
-    for (int it = threadIdx.x; it < items; it += SW_T) {
-      const int t = it / rch, i = i0 + (it - t * rch);
-      const int rc = st.rank[t];
-      const double* M = M0 + st.off[t] + i;
-      const double* qc = v.qhat + st.skel[t];
-      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-      int cc = 0;
-      for (; cc + 3 < rc; cc += 4) {
-        a0 += M[(long)cc * r] * qc[cc];
-        a1 += M[(long)(cc + 1) * r] * qc[cc + 1];
-        a2 += M[(long)(cc + 2) * r] * qc[cc + 2];
-        a3 += M[(long)(cc + 3) * r] * qc[cc + 3];
-      }
-      for (; cc < rc; ++cc) a0 += M[(long)cc * r] * qc[cc];
-      part[it] = (a0 + a1) + (a2 + a3);
+    const double* qc = v.qhat + v.skel_off[c];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int cc = 0;
+    for (; cc + 3 < rc; cc += 4) {
+      a0 += M[(long)cc * r] * qc[cc];
+      a1 += M[(long)(cc + 1) * r] * qc[cc + 1];
+      a2 += M[(long)(cc + 2) * r] * qc[cc + 2];
+      a3 += M[(long)(cc + 3) * r] * qc[cc + 3];
     }
-    __syncthreads();
-    for (int ii = threadIdx.x; ii < rch; ii += SW_T) {
-      double s = 0.0;
-      for (int t = 0; t < st.n; ++t) s += part[t * rch + ii];
-      v.yhat[so + i0 + ii] = s;
-    }
-    __syncthreads();
+    for (; cc < rc; ++cc) a0 += M[(long)cc * r] * qc[cc];
+    acc += (a0 + a1) + (a2 + a3);
+    M += (long)r * rc;
   }
+  v.yhat[row] = acc;
 }
 
-// L2L (src/AFMM2DTree.cpp:1180-1197): t = L2P_b yhat_b; added to the children's
-// incoming potentials, or written as the leaf potential.  One CTA per box,
-// threads over rows (column-major L2P: coalesced).
-__global__ void __launch_bounds__(SW_T) k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys,
-                                              int leaf) {
-  const long b = blockIdx.x;
+// L2L (src/AFMM2DTree.cpp:1180-1197): t = L2P_b yhat_b, one thread per node
+// row of the level (column-major L2P: a warp's consecutive rows read
+// contiguously); added to the child's incoming potential (node row g of
+// level j is skeleton row g of level j+1), or written as the leaf potential.
+__global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= v.nnodes) return;
+  const int b = v.node_box[g];
   const int r = v.rank[b];
   const int n = v.node_off[b + 1] - v.node_off[b];
-  const double* P = v.l2p + v.l2p_off[b];
+  const int i = (int)(g - v.node_off[b]);
+  const double* P = v.l2p + v.l2p_off[b] + i;  // (i, c) at c*n + i
   const double* yb = v.yhat + v.skel_off[b];
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    double t = 0.0;
-#pragma unroll 8
-    for (int c = 0; c < r; ++c) t += P[(long)c * n + i] * yb[c];
-    if (leaf) ys[v.leaf_start[b] + i] = t;
-    else child_yhat[v.node_off[b] + i] += t;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int c = 0;
+  for (; c + 3 < r; c += 4) {
+    a0 += P[(long)c * n] * yb[c];
+    a1 += P[(long)(c + 1) * n] * yb[c + 1];
+    a2 += P[(long)(c + 2) * n] * yb[c + 2];
+    a3 += P[(long)(c + 3) * n] * yb[c + 3];
   }
+  for (; c < r; ++c) a0 += P[(long)c * n] * yb[c];
+  const double t = (a0 + a1) + (a2 + a3);
+  if (leaf) ys[v.leaf_start[b] + i] = t;
+  else child_yhat[g] += t;
 }
 
 // Near field (src/AFMM2DTree.cpp:1199-1213): per leaf, neighbours 0..7 and
@@ -347,9 +328,8 @@ struct P2p64Run {
 void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches) {
   for (int j = p.L; j >= 2; --j) {
     const LevelView& v = p.lv[j];
-    size_t sm = sizeof(double) * SW_WARPS * std::max(p.rmax[j], 1);
-    allow_smem(k_m2m, sm);
-    k_m2m<<<(int)v.nbox, SW_T, sm, s>>>(v, j == p.L ? qs : p.lv[j + 1].qhat, j == p.L);
+    if (v.nrows == 0) continue;
+    k_m2m<<<(int)((v.nrows + 127) / 128), 128, 0, s>>>(v, j == p.L ? qs : p.lv[j + 1].qhat, j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
@@ -358,7 +338,8 @@ void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* l
 void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches) {
   for (int j = 2; j <= p.L; ++j) {
     const LevelView& v = p.lv[j];
-    k_l2l<<<(int)v.nbox, sweep_threads(p.n1max[j]), 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys, j == p.L);
+    if (v.nnodes == 0) continue;
+    k_l2l<<<(int)((v.nnodes + 127) / 128), 128, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys, j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
@@ -375,13 +356,8 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   sweep_m2m(p, p.qs, s, launches);
   if (tm) tm->mark(s, "m2l");
   {
-    long boxes = 0;
-    int rm = 1;
-    for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
-    for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
-    size_t sm = sizeof(double) * 40 * std::min(rm, M2L_RCH);
-    allow_smem(k_m2l_apply, sm);
-    k_m2l_apply<<<(int)boxes, SW_T, sm, s>>>(p.levels);
+    const long rows = p.levels.row0[p.levels.nlev];
+    k_m2l_apply<<<(int)((rows + 127) / 128), 128, 0, s>>>(p.levels);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }

@@ -42,11 +42,18 @@ struct LevelView {
   const double2* skel_xy = nullptr;
   double* qhat = nullptr;
   double* yhat = nullptr;
+  const int32_t* skel_box = nullptr;  // skeleton row -> box
+  const int32_t* node_box = nullptr;  // node row -> box
+  long nrows = 0;                     // skeleton rows (sum of ranks)
+  long nnodes = 0;                    // node rows (sum of node counts)
 };
 
+// Levels 2..L and the prefix of their skeleton row counts: the M2L kernels
+// run one thread per skeleton row over this flat row space.
 struct LevelSet {
   int nlev = 0;
   LevelView lv[kMaxLevels];
+  long row0[kMaxLevels + 1] = {0};
 };
 
 // Leaf-level data for the near field.
@@ -138,6 +145,8 @@ inline P2pShape p2p_shape(int nmax) {
 }
 
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
+// map[off[b] + l] = b for l < off[b+1] - off[b]
+void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
 void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);

@@ -76,79 +76,65 @@ __device__ __forceinline__ float fallback_r2(float span_b, float span_c) {
   return t;
 }
 
-// M2L on the fly in FP64 for every level: one CTA per box (upper levels
-// first), (slot, row) items over all threads, each item the dot product of
-// row i of K(R_b, R_c) -- evaluated from the skeleton coordinates -- with the
-// outgoing charges of slot box c; per-row sums in slot order.
+// M2L on the fly in FP64 for every level, one thread per skeleton row
+// (upper levels first): row i of box b sums, slot by slot in the reference's
+// order, K(R_b[i], R_c[cc]) * qhat_c[cc] with the entries evaluated from the
+// skeleton coordinates (a warp's rows share the source points: broadcast
+// loads).
 template <class K>
-__global__ void __launch_bounds__(SW_T) k_m2l_otf(LevelSet ls, KernelParams kp) {
-  extern __shared__ double part[];  // nslots x rch
-  __shared__ SlotTable st;
-  long b = blockIdx.x;
+__global__ void k_m2l_otf(LevelSet ls, KernelParams kp) {
+  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= ls.row0[ls.nlev]) return;
   int j = 0;
-  while (j < ls.nlev && b >= ls.lv[j].nbox) b -= ls.lv[j++].nbox;
-  if (j >= ls.nlev) return;
+  while (j + 1 < ls.nlev && g >= ls.row0[j + 1]) ++j;
   const LevelView& v = ls.lv[j];
-  const int r = v.rank[b];
-  if (r == 0) return;
-  if (threadIdx.x == 0) {
-    int m = 0;
-    for (int s = 0; s < 40; ++s) {
-      int c = v.il[b * 40 + s];
-      if (c < 0 || v.rank[c] == 0) continue;
-      st.box[m] = c;
-      st.rank[m] = v.rank[c];
-      st.skel[m] = v.skel_off[c];
-      ++m;
+  const long row = g - ls.row0[j];
+  const int b = v.skel_box[row];
+  const double2 xi = v.skel_xy[row];
+  double acc = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int c = v.il[(long)b * 40 + s];
+    if (c < 0) continue;
+    const int rc = v.rank[c];
+    const double2* xc = v.skel_xy + v.skel_off[c];
+    const double* qc = v.qhat + v.skel_off[c];
+    double a0 = 0.0, a1 = 0.0;
+    int cc = 0;
+    for (; cc + 1 < rc; cc += 2) {
+      const double2 p0 = xc[cc], p1 = xc[cc + 1];
+      const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+      const double dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
+      a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+      a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * qc[cc + 1];
     }
-    st.n = m;
+    if (cc < rc) {
+      const double2 p0 = xc[cc];
+      const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+      a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
+    }
+    acc += a0 + a1;
   }
-  __syncthreads();
-  const int so = v.skel_off[b];
-  for (int i0 = 0; i0 < r; i0 += M2L_RCH) {
-    const int rch = min(M2L_RCH, r - i0);
-    const int items = st.n * rch;
-    for (int it = threadIdx.x; it < items; it += SW_T) {
-      const int t = it / rch, i = i0 + (it - t * rch);
-      const int rc = st.rank[t];
-      const double2 xi = v.skel_xy[so + i];
-      const double2* xc = v.skel_xy + st.skel[t];
-      const double* qc = v.qhat + st.skel[t];
-      double a0 = 0.0, a1 = 0.0;
-      int cc = 0;
-      for (; cc + 1 < rc; cc += 2) {
-        const double2 p0 = xc[cc], p1 = xc[cc + 1];
-        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
-        const double dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
-        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
-        a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * qc[cc + 1];
-      }
-      if (cc < rc) {
-        const double2 p0 = xc[cc];
-        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
-        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * qc[cc];
-      }
-      part[it] = a0 + a1;
-    }
-    __syncthreads();
-    for (int ii = threadIdx.x; ii < rch; ii += SW_T) {
-      double s = 0.0;
-      for (int t = 0; t < st.n; ++t) s += part[t * rch + ii];
-      v.yhat[so + i0 + ii] = s;
-    }
-    __syncthreads();
-  }
+  v.yhat[row] = acc;
 }
 
 template <class K>
 struct M2lOtfRun {
-  static void run(const LevelSet& ls, const KernelParams& kp, long boxes, int rmax, cudaStream_t s) {
-    size_t sm = sizeof(double) * 40 * std::min(std::max(rmax, 1), M2L_RCH);
-    allow_smem(k_m2l_otf<K>, sm);
-    k_m2l_otf<K><<<(int)boxes, SW_T, sm, s>>>(ls, kp);
+  static void run(const LevelSet& ls, const KernelParams& kp, cudaStream_t s) {
+    const long rows = ls.row0[ls.nlev];
+    k_m2l_otf<K><<<(int)((rows + 127) / 128), 128, 0, s>>>(ls, kp);
     AFMM_LAUNCH_CHECK();
   }
 };
+
+// Kernel entry of a close pair in FP64 from the exact coordinates; a point
+// with itself (the diagonal) takes the kernel's value at zero distance
+// without any FP64 work, so the self-interaction costs no divergent branch.
+template <class K>
+__device__ __forceinline__ float near_pair(const NearView& nv, const KernelParams& kp, int p, int q) {
+  if (p == q) return (float)K::at_zero();
+  const double2 a = nv.pts[p], c = nv.pts[q];
+  return (float)K::eval_exact(r2_exact(a.x, a.y, c.x, c.y), kp);
+}
 
 // Near field in FP32 from leaf-relative coordinates.  One CTA per leaf; all
 // source leaves (neighbours 0..7, then the leaf) are staged in shared memory
@@ -211,18 +197,10 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
         const float dx0 = ox - p0.x, dy0 = oy - p0.y, dx1 = ox - p1.x, dy1 = oy - p1.y;
         const float R0 = fmaf(dx0, dx0, dy0 * dy0), R1 = fmaf(dx1, dx1, dy1 * dy1);
         float k0, k1;
-        if (R0 < thr) {
-          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t];
-          k0 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-        } else {
-          k0 = K::eval32(R0, a32, p32);
-        }
-        if (R1 < thr) {
-          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t + 1];
-          k1 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-        } else {
-          k1 = K::eval32(R1, a32, p32);
-        }
+        if (R0 < thr) k0 = near_pair<K>(nv, kp, s0 + i, s_src[m] + t);
+        else k0 = K::eval32(R0, a32, p32);
+        if (R1 < thr) k1 = near_pair<K>(nv, kp, s0 + i, s_src[m] + t + 1);
+        else k1 = K::eval32(R1, a32, p32);
         a0 = fmaf(k0, sq[o + t], a0);
         a1 = fmaf(k1, sq[o + t + 1], a1);
       }
@@ -231,12 +209,8 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
         const float dx0 = ox - p0.x, dy0 = oy - p0.y;
         const float R0 = fmaf(dx0, dx0, dy0 * dy0);
         float k0;
-        if (R0 < thr) {
-          const double2 p = nv.pts[s0 + i], q = nv.pts[s_src[m] + t];
-          k0 = (float)K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-        } else {
-          k0 = K::eval32(R0, a32, p32);
-        }
+        if (R0 < thr) k0 = near_pair<K>(nv, kp, s0 + i, s_src[m] + t);
+        else k0 = K::eval32(R0, a32, p32);
         a0 = fmaf(k0, sq[o + t], a0);
       }
       acc += (double)a0 + (double)a1;
@@ -297,10 +271,6 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
                   cudaStream_t s, StageTimer* tm, int64_t* launches) {
   if (!ms.ready) throw Error{AFMM_BAD_ARG, "mixed precision operators are not set up"};
   const int N = p.N;
-  long boxes = 0;
-  int rm = 1;
-  for (int j = 0; j < p.levels.nlev; ++j) boxes += p.levels.lv[j].nbox;
-  for (int j = 2; j <= p.L; ++j) rm = std::max(rm, p.rmax[j]);
   NearView nv = p.near;
   nv.anchor = ms.leaf_anchor;
   nv.rel = ms.rel;
@@ -313,7 +283,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     if (tm) tm->mark(s, "m2m");
     sweep_m2m(p, ms.qs, s, launches);
     if (tm) tm->mark(s, "m2l");
-    dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, boxes, rm, s);
+    dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
     ++*launches;
     if (tm) tm->mark(s, "l2l");
     sweep_l2l(p, ms.ys, s, launches);
