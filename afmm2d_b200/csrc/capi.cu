@@ -36,6 +36,7 @@ struct afmm_handle {
   double* d_y = nullptr;
   MatvecPlan plan;
   MixedState mixed;
+  BatchState batch;
   StageTimer timer;
   bool profiling = false;
   std::vector<std::pair<std::string, double>> stage_ms;
@@ -492,17 +493,22 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
     StageTimer* tm = h->profiling ? &h->timer : nullptr;
     if (precision == AFMM_PREC_MIXED) {
       mixed_reserve(h->mixed, h->N, 1, h->arena);
+      if (nrhs > 1) batch_reserve(h->plan, h->batch, h->arena, s);
+      auto run = [&](const double* qq, int64_t ldq, double* yy, int64_t ldy) {
+        if (nrhs > 1) matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nrhs, s, tm, &h->launches);
+        else matvec_mixed(h->plan, h->mixed, qq, ldq, yy, ldy, nrhs, s, tm, &h->launches);
+      };
       if (!mem_device) {
         if (h->mixed.host_cap < (size_t)nrhs) mixed_reserve_io(h->mixed, h->N, nrhs, h->arena);
         if (tm) tm->mark(s, "h2d");
         for (int c = 0; c < nrhs; ++c)
           AFMM_CUDA(cudaMemcpyAsync(h->mixed.d_qin + (size_t)c * h->N, q + (size_t)c * ld, bytes, cudaMemcpyHostToDevice, s));
-        matvec_mixed(h->plan, h->mixed, h->mixed.d_qin, h->N, h->mixed.d_yout, h->N, nrhs, s, tm, &h->launches);
+        run(h->mixed.d_qin, h->N, h->mixed.d_yout, h->N);
         if (tm) tm->mark(s, "d2h");
         for (int c = 0; c < nrhs; ++c)
           AFMM_CUDA(cudaMemcpyAsync(y + (size_t)c * ld, h->mixed.d_yout + (size_t)c * h->N, bytes, cudaMemcpyDeviceToHost, s));
       } else {
-        matvec_mixed(h->plan, h->mixed, q, ld, y, ld, nrhs, s, tm, &h->launches);
+        run(q, ld, y, ld);
       }
       if (tm) tm->mark(s, "end");
     } else {

@@ -23,6 +23,23 @@ struct MixedState {
   float2* rel = nullptr;    // sorted point minus its leaf anchor (FP32)
 };
 
+// Buffers of the batched path (kBatchMax right-hand sides per pass).
+constexpr int kBatchMax = 16;
+struct BatchState {
+  bool ready = false;
+  double* qs = nullptr;     // sorted charges, point-major N x kBatchMax
+  float* qs32 = nullptr;
+  double* ys = nullptr;     // sorted potentials, point-major
+  double* qhat[kMaxLevels] = {nullptr};
+  double* yhat[kMaxLevels] = {nullptr};
+  const double** d_qhat_lv = nullptr;  // device copies indexed by level - 2
+  double** d_yhat_lv = nullptr;
+};
+void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s);
+// y = K q for nrhs > 1 columns in passes of 4, 8 or 16 right-hand sides.
+void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const double* q, int64_t ldq, double* y,
+                    int64_t ldy, int nrhs, cudaStream_t s, StageTimer* tm, int64_t* launches);
+
 // Builds the FP32 operators and anchors after assembly.
 void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevArena& arena, cudaStream_t s,
                  int64_t* launches);

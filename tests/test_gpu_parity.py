@@ -241,3 +241,33 @@ def correctly_rounded_kernel(kernel, a, p, q, param=0.01):
     if kernel == "gaussian":
         return float(Decimal(-(R2 / param)).exp())
     raise AssertionError("kernel without transcendental: " + kernel)
+
+
+@pytest.mark.parametrize("nrhs", [3, 8, 21])
+def test_batched_mixed_vs_fp64(nrhs):
+    """Batched mixed path (passes of 4, 8 and 16 right-hand sides, ragged
+    remainders) against the FP64 path, column by column."""
+    pts, _, _ = workloads.make("mixture4m", N=65536)
+    a = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
+    a.assemble()
+    Q = np.random.default_rng(nrhs).standard_normal((65536, nrhs))
+    Ym = a.computeMatVecProduct(Q, precision="mixed")
+    for c in range(nrhs):
+        y64 = a.computeMatVecProduct(Q[:, c])
+        assert np.linalg.norm(Ym[:, c] - y64) / np.linalg.norm(y64) <= MIXED_TOL, c
+
+
+def test_batched_host_device_and_kernels():
+    torch = pytest.importorskip("torch")
+    pts, _, _ = workloads.make("gauss1m", N=16384)
+    a = A.AFMM(16384, 64, 8, pts, kernel="gaussian")
+    a.assemble()
+    Q = np.random.default_rng(7).standard_normal((16384, 16))
+    Yh = a.computeMatVecProduct(Q, precision="mixed")
+    dq = torch.tensor(Q.T.copy(), device="cuda")
+    dy = torch.zeros_like(dq)
+    a.matvec_device(dq.data_ptr(), dy.data_ptr(), 16, 16384, precision="mixed")
+    np.testing.assert_array_equal(dy.cpu().numpy().T, Yh)
+    for c in (0, 15):
+        y64 = a.computeMatVecProduct(Q[:, c])
+        assert np.linalg.norm(Yh[:, c] - y64) / np.linalg.norm(y64) <= MIXED_TOL
