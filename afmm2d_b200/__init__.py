@@ -50,6 +50,7 @@ _SIGS = {
     "afmm_get_launch_count": [_vp, _vp],
     "afmm_get_stream": [_vp, _vp],
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
+    "afmm_measure_fma_peaks": [_vp, _vp],
     "afmm_destroy": [_vp],
 }
 _lib = None
@@ -100,6 +101,13 @@ def kernel_eval(kernel, a, xy1, xy2, mode="exact", param=0.01):
     m = {"exact": 0, "fp64": 1, "fp32": 2}[mode]
     _check(lib().afmm_kernel_eval(kid, float(a), float(param), len(xy1), _ptr(xy1), _ptr(xy2), _ptr(out), m))
     return out
+
+
+def measure_fma_peaks():
+    """(FP64, FP32) FMA throughput of the current device in TFLOP/s."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    _check(lib().afmm_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b)))
+    return a.value, b.value
 
 
 def nlevels(N, M):

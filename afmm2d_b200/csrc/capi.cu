@@ -139,6 +139,47 @@ struct DenseRun {
   }
 };
 
+// FMA throughput: 8 independent chains per thread, `iters` rounds.
+template <class T>
+__global__ void k_fma_peak(T seed, int iters, T* out) {
+  T a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = seed + (T)(threadIdx.x + k);
+  const T m = (T)0.999999, c = (T)1e-7;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = a[k] * m + c;
+  }
+  T s = 0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += a[k];
+  if (s == (T)-1) out[0] = s;  // never true; keeps the chains live
+}
+
+template <class T>
+double fma_peak_tflops() {
+  int dev = 0, sms = 0;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  AFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DevArena tmp;
+  T* out = tmp.alloc<T>(1);
+  const int blocks = sms * 8, threads = 256, iters = sizeof(T) == 8 ? 8192 : 16384;
+  k_fma_peak<T><<<blocks, threads>>>((T)1, 64, out);  // warm-up
+  cudaEvent_t e0, e1;
+  AFMM_CUDA(cudaEventCreate(&e0));
+  AFMM_CUDA(cudaEventCreate(&e1));
+  AFMM_CUDA(cudaEventRecord(e0));
+  k_fma_peak<T><<<blocks, threads>>>((T)1, iters, out);
+  AFMM_CUDA(cudaEventRecord(e1));
+  AFMM_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  AFMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  AFMM_LAUNCH_CHECK();
+  return 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3) / 1e12;
+}
+
 template <class K>
 __global__ void k_kernel_pairs(const double2* __restrict__ a, const double2* __restrict__ b, long n, KernelParams kp,
                                int mode, double* out) {
@@ -712,6 +753,15 @@ afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, c
     AFMM_CUDA(cudaMemcpy(db, xy2, sizeof(double2) * n, cudaMemcpyHostToDevice));
     dispatch_kernel<PairsRun>(kernel_id, da, db, (long)n, KernelParams{kernel_id, a, param}, mode, dout);
     AFMM_CUDA(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
+  });
+}
+
+afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops) {
+  if (!fp64_tflops || !fp32_tflops) return AFMM_BAD_ARG;
+  return guard(nullptr, [&] {
+    check_device();
+    *fp64_tflops = fma_peak_tflops<double>();
+    *fp32_tflops = fma_peak_tflops<float>();
   });
 }
 

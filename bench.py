@@ -1,10 +1,13 @@
 #!/usr/bin/env python
 """AFMM2D matvec benchmark on B200.
 
-One step = one matvec y = K q over the workload's N points (one right-hand
-side), with the assembled operators resident in HBM.  The default workload is
-the N = 4,194,304 Gaussian-mixture problem (16 components, sigma 0.02,
-kernel 1/r, M = 64, TOL_POW = 6); inputs are seeded synthetic data.
+One step = one batched matvec Y = K Q over the workload's N points with
+--nrhs right-hand sides (default 16) in the mixed-precision path, with the
+assembled operators resident in HBM; value = N * nrhs / step time.  The FP64
+plain path and the single-RHS mixed path are timed beside it.  The default
+workload is the N = 4,194,304 Gaussian-mixture problem (16 components,
+sigma 0.02, kernel 1/r, M = 64, TOL_POW = 6); inputs are seeded synthetic
+data.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -30,7 +33,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-METRIC = "points*RHS/s per matvec at N=4M (mixture, 1/r, TOL 6)"
+METRIC = "points*RHS/s per matvec at N=4M (mixture, 1/r, TOL 6), mixed batched vs FP64 GPU"
 UNIT = "points*RHS/s"
 CPU_SAMPLE_N = 65536
 
@@ -43,6 +46,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="mixture4m")
     ap.add_argument("--N", type=int, default=None, help="override N (same distribution)")
+    ap.add_argument("--nrhs", type=int, default=16, help="right-hand sides of the batched (headline) path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
     return ap.parse_args()
@@ -152,122 +156,147 @@ def run_ours(args):
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    R = args.nrhs
     pts, q, p = workloads.make(args.workload, N=args.N)
     N = len(pts)
+    Q = np.random.Generator(np.random.PCG64(p["seed"] + 1)).standard_normal((N, R))
+    Q[:, 0] = q
     t0 = time.perf_counter()
     a = A.AFMM(N, p["M"], p["tol"], pts, kernel=p["kernel"])
     a.assemble()
     setup_s = time.perf_counter() - t0
-    st = a.setup_times()
     counts = a.counts()
+    dev = f"cuda:{local}"
     stream = torch.cuda.ExternalStream(a.stream())
-    dq = torch.from_numpy(q).to(f"cuda:{local}")
-    dy = torch.empty_like(dq)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")  # > 126 MB L2
+    dQ = torch.from_numpy(np.asfortranarray(Q).T.copy()).to(dev)  # row c = column c (column-major N x R)
+    dY = torch.empty_like(dQ)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    def timed(prec, steps, warm):
+    paths = {"fp64": ("fp64", 1), "mixed": ("mixed", 1), "batched": ("mixed", R)}
+
+    def call(name):
+        prec, nr = paths[name]
+        a.matvec_device(dQ.data_ptr(), dY.data_ptr(), nr, N, prec)
+
+    def timed(name, steps, warm):
         for _ in range(warm):
-            a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
+            call(name)
         ms = []
         for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
+            call(name)
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
-        return ms
+        return float(np.mean(ms))
 
     if args.profile_once:
-        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "fp64")
+        for name in paths:
+            call(name)
         torch.cuda.synchronize()
         return
-    precs = ["fp64"]
-    try:
-        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "mixed")
-        precs.append("mixed")
-    except A.AFMMError:
-        pass
-    head = precs[-1]
-    # per-stage device times (separate, untimed pass)
+    # per-stage device times (separate, untimed passes)
     a.set_profiling(True)
     stages = {}
-    for prec in precs:
-        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, prec)
-        stages[prec] = a.stage_times()
+    for name in paths:
+        call(name)
+        stages[name] = a.stage_times()
     a.set_profiling(False)
-    launches0 = a.launch_count()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     clk = ClockSampler(local)
     clk.start()
-    ms = {prec: timed(prec, args.steps, args.warmup) for prec in precs}
+    t_dev = {}
+    launches = {}
+    for name in paths:
+        l0 = a.launch_count()
+        t_dev[name] = timed(name, args.steps, args.warmup)
+        launches[name] = (a.launch_count() - l0) // (args.steps + args.warmup)
     torch.cuda.synchronize()
     clocks = clk.stop()
-    launches = (a.launch_count() - launches0) // max(1, len(precs) * (args.steps + args.warmup))
-    y64 = np.empty(N)
-    a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "fp64")
-    y64[:] = dy.cpu().numpy()
+    # accuracy: the batched and single-RHS mixed paths against the FP64 path
+    y64 = np.empty((N, R))
+    for c in range(R):
+        a.matvec_device(dQ[c].data_ptr(), dY[c].data_ptr(), 1, N, "fp64")
+    y64[:] = dY.cpu().numpy().T
     err_dense = a.evaluateError(nsample=16, seed=1234)
-    err_mixed = None
-    if "mixed" in precs:
-        a.matvec_device(dq.data_ptr(), dy.data_ptr(), 1, N, "mixed")
-        ym = dy.cpu().numpy()
-        err_mixed = float(np.linalg.norm(ym - y64) / np.linalg.norm(y64))
-    # end to end through the C ABI with pinned host buffers
-    hq = torch.from_numpy(q).pin_memory()
-    hy = torch.empty(N, dtype=torch.float64).pin_memory()
+    call("batched")
+    yb = dY.cpu().numpy().T
+    err_batched = float(np.max([np.linalg.norm(yb[:, c] - y64[:, c]) / np.linalg.norm(y64[:, c]) for c in range(R)]))
+    call("mixed")
+    err_mixed = float(np.linalg.norm(dY[0].cpu().numpy() - y64[:, 0]) / np.linalg.norm(y64[:, 0]))
+    # end to end through the C ABI with pinned host buffers (the headline workload)
+    hQ = torch.from_numpy(np.asfortranarray(Q).T.copy()).pin_memory()
+    hY = torch.empty_like(hQ).pin_memory()
     for _ in range(args.warmup):
-        a.matvec_host_ptr(hq.data_ptr(), hy.data_ptr(), 1, N, head)
+        a.matvec_host_ptr(hQ.data_ptr(), hY.data_ptr(), R, N, "mixed")
     e2e = []
     for _ in range(args.steps):
         t1 = time.perf_counter()
-        a.matvec_host_ptr(hq.data_ptr(), hy.data_ptr(), 1, N, head)
+        a.matvec_host_ptr(hQ.data_ptr(), hY.data_ptr(), R, N, "mixed")
         e2e.append(time.perf_counter() - t1)
-    t_dev = {prec: float(np.mean(v)) for prec, v in ms.items()}
     t_e2e = float(np.mean(e2e))
     if dist:
-        for prec in precs:
-            t = torch.tensor([t_dev[prec]], device=f"cuda:{local}")
+        for name in paths:
+            t = torch.tensor([t_dev[name]], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_dev[prec] = float(t.item())
-        t = torch.tensor([t_e2e], device=f"cuda:{local}")
+            t_dev[name] = float(t.item())
+        t = torch.tensor([t_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = float(t.item())
-    value = world * N / (t_dev[head] * 1e-3)
+    value = world * N * R / (t_dev["batched"] * 1e-3)
     hbm, bf16, peak_kind = load_peaks()
-    # roofline of the dominant stage of the headline path
-    sd = stages[head]
-    dom = max((k for k in sd if k not in ("end", "h2d", "d2h")), key=lambda k: sd[k])
-    w = 8 if head == "fp64" else 4
+    fp64_peak, fp32_peak = A.measure_fma_peaks()
+    # roofline of the dominant kernel of the headline (batched) path
+    sb = stages["batched"]
+    dom = max((k for k in sb if k not in ("end", "h2d", "d2h")), key=lambda k: sb[k])
     if dom == "m2l":
-        byts = counts["m2l_entries"] * w + 2 * counts["sum_rank"] * w
-        achieved = byts / (sd[dom] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": "m2l_apply", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
-                "algorithmic_bytes": byts, "ms": sd[dom]}
+        flops = 2.0 * R * counts["m2l_entries"]
+        roof = {"bound": "fp64", "kernel": "k_m2l_b (M2L on the fly, FP64)", "unit": "TFLOP/s",
+                "achieved": flops / (sb[dom] * 1e-3) / 1e12, "peak": fp64_peak,
+                "peak_kind": "measured live (register-only FP64 FMA loop)", "traffic": None,
+                "algorithmic_flops": flops, "flop_definition": "2*nrhs FP64 FMA flops per M2L entry",
+                "ms": sb[dom]}
+    elif dom == "p2p":
+        flops = 2.0 * R * counts["near_evals"]
+        roof = {"bound": "fp32", "kernel": "k_p2p_b (near field, FP32)", "unit": "TFLOP/s",
+                "achieved": flops / (sb[dom] * 1e-3) / 1e12, "peak": fp32_peak,
+                "peak_kind": "measured live (register-only FP32 FMA loop)", "traffic": None,
+                "algorithmic_flops": flops, "flop_definition": "2*nrhs FP32 FMA flops per near-field pair",
+                "ms": sb[dom]}
     else:
-        evals = counts["near_evals"]
-        roof = {"bound": "compute", "kernel": dom, "achieved": evals / (sd[dom] * 1e-3) / 1e9,
-                "unit": "G kernel evals/s", "peak": None, "frac": None, "traffic": None,
-                "algorithmic_evals": evals, "ms": sd[dom]}
+        byts = counts["l2p_entries"] * 8 * 2
+        roof = {"bound": "hbm", "kernel": dom, "unit": "GB/s", "achieved": byts / (sb[dom] * 1e-3) / 1e9,
+                "peak": hbm, "peak_kind": peak_kind, "traffic": None, "ms": sb[dom]}
+    roof["frac"] = roof["achieved"] / roof["peak"] if roof.get("peak") else None
+    # the FP64 path's stored M2L is HBM-bound
+    s64 = stages["fp64"]
+    m2l_bytes = counts["m2l_entries"] * 8
+    roof64 = {"bound": "hbm", "kernel": "k_m2l_apply (stored FP64 M2L)", "unit": "GB/s",
+              "achieved": m2l_bytes / (s64["m2l"] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
+              "algorithmic_bytes": m2l_bytes, "ms": s64["m2l"]}
+    roof64["frac"] = roof64["achieved"] / hbm
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": t_dev[head], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if head == "fp64" else "f32+f64",
-            "data": "synthetic (seeded)",
+            "warmup": args.warmup, "ms_per_step": t_dev["batched"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "N": N, "kernel": p["kernel"], "M": p["M"], "TOL_POW": p["tol"],
-                       "nrhs": 1, "precision": head, "l2": "flushed (256 MB write) before every timed step",
+                       "nrhs": R, "precision": "mixed, batched", "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"replicas x{world}"},
-            "fp64_points_per_s": world * N / (t_dev["fp64"] * 1e-3), "fp64_ms": t_dev["fp64"],
-            "mixed_ms": t_dev.get("mixed"), "rel_err_mixed_vs_fp64": err_mixed,
+            "paths": {name: {"ms_per_step": t_dev[name], "nrhs": paths[name][1],
+                             "points_rhs_per_s": world * N * paths[name][1] / (t_dev[name] * 1e-3),
+                             "gpu_launches": launches[name]} for name in paths},
+            "speedup_batched_vs_fp64": (N * R / t_dev["batched"]) / (N / t_dev["fp64"]),
+            "rel_err_batched_vs_fp64_max_col": err_batched, "rel_err_mixed_vs_fp64": err_mixed,
             "rel_err_fp64_vs_dense_16_leaves": err_dense,
-            "setup_s": setup_s, "setup": st, "stages_ms": stages, "counts": counts,
-            "roofline": roof, "clocks": clocks, "gpu_launches": int(launches),
-            "e2e": {"value": world * N / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N,
-                    "d2h_bytes_per_step": 8 * N, "ms_per_step": t_e2e * 1e3}}
+            "setup_s": setup_s, "setup": a.setup_times(), "stages_ms": stages, "counts": counts,
+            "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
+            "clocks": clocks, "gpu_launches": int(launches["batched"]),
+            "e2e": {"value": world * N * R / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N * R,
+                    "d2h_bytes_per_step": 8 * N * R, "ms_per_step": t_e2e * 1e3, "nrhs": R}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_reference(args.workload, CPU_SAMPLE_N, 5, 1)
         if cb:

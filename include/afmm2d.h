@@ -145,6 +145,11 @@ afmm_status afmm_get_stream(afmm_handle* h, void** stream);
 afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, const double* xy1, const double* xy2,
                              double* out, int mode);
 
+/* Measures this device's FP64 and FP32 fused-multiply-add throughput (TFLOP/s,
+ * 2 flops per FMA) with a register-only kernel of ~50 ms each: the roofline
+ * denominators of the compute-bound kernels.  Replaces no reference interface. */
+afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
+
 afmm_status afmm_destroy(afmm_handle* h);
 const char* afmm_status_string(afmm_status s);
 const char* afmm_last_error(afmm_handle* h);
