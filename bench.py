@@ -56,6 +56,17 @@ def rank_info():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(values, dist, device):
+    """Element-wise max of a list of floats over all ranks (the step time of a
+    replicas run is the slowest rank's)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 class ClockSampler:
     """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
 
@@ -240,14 +251,10 @@ def run_ours(args):
         a.matvec_host_ptr(hQ.data_ptr(), hY.data_ptr(), R, N, "mixed")
         e2e.append(time.perf_counter() - t1)
     t_e2e = float(np.mean(e2e))
-    if dist:
-        for name in paths:
-            t = torch.tensor([t_dev[name]], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            t_dev[name] = float(t.item())
-        t = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    names = list(paths)
+    red = max_over_ranks([t_dev[n] for n in names] + [t_e2e], dist, dev)
+    t_dev = dict(zip(names, red[:-1]))
+    t_e2e = red[-1]
     value = world * N * R / (t_dev["batched"] * 1e-3)
     hbm, bf16, peak_kind = load_peaks()
     fp64_peak, fp32_peak = A.measure_fma_peaks()
