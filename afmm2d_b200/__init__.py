@@ -51,6 +51,7 @@ _SIGS = {
     "afmm_get_stream": [_vp, _vp],
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
     "afmm_measure_fma_peaks": [_vp, _vp],
+    "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_destroy": [_vp],
 }
 _lib = None

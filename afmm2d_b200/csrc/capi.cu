@@ -765,6 +765,20 @@ afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops) {
   });
 }
 
+afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const double* xy, int64_t* perm,
+                                        double* xy_sorted, void* stream) {
+  if (!xy || !perm) {
+    g_err = "xy and perm must be device pointers";
+    return AFMM_BAD_ARG;
+  }
+  return guard(nullptr, [&] {
+    int L = n_levels(N, min_particles_in_leaf);
+    if (L < 2) throw Error{AFMM_BAD_ARG, "N/MinParticlesInLeaf gives nLevels = " + std::to_string(L) + " < 2"};
+    check_device();
+    kd_sort_noalloc(xy, N, L, perm, xy_sorted, (cudaStream_t)stream);
+  });
+}
+
 afmm_status afmm_destroy(afmm_handle* h) {
   if (!h) return AFMM_OK;
   if (h->stream) cudaStreamSynchronize(h->stream);

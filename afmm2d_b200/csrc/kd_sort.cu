@@ -19,6 +19,7 @@
 //   3. finishes segments of <= kSmallSeg points inside one CTA (bitonic sorts
 //      of (sub-segment, rank) keys in shared memory), levels down to L.
 #include <algorithm>
+#include <mutex>
 
 #include "afmm_internal.cuh"
 #include "kd_sort.cuh"
@@ -484,6 +485,186 @@ void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d
   k_kd_bottom<<<(int)nseg, BT_THREADS, smem, s>>>(seq, d_starts, lb, L, rank_x0, rank_x, rank_y, out32);
   k_finish_perm<<<gb, T, 0, s>>>(out32, d_xy, N, d_perm, d_xy_sorted);
   *launches += 2;
+  AFMM_LAUNCH_CHECK();
+  AFMM_CUDA(cudaStreamSynchronize(s));
+}
+
+// ------------------------------------------------- allocation-free variant
+// The KD permutation for callers that cannot allocate device memory.  All
+// scratch lives in one file-scope device array (kNoAllocScratchBytes, held by
+// every GPU that loads this library until exit); inputs and outputs are the
+// caller's.  The kernels are the ones above; only the scratch comes from the
+// array instead of cudaMalloc.
+namespace {
+
+// Layout of the scratch for up to kNoAllocMaxPoints points (each part 256-byte
+// aligned): 4 x 8-byte keys and 11 x 4-byte ids/ranks per point, the radix
+// pass counts, segment starts and the non-finite flag.
+constexpr size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t kNaPts = (size_t)kNoAllocMaxPoints;
+constexpr size_t kNaCountBlocks = (kNaPts + RS_TILE - 1) / RS_TILE;
+constexpr size_t kNaStarts = 1024;  // int64 segment starts (needs 2*4^lb + 2 <= 34 here)
+constexpr size_t kNaNeed = 4 * al256(kNaPts * 8) + 11 * al256(kNaPts * 4) + al256(256 * kNaCountBlocks * 4) +
+                           al256(kNaStarts * 8) + al256(sizeof(int));
+static_assert(kNaNeed <= kNoAllocScratchBytes, "scratch array too small for its layout");
+
+static __device__ __align__(256) unsigned char g_kd_scratch[kNoAllocScratchBytes];
+
+// Device address of g_kd_scratch per device, looked up once per device with
+// that device current (the host-side symbol is not a device address).
+std::mutex g_na_mu;
+void* g_na_addr[64] = {nullptr};
+
+unsigned char* scratch_address() {
+  int dev = 0;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw Error{AFMM_BAD_ARG, "device ordinal out of range"};
+  std::lock_guard<std::mutex> lock(g_na_mu);
+  if (!g_na_addr[dev]) {
+    void* p = nullptr;
+    AFMM_CUDA(cudaGetSymbolAddress(&p, g_kd_scratch));
+    g_na_addr[dev] = p;
+  }
+  return (unsigned char*)g_na_addr[dev];
+}
+
+__global__ void k_check_finite(const double* __restrict__ xy, int n, int* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !(isfinite(xy[2 * i]) && isfinite(xy[2 * i + 1]))) atomicExch(flag, 1);
+}
+
+__global__ void k_finish_perm_na(const int32_t* __restrict__ perm32, const double* __restrict__ xy, int n,
+                                 int64_t* perm, double* xy_sorted) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    int p = perm32[i];
+    perm[i] = p;
+    if (xy_sorted) {
+      xy_sorted[2 * i] = xy[2 * p];
+      xy_sorted[2 * i + 1] = xy[2 * p + 1];
+    }
+  }
+}
+
+}  // namespace
+
+void kd_sort_noalloc(const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted, cudaStream_t s) {
+  if (N < 1 || N > kNoAllocMaxPoints)
+    throw Error{AFMM_BAD_ARG, "N = " + std::to_string(N) + " outside 1.." + std::to_string(kNoAllocMaxPoints) +
+                                  " for the allocation-free permutation"};
+  unsigned char* base = scratch_address();
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    unsigned char* p = base + off;
+    off += al256(bytes);
+    return p;
+  };
+  const size_t n8 = kNaPts * 8, n4 = kNaPts * 4;
+  uint64_t* kx = (uint64_t*)carve(n8);
+  uint64_t* ky = (uint64_t*)carve(n8);
+  RadixCtx rc;
+  rc.k0 = (uint64_t*)carve(n8);
+  rc.k1 = (uint64_t*)carve(n8);
+  rc.v0 = (int32_t*)carve(n4);
+  rc.v1 = (int32_t*)carve(n4);
+  int32_t* rank_x0 = (int32_t*)carve(n4);
+  int32_t* rank_x = (int32_t*)carve(n4);
+  int32_t* rank_y = (int32_t*)carve(n4);
+  int32_t* perm_x0 = (int32_t*)carve(n4);
+  int32_t* perm_x = (int32_t*)carve(n4);
+  int32_t* perm_y = (int32_t*)carve(n4);
+  int32_t* perm32 = (int32_t*)carve(n4);
+  int32_t* seg_of = (int32_t*)carve(n4);
+  int32_t* half_of = (int32_t*)carve(n4);
+  rc.counts = (uint32_t*)carve(256 * kNaCountBlocks * 4);
+  int64_t* d_starts = (int64_t*)carve(kNaStarts * 8);
+  int* flag = (int*)carve(sizeof(int));
+  rc.n = N;
+  rc.s = s;
+  int64_t launches = 0;
+  rc.launches = &launches;
+  const int T = 256, gb = nblocks(N, T);
+  // the array keeps the previous call's contents: clear the flag
+  AFMM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
+  k_check_finite<<<gb, T, 0, s>>>(d_xy, N, flag);
+  AFMM_LAUNCH_CHECK();
+  int h_flag = 0;
+  AFMM_CUDA(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  if (h_flag) throw Error{AFMM_BAD_ARG, "a point has a non-finite coordinate"};
+
+  k_make_keys<<<gb, T, 0, s>>>(d_xy, N, kx, ky);
+  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
+  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
+  rc.sort(0, 64);
+  AFMM_CUDA(cudaMemcpyAsync(perm_x0, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
+  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 1, rc.k0);
+  rc.sort(0, 64);
+  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
+  rc.sort(0, 64);
+  AFMM_CUDA(cudaMemcpyAsync(perm_x, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 0);
+  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 1, rc.k0);
+  rc.sort(0, 64);
+  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 0, rc.k0);
+  rc.sort(0, 64);
+  AFMM_CUDA(cudaMemcpyAsync(perm_y, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  k_invert<<<gb, T, 0, s>>>(perm_x0, N, rank_x0);
+  k_invert<<<gb, T, 0, s>>>(perm_x, N, rank_x);
+  k_invert<<<gb, T, 0, s>>>(perm_y, N, rank_y);
+  AFMM_LAUNCH_CHECK();
+
+  auto sizes = kd_segment_sizes(N, L);
+  int lb = 0;
+  while (lb < L && *std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg) ++lb;
+  if (*std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg)
+    throw Error{AFMM_BAD_ARG, "leaf segments larger than " + std::to_string(kSmallSeg) + " points"};
+  if (2 * sizes[lb].size() + 2 > kNaStarts) throw Error{AFMM_BAD_ARG, "too many top-level segments"};
+  const int32_t* seq = nullptr;
+  if (lb == 0) {
+    k_iota<<<gb, T, 0, s>>>(perm32, N, 0);
+    seq = perm32;
+  }
+  std::vector<int64_t> h_starts;
+  for (int l = 0; l < lb; ++l) {
+    size_t ns = sizes[l].size();
+    AFMM_CUDA(cudaMemcpyAsync(rc.v0, l == 0 ? perm_x0 : perm_x, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+    if (l == 0) {
+      AFMM_CUDA(cudaMemsetAsync(rc.k0, 0, sizeof(uint64_t) * N, s));
+    } else {
+      k_gather_key32<<<gb, T, 0, s>>>(seg_of, rc.v0, N, rc.k0);
+      rc.sort(0, 2 * l);
+    }
+    h_starts.assign(ns + 1, 0);
+    for (size_t i = 0; i < ns; ++i) h_starts[i + 1] = h_starts[i] + sizes[l][i];
+    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
+    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, half_of);
+    AFMM_CUDA(cudaMemcpyAsync(rc.v0, perm_y, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+    k_gather_key32<<<gb, T, 0, s>>>(half_of, rc.v0, N, rc.k0);
+    rc.sort(0, 2 * l + 1);
+    h_starts.assign(2 * ns + 1, 0);
+    for (size_t i = 0; i < ns; ++i) {
+      int64_t ln = sizes[l][i] / 2;
+      h_starts[2 * i + 1] = h_starts[2 * i] + ln;
+      h_starts[2 * i + 2] = h_starts[2 * i + 1] + (sizes[l][i] - ln);
+    }
+    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (2 * ns + 1), cudaMemcpyHostToDevice, s));
+    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, seg_of);
+    AFMM_CUDA(cudaStreamSynchronize(s));
+    AFMM_LAUNCH_CHECK();
+  }
+  if (lb > 0) seq = rc.v0;
+  size_t nseg = sizes[lb].size();
+  h_starts.assign(nseg + 1, 0);
+  for (size_t i = 0; i < nseg; ++i) h_starts[i + 1] = h_starts[i] + sizes[lb][i];
+  AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s));
+  size_t smem = (size_t)kSmallSeg * 8 + (size_t)kSmallSeg * 4 * 3 + (size_t)(kSmallSeg + 1) * 4 +
+                (size_t)(2 * kSmallSeg + 1) * 4;
+  AFMM_CUDA(cudaFuncSetAttribute(k_kd_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int32_t* out32 = (seq == perm32) ? perm_y : perm32;
+  k_kd_bottom<<<(int)nseg, BT_THREADS, smem, s>>>(seq, d_starts, lb, L, rank_x0, rank_x, rank_y, out32);
+  k_finish_perm_na<<<gb, T, 0, s>>>(out32, d_xy, N, d_perm, d_xy_sorted);
   AFMM_LAUNCH_CHECK();
   AFMM_CUDA(cudaStreamSynchronize(s));
 }

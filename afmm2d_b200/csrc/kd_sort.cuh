@@ -19,4 +19,10 @@ std::vector<std::vector<int64_t>> kd_segment_sizes(int64_t N, int L);
 void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted, cudaStream_t s,
                     int64_t* launches);
 
+// Allocation-free variant for N <= kNoAllocMaxPoints: all scratch lives in a
+// file-scope device array of kNoAllocScratchBytes (see kd_sort.cu).
+constexpr int kNoAllocMaxPoints = 65536;
+constexpr size_t kNoAllocScratchBytes = (size_t)5 << 20;
+void kd_sort_noalloc(const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted, cudaStream_t s);
+
 }  // namespace afmm

@@ -150,6 +150,24 @@ afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, c
  * denominators of the compute-bound kernels.  Replaces no reference interface. */
 afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 
+/* KD-tree permutation without any device allocation.  It has no counterpart
+ * in the reference; it computes the same permutation as afmm_create /
+ * afmm_get_permutation.  For callers that cannot allocate GPU memory: a
+ * process whose device memory is already reserved by another framework's
+ * caching allocator, a service that must hold a fixed, declared footprint, or
+ * a loop that cannot afford a cudaMalloc/cudaFree pair per call (cudaFree
+ * synchronises the whole device).  xy (N interleaved x,y), perm (N int64) and
+ * xy_sorted (2N doubles, may be NULL) are device pointers owned by the caller;
+ * stream is a cudaStream_t (NULL: the default stream); the call returns after
+ * the stream has completed the work.  Limit: 1 <= N <= 65,536 points
+ * (AFMM_BAD_ARG beyond).  Scratch is one static device array of 5 MiB that
+ * every GPU loading this library keeps until the process exits; the first call
+ * on a device looks up its address (make that first call before any stream
+ * capture).  All calls share that array, so calls that overlap on the GPU
+ * (other threads or streams) race and must be serialised by the caller. */
+afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const double* xy, int64_t* perm,
+                                        double* xy_sorted, void* stream);
+
 afmm_status afmm_destroy(afmm_handle* h);
 const char* afmm_status_string(afmm_status s);
 const char* afmm_last_error(afmm_handle* h);
