@@ -8,11 +8,13 @@
 //  * M2M / L2L: FP64 L2P (row-major / column-major), one thread per output
 //    row with RC FP64 accumulators.
 //  * M2L: entries evaluated on the fly in FP64 from the skeleton coordinates
-//    (as in the single-RHS mixed path), RC FP64 multiply-adds per entry.
+//    (as in the single-RHS mixed path) and multiplied with the RC-column
+//    charge blocks on the FP64 tensor cores (8 rows x 4 sources tiles).
 //  * Near field: entries in FP32 from leaf-relative coordinates with the FP64
-//    fallback for close pairs (as in the single-RHS mixed path), RC FP32
-//    multiply-adds per entry, FP32 partial sums per source leaf accumulated
-//    in FP64.
+//    fallback for close pairs (as in the single-RHS mixed path), multiplied
+//    on the TF32 tensor cores in a three-term high/low split (16 targets x 8
+//    sources tiles), tile sums per source leaf accumulated in FP64.
+// With RC = 4 the same products run on the FMA pipes.
 #include <algorithm>
 
 #include "mixed.cuh"
@@ -21,24 +23,29 @@ namespace afmm {
 
 namespace {
 
+// Gather: thread (j, c) reads q[c][j] (original order; a block's consecutive j
+// share sectors of every column) and writes the sorted point-major block
+// qs[iperm[j]][c] (16 lanes fill one 128-byte row).
 template <int RC>
-__global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int64_t* __restrict__ perm,
+__global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int32_t* __restrict__ iperm,
                            int N, double* qs, float* qs32) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)N * RC) return;
-  const int i = (int)(t / RC), c = (int)(t % RC);
-  const double v = c < ncols ? q[(long)c * ldq + perm[i]] : 0.0;
-  qs[t] = v;
-  qs32[t] = (float)v;
+  const int j = (int)(t / RC), c = (int)(t % RC);
+  const double v = c < ncols ? q[(long)c * ldq + j] : 0.0;
+  const long d = (long)iperm[j] * RC + c;
+  qs[d] = v;
+  qs32[d] = (float)v;
 }
 
+// Scatter: thread (j, c) reads the sorted row of j and writes y[c][j].
 template <int RC>
-__global__ void k_scatter_b(const double* __restrict__ ys, const int64_t* __restrict__ perm, int N, int ncols,
+__global__ void k_scatter_b(const double* __restrict__ ys, const int32_t* __restrict__ iperm, int N, int ncols,
                             double* y, int64_t ldy) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)N * RC) return;
-  const int i = (int)(t / RC), c = (int)(t % RC);
-  if (c < ncols) y[(long)c * ldy + perm[i]] = ys[t];
+  const int j = (int)(t / RC), c = (int)(t % RC);
+  if (c < ncols) y[(long)c * ldy + j] = ys[(long)iperm[j] * RC + c];
 }
 
 template <int RC>
@@ -253,6 +260,225 @@ __global__ void k_p2p_b(NearView nv, KernelParams kp, const float* __restrict__ 
   store_vec<RC>(out, cur);
 }
 
+// ------------------------------------------------------- tensor-core tiles
+// FP64 MMA m8n8k4 (D = A B + C; A 8x4 row-major, B 4x8 column-major): lane l
+// holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4) .. 2(l%4)+1].
+__device__ __forceinline__ void mma_f64_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+// TF32 MMA m16n8k8: lane l = 4g + t holds A[g][t], A[g+8][t], A[g][t+4],
+// A[g+8][t+4]; B[t][g], B[t+4][g]; D[g][2t], D[g][2t+1], D[g+8][2t], D[g+8][2t+1].
+__device__ __forceinline__ void mma_tf32_16x8x8(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// x = hi + lo with both parts TF32 (hi: 11 significant bits, lo: the next 11).
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+
+// M2L on the fly with FP64 tensor-core tiles: one warp per row group (up to 8
+// skeleton rows of one box).  For every interaction-list box and every 4 of
+// its skeleton points, each lane evaluates the one FP64 entry it holds in the
+// A fragment (row l/4, source l%4: no entry is evaluated twice) and the warp
+// multiplies the 8x4 tile with the 4 x RC block of outgoing charges.
+template <class K, int RC>
+__global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, const double* const* __restrict__ qhat_lv,
+                                                 double* const* __restrict__ yhat_lv) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ls.grp0[ls.nlev]) return;  // whole warps only
+  int j = 0;
+  while (j + 1 < ls.nlev && gw >= ls.grp0[j + 1]) ++j;
+  const LevelView& v = ls.lv[j];
+  const double* qh = qhat_lv[j];
+  const long g = gw - ls.grp0[j];
+  const int b = v.grp_box[g];
+  const int r0 = v.grp_row[g];
+  const int nv = min(8, v.skel_off[b] + v.rank[b] - r0);
+  const int trow = lane >> 2, tsrc = lane & 3;
+  const bool vrow = trow < nv;
+  const double2 xi = vrow ? v.skel_xy[r0 + trow] : make_double2(0.0, 0.0);
+  double c[RC / 8][2];
+#pragma unroll
+  for (int t = 0; t < RC / 8; ++t) c[t][0] = c[t][1] = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int cb = v.il[(long)b * 40 + s];
+    if (cb < 0) continue;
+    const int rc = v.rank[cb];
+    const int sc = v.skel_off[cb];
+    for (int cc0 = 0; cc0 < rc; cc0 += 4) {
+      const int cs = cc0 + tsrc;
+      const bool vs = cs < rc;
+      double a = 0.0;
+      if (vrow && vs) {
+        const double2 p = v.skel_xy[sc + cs];
+        const double dx = xi.x - p.x, dy = xi.y - p.y;
+        a = K::eval(dx * dx + dy * dy, kp);
+      }
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) {
+        const double bq = vs ? qh[(long)(sc + cs) * RC + t * 8 + trow] : 0.0;
+        mma_f64_8x8x4(c[t][0], c[t][1], a, bq);
+      }
+    }
+  }
+  if (vrow) {
+    double* out = yhat_lv[j] + (long)(r0 + trow) * RC;
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) {
+      out[t * 8 + 2 * tsrc] = c[t][0];
+      out[t * 8 + 2 * tsrc + 1] = c[t][1];
+    }
+  }
+}
+
+// Near field with TF32 tensor-core tiles in a three-term split
+// (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy): one CTA per leaf, all
+// source leaves staged in shared memory (coordinates relative to their leaf
+// anchor, charges pre-split into TF32 high / low parts).  Each warp takes
+// tiles of 16 targets; for every 8 sources each lane evaluates the four FP32
+// entries of its A fragment (FP64 fallback for close pairs), and the 16 x 8
+// tile is multiplied with the 8 x RC charge block.  Tile sums per source leaf
+// are accumulated in FP64.
+template <class K, int RC>
+__global__ void k_p2p_mma(NearView nv, KernelParams kp, const float* __restrict__ qs32, double* __restrict__ ys) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
+  __shared__ float s_dx[9], s_dy[9], s_thr[9];
+  const long b = blockIdx.x;
+  const int n = nv.leaf_cnt[b];
+  const int s0 = nv.leaf_start[b];
+  const float a32 = (float)kp.a, p32 = (float)kp.param;
+  if (threadIdx.x == 0) {
+    const double2 ab = nv.anchor[b];
+    const float sb = nv.span[b];
+    int m = 0, off = 0;
+    for (int slot = 0; slot < 9; ++slot) {
+      const long cbx = slot < 8 ? nv.nbr[b * 8 + slot] : b;
+      if (cbx < 0) continue;
+      const double2 ac = nv.anchor[cbx];
+      s_src[m] = nv.leaf_start[cbx];
+      s_cnt[m] = nv.leaf_cnt[cbx];
+      s_off[m] = off;
+      s_dx[m] = (float)(ab.x - ac.x);
+      s_dy[m] = (float)(ab.y - ac.y);
+      s_thr[m] = fallback_r2_b<K>(sb, nv.span[cbx]);
+      off += nv.leaf_cnt[cbx];
+      ++m;
+    }
+    s_off[m] = off;
+    s_ns = m;
+  }
+  __syncthreads();
+  const int ns = s_ns;
+  const int tot = s_off[ns];
+  uint32_t* qhi = (uint32_t*)smem;                // tot x RC
+  uint32_t* qlo = qhi + (size_t)9 * nv.nmax * RC;  // tot x RC
+  float2* sx = (float2*)(qlo + (size_t)9 * nv.nmax * RC);
+  for (int m = 0; m < ns; ++m) {
+    const int o = s_off[m], nc = s_cnt[m], src = s_src[m];
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) sx[o + t] = nv.rel[src + t];
+    for (int e = threadIdx.x; e < nc * RC; e += blockDim.x) {
+      uint32_t h, l;
+      split_tf32(qs32[(long)src * RC + e], h, l);
+      qhi[(long)o * RC + e] = h;
+      qlo[(long)o * RC + e] = l;
+    }
+  }
+  __syncthreads();
+  (void)tot;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int gq = lane >> 2, tq = lane & 3;
+  for (int tile = warp; tile * 16 < n; tile += nw) {
+    const int t0 = tile * 16 + gq, t1 = t0 + 8;
+    const bool v0 = t0 < n, v1 = t1 < n;
+    const float2 x0 = v0 ? nv.rel[s0 + t0] : make_float2(0.f, 0.f);
+    const float2 x1 = v1 ? nv.rel[s0 + t1] : make_float2(0.f, 0.f);
+    double acc[RC / 8][4];
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+    for (int m = 0; m < ns; ++m) {
+      const int o = s_off[m], nc = s_cnt[m], src = s_src[m];
+      const float thr = s_thr[m];
+      const float ox0 = x0.x + s_dx[m], oy0 = x0.y + s_dy[m], ox1 = x1.x + s_dx[m], oy1 = x1.y + s_dy[m];
+      float cf[RC / 8][4];
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) cf[t][0] = cf[t][1] = cf[t][2] = cf[t][3] = 0.0f;
+      for (int k0 = 0; k0 < nc; k0 += 8) {
+        const int sa = k0 + tq, sb2 = k0 + tq + 4;
+        const bool va = sa < nc, vb = sb2 < nc;
+        float kv[4];  // A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]
+        const bool vv[4] = {v0 && va, v1 && va, v0 && vb, v1 && vb};
+        const int tgt[4] = {t0, t1, t0, t1}, srs[4] = {sa, sa, sb2, sb2};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          kv[e] = 0.0f;
+          if (vv[e]) {
+            const float2 p = sx[o + srs[e]];
+            const float ox = (e & 1) ? ox1 : ox0, oy = (e & 1) ? oy1 : oy0;
+            const float dx = ox - p.x, dy = oy - p.y;
+            const float R2 = fmaf(dx, dx, dy * dy);
+            if (R2 < thr) {
+              const int pi = s0 + tgt[e], qi = src + srs[e];
+              if (pi == qi) {
+                kv[e] = (float)K::at_zero();
+              } else {
+                const double2 a = nv.pts[pi], c2 = nv.pts[qi];
+                kv[e] = (float)K::eval_exact(r2_exact(a.x, a.y, c2.x, c2.y), kp);
+              }
+            } else {
+              kv[e] = K::eval32(R2, a32, p32);
+            }
+          }
+        }
+        uint32_t ah[4], al[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) split_tf32(kv[e], ah[e], al[e]);
+#pragma unroll
+        for (int t = 0; t < RC / 8; ++t) {
+          const long ra = (long)(o + sa) * RC + t * 8 + gq, rb = (long)(o + sb2) * RC + t * 8 + gq;
+          const uint32_t bh0 = va ? qhi[ra] : 0u, bl0 = va ? qlo[ra] : 0u;
+          const uint32_t bh1 = vb ? qhi[rb] : 0u, bl1 = vb ? qlo[rb] : 0u;
+          mma_tf32_16x8x8(cf[t], ah, bh0, bh1);
+          mma_tf32_16x8x8(cf[t], ah, bl0, bl1);
+          mma_tf32_16x8x8(cf[t], al, bh0, bh1);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc[t][e] += (double)cf[t][e];
+    }
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) {
+      if (v0) {
+        double* out = ys + (long)(s0 + t0) * RC + t * 8 + 2 * tq;
+        out[0] += acc[t][0];
+        out[1] += acc[t][1];
+      }
+      if (v1) {
+        double* out = ys + (long)(s0 + t1) * RC + t * 8 + 2 * tq;
+        out[0] += acc[t][2];
+        out[1] += acc[t][3];
+      }
+    }
+  }
+}
+
 inline int nbk(long n, int t) { return (int)((n + t - 1) / t); }
 
 template <int RC>
@@ -261,18 +487,31 @@ struct Pass {
   struct M2l {
     static void run(const LevelSet& ls, const KernelParams& kp, const double* const* qh, double* const* yh,
                     cudaStream_t s) {
-      const long rows = ls.row0[ls.nlev];
-      k_m2l_b<K, RC><<<nbk(rows, 128), 128, 0, s>>>(ls, kp, qh, yh);
+      if (RC >= 8) {
+        const long warps = ls.grp0[ls.nlev];
+        k_m2l_mma<K, (RC >= 8 ? RC : 8)><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
+      } else {
+        const long rows = ls.row0[ls.nlev];
+        k_m2l_b<K, RC><<<nbk(rows, 128), 128, 0, s>>>(ls, kp, qh, yh);
+      }
       AFMM_LAUNCH_CHECK();
     }
   };
   template <class K>
   struct P2p {
     static void run(const NearView& nv, const KernelParams& kp, const float* qs32, double* ys, cudaStream_t s) {
-      const int T = (nv.nmax + 31) / 32 * 32;
-      size_t smem = (size_t)9 * nv.nmax * (sizeof(float) * RC + sizeof(float2));
-      allow_smem(k_p2p_b<K, RC>, smem);
-      k_p2p_b<K, RC><<<(int)nv.nleaf, T, smem, s>>>(nv, kp, qs32, ys);
+      constexpr int RM = RC >= 8 ? RC : 8;
+      const size_t smem_mma = (size_t)9 * nv.nmax * (2 * sizeof(uint32_t) * RM + sizeof(float2));
+      if (RC >= 8 && smem_mma <= 200 * 1024) {
+        const int warps = std::min(8, (nv.nmax + 15) / 16);
+        allow_smem(k_p2p_mma<K, RM>, smem_mma);
+        k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qs32, ys);
+      } else {
+        const int T = (nv.nmax + 31) / 32 * 32;
+        size_t smem = (size_t)9 * nv.nmax * (sizeof(float) * RC + sizeof(float2));
+        allow_smem(k_p2p_b<K, RC>, smem);
+        k_p2p_b<K, RC><<<(int)nv.nleaf, T, smem, s>>>(nv, kp, qs32, ys);
+      }
       AFMM_LAUNCH_CHECK();
     }
   };
@@ -281,7 +520,7 @@ struct Pass {
                   int64_t ldy, int ncols, cudaStream_t s, StageTimer* tm, int64_t* launches) {
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.perm, N, bs.qs, bs.qs32);
+    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
@@ -308,7 +547,7 @@ struct Pass {
     dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
-    k_scatter_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(bs.ys, p.perm, N, ncols, y, ldy);
+    k_scatter_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }

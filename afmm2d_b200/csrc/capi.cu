@@ -23,6 +23,7 @@ struct afmm_handle {
   DevArena arena;
   double2* d_pts = nullptr;
   int64_t* d_perm = nullptr;
+  int32_t* d_iperm = nullptr;  // original index -> sorted position
   std::vector<int32_t> h_counts, h_boxnum;          // DFS order
   std::vector<int32_t> h_leaf_start, h_leaf_cnt;    // quadtree order
   int32_t* d_leaf_start = nullptr;
@@ -211,6 +212,7 @@ void build_plan(afmm_handle* h) {
   p.L = h->L;
   p.kp = h->kp;
   p.perm = h->d_perm;
+  p.iperm = h->d_iperm;
   p.qs = h->d_qs;
   p.ys = h->d_ys;
   for (int j = 0; j <= h->L; ++j) {
@@ -233,14 +235,19 @@ void build_plan(afmm_handle* h) {
     v.yhat = d.yhat;
     v.skel_box = d.skel_box;
     v.node_box = d.node_box;
+    v.grp_box = d.grp_box;
+    v.grp_row = d.grp_row;
+    v.ngroups = d.ngroups;
     v.nrows = d.total_rank;
     v.nnodes = d.h_node_off.empty() ? 0 : d.h_node_off[d.nbox];
   }
   p.levels.nlev = 0;
   p.levels.row0[0] = 0;
+  p.levels.grp0[0] = 0;
   for (int j = 2; j <= h->L; ++j) {
     p.levels.lv[p.levels.nlev] = p.lv[j];
     p.levels.row0[p.levels.nlev + 1] = p.levels.row0[p.levels.nlev] + p.lv[j].nrows;
+    p.levels.grp0[p.levels.nlev + 1] = p.levels.grp0[p.levels.nlev] + p.lv[j].ngroups;
     ++p.levels.nlev;
   }
   for (int j = 0; j <= h->L; ++j) {
@@ -281,6 +288,9 @@ void do_create(afmm_handle* h, const double* loc, int layout) {
   h->d_perm = h->arena.alloc<int64_t>(N);
   h->d_pts = h->arena.alloc<double2>(N);
   kd_sort_device(d_xy, N, L, h->d_perm, (double*)h->d_pts, s, &h->launches);
+  h->d_iperm = h->arena.alloc<int32_t>(N);
+  invert_permutation(h->d_perm, N, h->d_iperm, s);
+  ++h->launches;
   h->arena.release(d_xy);
   // Leaf layout: DFS leaf d owns a contiguous sorted range; its quadtree box
   // number follows src/KDTree.cpp:211-223 (children 4p+0, 4p+3, 4p+1, 4p+2).
@@ -425,6 +435,21 @@ void do_assemble(afmm_handle* h) {
     fill_box_map(v.skel_off, v.nbox, v.skel_box, s);
     fill_box_map(v.node_off, v.nbox, v.node_box, s);
     h->launches += 2;
+    // row groups of at most 8 skeleton rows of one box (tensor-core M2L tiles)
+    std::vector<int32_t> gb, gr;
+    for (long b = 0; b < v.nbox; ++b)
+      for (int i = 0; i < v.h_rank[b]; i += 8) {
+        gb.push_back((int32_t)b);
+        gr.push_back(v.h_skel_off[b] + i);
+      }
+    v.ngroups = (long)gb.size();
+    v.grp_box = h->arena.alloc<int32_t>(gb.size());
+    v.grp_row = h->arena.alloc<int32_t>(gr.size());
+    if (!gb.empty()) {
+      AFMM_CUDA(cudaMemcpyAsync(v.grp_box, gb.data(), sizeof(int32_t) * gb.size(), cudaMemcpyHostToDevice, s));
+      AFMM_CUDA(cudaMemcpyAsync(v.grp_row, gr.data(), sizeof(int32_t) * gr.size(), cudaMemcpyHostToDevice, s));
+      AFMM_CUDA(cudaStreamSynchronize(s));
+    }
   }
   for (int j = 2; j <= L; ++j) {
     LevelDev& v = h->lv[j];

@@ -77,6 +77,16 @@ __global__ void k_fill_box_map(const int32_t* __restrict__ off, long nbox, int32
   for (int32_t t = off[b]; t < off[b + 1]; ++t) map[t] = (int32_t)b;
 }
 
+__global__ void k_invert_perm(const int64_t* __restrict__ perm, int n, int32_t* iperm) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) iperm[perm[i]] = i;
+}
+
+void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t s) {
+  k_invert_perm<<<(n + 255) / 256, 256, 0, s>>>(perm, n, iperm);
+  AFMM_LAUNCH_CHECK();
+}
+
 void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s) {
   k_fill_box_map<<<(int)((nbox + 255) / 256), 256, 0, s>>>(off, nbox, map);
   AFMM_LAUNCH_CHECK();

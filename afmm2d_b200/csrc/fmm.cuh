@@ -44,6 +44,9 @@ struct LevelView {
   double* yhat = nullptr;
   const int32_t* skel_box = nullptr;  // skeleton row -> box
   const int32_t* node_box = nullptr;  // node row -> box
+  const int32_t* grp_box = nullptr;   // row group (<= 8 rows of one box) -> box
+  const int32_t* grp_row = nullptr;   // row group -> first skeleton row
+  long ngroups = 0;
   long nrows = 0;                     // skeleton rows (sum of ranks)
   long nnodes = 0;                    // node rows (sum of node counts)
 };
@@ -54,6 +57,7 @@ struct LevelSet {
   int nlev = 0;
   LevelView lv[kMaxLevels];
   long row0[kMaxLevels + 1] = {0};
+  long grp0[kMaxLevels + 1] = {0};  // prefix of row-group counts
 };
 
 // Leaf-level data for the near field.
@@ -108,6 +112,7 @@ struct MatvecPlan {
   int N = 0, L = 0;
   KernelParams kp;
   const int64_t* perm = nullptr;
+  const int32_t* iperm = nullptr;  // original index -> sorted position
   double* qs = nullptr;  // sorted charges
   double* ys = nullptr;  // sorted potentials
   LevelView lv[kMaxLevels];
@@ -147,6 +152,8 @@ inline P2pShape p2p_shape(int nmax) {
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
 // map[off[b] + l] = b for l < off[b+1] - off[b]
 void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s);
+// iperm[perm[i]] = i
+void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
 void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
