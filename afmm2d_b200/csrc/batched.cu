@@ -26,16 +26,35 @@ namespace {
 // Gather: thread (j, c) reads q[c][j] (original order; a block's consecutive j
 // share sectors of every column) and writes the sorted point-major block
 // qs[iperm[j]][c] (16 lanes fill one 128-byte row).
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// x = hi + lo with both parts TF32 (hi: 11 significant bits, lo: the next 11).
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+  hi = to_tf32(x);
+  lo = to_tf32(x - __uint_as_float(hi));
+}
+
+// The sorted charges are also written as FP32 and as the TF32 high / low
+// parts the tensor-core near field multiplies with (split once per pass).
 template <int RC>
 __global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int32_t* __restrict__ iperm,
-                           int N, double* qs, float* qs32) {
+                           int N, double* qs, float* qs32, uint32_t* qhi, uint32_t* qlo) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)N * RC) return;
   const int j = (int)(t / RC), c = (int)(t % RC);
   const double v = c < ncols ? q[(long)c * ldq + j] : 0.0;
   const long d = (long)iperm[j] * RC + c;
   qs[d] = v;
-  qs32[d] = (float)v;
+  const float f = (float)v;
+  qs32[d] = f;
+  uint32_t h, l;
+  split_tf32(f, h, l);
+  qhi[d] = h;
+  qlo[d] = l;
 }
 
 // Scatter: thread (j, c) reads the sorted row of j and writes y[c][j].
@@ -278,18 +297,6 @@ __device__ __forceinline__ void mma_tf32_16x8x8(float (&c)[4], const uint32_t (&
       : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
 
-__device__ __forceinline__ uint32_t to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return r;
-}
-
-// x = hi + lo with both parts TF32 (hi: 11 significant bits, lo: the next 11).
-__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
-  hi = to_tf32(x);
-  lo = to_tf32(x - __uint_as_float(hi));
-}
-
 // M2L on the fly with FP64 tensor-core tiles: one warp per row group (up to 8
 // skeleton rows of one box).  For every interaction-list box and every 4 of
 // its skeleton points, each lane evaluates the one FP64 entry it holds in the
@@ -347,15 +354,17 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
 }
 
 // Near field with TF32 tensor-core tiles in a three-term split
-// (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy): one CTA per leaf, all
-// source leaves staged in shared memory (coordinates relative to their leaf
-// anchor, charges pre-split into TF32 high / low parts).  Each warp takes
+// (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy): one CTA per leaf, the
+// source leaves' coordinates (relative to their leaf anchor) staged in shared
+// memory, the charges' TF32 high / low parts read from L2 (split once per
+// pass by the gather).  Each warp takes
 // tiles of 16 targets; for every 8 sources each lane evaluates the four FP32
 // entries of its A fragment (FP64 fallback for close pairs), and the 16 x 8
 // tile is multiplied with the 8 x RC charge block.  Tile sums per source leaf
 // are accumulated in FP64.
 template <class K, int RC>
-__global__ void k_p2p_mma(NearView nv, KernelParams kp, const float* __restrict__ qs32, double* __restrict__ ys) {
+__global__ void k_p2p_mma(NearView nv, KernelParams kp, const uint32_t* __restrict__ qhi,
+                          const uint32_t* __restrict__ qlo, double* __restrict__ ys) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
@@ -385,22 +394,12 @@ __global__ void k_p2p_mma(NearView nv, KernelParams kp, const float* __restrict_
   }
   __syncthreads();
   const int ns = s_ns;
-  const int tot = s_off[ns];
-  uint32_t* qhi = (uint32_t*)smem;                // tot x RC
-  uint32_t* qlo = qhi + (size_t)9 * nv.nmax * RC;  // tot x RC
-  float2* sx = (float2*)(qlo + (size_t)9 * nv.nmax * RC);
+  float2* sx = (float2*)smem;
   for (int m = 0; m < ns; ++m) {
     const int o = s_off[m], nc = s_cnt[m], src = s_src[m];
     for (int t = threadIdx.x; t < nc; t += blockDim.x) sx[o + t] = nv.rel[src + t];
-    for (int e = threadIdx.x; e < nc * RC; e += blockDim.x) {
-      uint32_t h, l;
-      split_tf32(qs32[(long)src * RC + e], h, l);
-      qhi[(long)o * RC + e] = h;
-      qlo[(long)o * RC + e] = l;
-    }
   }
   __syncthreads();
-  (void)tot;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   for (int tile = warp; tile * 16 < n; tile += nw) {
@@ -450,7 +449,7 @@ __global__ void k_p2p_mma(NearView nv, KernelParams kp, const float* __restrict_
         for (int e = 0; e < 4; ++e) split_tf32(kv[e], ah[e], al[e]);
 #pragma unroll
         for (int t = 0; t < RC / 8; ++t) {
-          const long ra = (long)(o + sa) * RC + t * 8 + gq, rb = (long)(o + sb2) * RC + t * 8 + gq;
+          const long ra = (long)(src + sa) * RC + t * 8 + gq, rb = (long)(src + sb2) * RC + t * 8 + gq;
           const uint32_t bh0 = va ? qhi[ra] : 0u, bl0 = va ? qlo[ra] : 0u;
           const uint32_t bh1 = vb ? qhi[rb] : 0u, bl1 = vb ? qlo[rb] : 0u;
           mma_tf32_16x8x8(cf[t], ah, bh0, bh1);
@@ -499,13 +498,14 @@ struct Pass {
   };
   template <class K>
   struct P2p {
-    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, double* ys, cudaStream_t s) {
+    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint32_t* qhi,
+                    const uint32_t* qlo, double* ys, cudaStream_t s) {
       constexpr int RM = RC >= 8 ? RC : 8;
-      const size_t smem_mma = (size_t)9 * nv.nmax * (2 * sizeof(uint32_t) * RM + sizeof(float2));
-      if (RC >= 8 && smem_mma <= 200 * 1024) {
+      const size_t smem_mma = (size_t)9 * nv.nmax * sizeof(float2);
+      if (RC >= 8) {
         const int warps = std::min(8, (nv.nmax + 15) / 16);
         allow_smem(k_p2p_mma<K, RM>, smem_mma);
-        k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qs32, ys);
+        k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qhi, qlo, ys);
       } else {
         const int T = (nv.nmax + 31) / 32 * 32;
         size_t smem = (size_t)9 * nv.nmax * (sizeof(float) * RC + sizeof(float2));
@@ -520,7 +520,7 @@ struct Pass {
                   int64_t ldy, int ncols, cudaStream_t s, StageTimer* tm, int64_t* launches) {
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32);
+    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhi, bs.qlo);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
@@ -544,7 +544,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "p2p");
-    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.ys, s);
+    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhi, bs.qlo, bs.ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
     k_scatter_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
@@ -560,6 +560,8 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
   const int RC = kBatchMax;
   bs.qs = arena.alloc<double>((size_t)p.N * RC);
   bs.qs32 = arena.alloc<float>((size_t)p.N * RC);
+  bs.qhi = arena.alloc<uint32_t>((size_t)p.N * RC);
+  bs.qlo = arena.alloc<uint32_t>((size_t)p.N * RC);
   bs.ys = arena.alloc<double>((size_t)p.N * RC);
   std::vector<const double*> hq(kMaxLevels, nullptr);
   std::vector<double*> hy(kMaxLevels, nullptr);
