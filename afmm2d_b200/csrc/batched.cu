@@ -7,9 +7,10 @@
 // source with one broadcast load.
 //  * M2M / L2L: FP64 L2P (row-major / column-major), one thread per output
 //    row with RC FP64 accumulators.
-//  * M2L: entries evaluated on the fly in FP64 from the skeleton coordinates
-//    (as in the single-RHS mixed path) and multiplied with the RC-column
-//    charge blocks on the FP64 tensor cores (8 rows x 4 sources tiles).
+//  * M2L: the stored FP64 blocks (one HBM read for all RC columns), or
+//    entries evaluated on the fly in FP64 from the skeleton coordinates when
+//    no blocks are stored, multiplied with the RC-column charge blocks on the
+//    FP64 tensor cores (8 rows x 4 sources tiles).
 //  * Near field: entries in FP32 from leaf-relative coordinates with the FP64
 //    fallback for close pairs (as in the single-RHS mixed path), multiplied
 //    on the TF32 tensor cores in a three-term high/low split (16 targets x 8
@@ -23,9 +24,6 @@ namespace afmm {
 
 namespace {
 
-// Gather: thread (j, c) reads q[c][j] (original order; a block's consecutive j
-// share sectors of every column) and writes the sorted point-major block
-// qs[iperm[j]][c] (16 lanes fill one 128-byte row).
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
@@ -38,8 +36,11 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
   lo = to_tf32(x - __uint_as_float(hi));
 }
 
-// The sorted charges are also written as FP32 and as the TF32 high / low
-// parts the tensor-core near field multiplies with (split once per pass).
+// Gather: thread (j, c) reads q[c][j] (original order; a block's consecutive j
+// share sectors of every column) and writes the sorted point-major block
+// qs[iperm[j]][c] (16 lanes fill one 128-byte row), also as FP32 and as the
+// TF32 high / low parts the tensor-core near field multiplies with (split
+// once per pass).
 template <int RC>
 __global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int32_t* __restrict__ iperm,
                            int N, double* qs, float* qs32, uint32_t* qhi, uint32_t* qlo) {
@@ -353,6 +354,87 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
   }
 }
 
+// M2L from the stored FP64 blocks (the same blocks the FP64 path applies)
+// with FP64 tensor-core tiles: one warp per chunk of up to 32 skeleton rows of
+// one box, i.e. NT <= 4 tiles of 8 rows that share every B fragment.  For a
+// 4-column step of a column-major block the warp's A loads are four
+// contiguous runs of up to 32 rows, all issued before the step's MMAs.  The
+// 40 slots' rank and skeleton offset are fetched once per warp and broadcast
+// by shuffles.
+template <int RC, int NT>
+__device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const double* __restrict__ qh,
+                                                 double* __restrict__ yb, int b, int r0, int lane) {
+  const int r = v.rank[b];
+  const int i0 = r0 - v.skel_off[b];
+  const int nrow = min(8 * NT, r - i0);
+  const int trow = lane >> 2, tsrc = lane & 3;
+  // slot table: lane l holds slot l (and slot 32 + l for l < 8)
+  const int sa = v.il[(long)b * 40 + lane];
+  const int sb = lane < 8 ? v.il[(long)b * 40 + 32 + lane] : -1;
+  const int ra = sa >= 0 ? v.rank[sa] : 0, rb = sb >= 0 ? v.rank[sb] : 0;
+  const int oa = sa >= 0 ? v.skel_off[sa] : 0, ob = sb >= 0 ? v.skel_off[sb] : 0;
+  bool rowok[NT];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  const double* M = v.m2l + v.m2l_off[b] + i0 + trow;
+  double c[NT][RC / 8][2];
+#pragma unroll
+  for (int u = 0; u < NT; ++u)
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) c[u][t][0] = c[u][t][1] = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
+    if (rc == 0) continue;  // empty slot or rank-0 box: no block stored
+    const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
+#pragma unroll 2
+    for (int cc0 = 0; cc0 < rc; cc0 += 4) {
+      const int cs = cc0 + tsrc;
+      const bool vs = cs < rc;
+      const double* Mc = M + (long)cs * r;
+      double a[NT], bq[RC / 8];
+#pragma unroll
+      for (int u = 0; u < NT; ++u) a[u] = (vs && rowok[u]) ? Mc[u * 8] : 0.0;
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) bq[t] = vs ? qh[(long)(sc + cs) * RC + t * 8 + trow] : 0.0;
+#pragma unroll
+      for (int u = 0; u < NT; ++u)
+#pragma unroll
+        for (int t = 0; t < RC / 8; ++t) mma_f64_8x8x4(c[u][t][0], c[u][t][1], a[u], bq[t]);
+    }
+    M += (long)r * rc;
+  }
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    if (rowok[u]) {
+      double* out = yb + (long)(r0 + u * 8 + trow) * RC;
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t)
+        *reinterpret_cast<double2*>(out + t * 8 + 2 * tsrc) = make_double2(c[u][t][0], c[u][t][1]);
+    }
+  }
+}
+
+template <int RC>
+__global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const double* const* __restrict__ qhat_lv,
+                                                        double* const* __restrict__ yhat_lv) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ls.cgrp0[ls.nlev]) return;  // whole warps only
+  int j = 0;
+  while (j + 1 < ls.nlev && gw >= ls.cgrp0[j + 1]) ++j;
+  const LevelView& v = ls.lv[j];
+  const long g = gw - ls.cgrp0[j];
+  const int b = v.cgrp_box[g];
+  const int r0 = v.cgrp_row[g];
+  const int nt = (min(32, v.skel_off[b] + v.rank[b] - r0) + 7) >> 3;  // warp-uniform
+  switch (nt) {
+    case 1: m2l_stored_chunk<RC, 1>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
+    case 2: m2l_stored_chunk<RC, 2>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
+    case 3: m2l_stored_chunk<RC, 3>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
+    default: m2l_stored_chunk<RC, 4>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
+  }
+}
+
 // Near field with TF32 tensor-core tiles in a three-term split
 // (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy): one CTA per leaf, the
 // source leaves' coordinates (relative to their leaf anchor) staged in shared
@@ -486,9 +568,14 @@ struct Pass {
   struct M2l {
     static void run(const LevelSet& ls, const KernelParams& kp, const double* const* qh, double* const* yh,
                     cudaStream_t s) {
-      if (RC >= 8) {
+      constexpr int RM = RC >= 8 ? RC : 8;
+      if (RC >= 8 && ls.lv[0].m2l != nullptr) {
+        // stored blocks: one HBM read of the blocks serves all RC columns
+        const long warps = ls.cgrp0[ls.nlev];
+        k_m2l_stored_mma<RM><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
+      } else if (RC >= 8) {
         const long warps = ls.grp0[ls.nlev];
-        k_m2l_mma<K, (RC >= 8 ? RC : 8)><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
+        k_m2l_mma<K, RM><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
       } else {
         const long rows = ls.row0[ls.nlev];
         k_m2l_b<K, RC><<<nbk(rows, 128), 128, 0, s>>>(ls, kp, qh, yh);

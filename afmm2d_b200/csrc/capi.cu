@@ -238,16 +238,21 @@ void build_plan(afmm_handle* h) {
     v.grp_box = d.grp_box;
     v.grp_row = d.grp_row;
     v.ngroups = d.ngroups;
+    v.cgrp_box = d.cgrp_box;
+    v.cgrp_row = d.cgrp_row;
+    v.ncgroups = d.ncgroups;
     v.nrows = d.total_rank;
     v.nnodes = d.h_node_off.empty() ? 0 : d.h_node_off[d.nbox];
   }
   p.levels.nlev = 0;
   p.levels.row0[0] = 0;
   p.levels.grp0[0] = 0;
+  p.levels.cgrp0[0] = 0;
   for (int j = 2; j <= h->L; ++j) {
     p.levels.lv[p.levels.nlev] = p.lv[j];
     p.levels.row0[p.levels.nlev + 1] = p.levels.row0[p.levels.nlev] + p.lv[j].nrows;
     p.levels.grp0[p.levels.nlev + 1] = p.levels.grp0[p.levels.nlev] + p.lv[j].ngroups;
+    p.levels.cgrp0[p.levels.nlev + 1] = p.levels.cgrp0[p.levels.nlev] + p.lv[j].ncgroups;
     ++p.levels.nlev;
   }
   for (int j = 0; j <= h->L; ++j) {
@@ -435,20 +440,31 @@ void do_assemble(afmm_handle* h) {
     fill_box_map(v.skel_off, v.nbox, v.skel_box, s);
     fill_box_map(v.node_off, v.nbox, v.node_box, s);
     h->launches += 2;
-    // row groups of at most 8 skeleton rows of one box (tensor-core M2L tiles)
-    std::vector<int32_t> gb, gr;
-    for (long b = 0; b < v.nbox; ++b)
-      for (int i = 0; i < v.h_rank[b]; i += 8) {
-        gb.push_back((int32_t)b);
-        gr.push_back(v.h_skel_off[b] + i);
+    // row groups of at most 8 (and chunks of at most 32) skeleton rows of one
+    // box: the tensor-core M2L tiles
+    for (int span : {8, 32}) {
+      std::vector<int32_t> gb, gr;
+      for (long b = 0; b < v.nbox; ++b)
+        for (int i = 0; i < v.h_rank[b]; i += span) {
+          gb.push_back((int32_t)b);
+          gr.push_back(v.h_skel_off[b] + i);
+        }
+      int32_t* db = h->arena.alloc<int32_t>(gb.size());
+      int32_t* dr = h->arena.alloc<int32_t>(gr.size());
+      if (!gb.empty()) {
+        AFMM_CUDA(cudaMemcpyAsync(db, gb.data(), sizeof(int32_t) * gb.size(), cudaMemcpyHostToDevice, s));
+        AFMM_CUDA(cudaMemcpyAsync(dr, gr.data(), sizeof(int32_t) * gr.size(), cudaMemcpyHostToDevice, s));
+        AFMM_CUDA(cudaStreamSynchronize(s));
       }
-    v.ngroups = (long)gb.size();
-    v.grp_box = h->arena.alloc<int32_t>(gb.size());
-    v.grp_row = h->arena.alloc<int32_t>(gr.size());
-    if (!gb.empty()) {
-      AFMM_CUDA(cudaMemcpyAsync(v.grp_box, gb.data(), sizeof(int32_t) * gb.size(), cudaMemcpyHostToDevice, s));
-      AFMM_CUDA(cudaMemcpyAsync(v.grp_row, gr.data(), sizeof(int32_t) * gr.size(), cudaMemcpyHostToDevice, s));
-      AFMM_CUDA(cudaStreamSynchronize(s));
+      if (span == 8) {
+        v.ngroups = (long)gb.size();
+        v.grp_box = db;
+        v.grp_row = dr;
+      } else {
+        v.ncgroups = (long)gb.size();
+        v.cgrp_box = db;
+        v.cgrp_row = dr;
+      }
     }
   }
   for (int j = 2; j <= L; ++j) {

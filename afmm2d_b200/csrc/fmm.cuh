@@ -47,6 +47,9 @@ struct LevelView {
   const int32_t* grp_box = nullptr;   // row group (<= 8 rows of one box) -> box
   const int32_t* grp_row = nullptr;   // row group -> first skeleton row
   long ngroups = 0;
+  const int32_t* cgrp_box = nullptr;  // row chunk (<= 32 rows of one box) -> box
+  const int32_t* cgrp_row = nullptr;  // row chunk -> first skeleton row
+  long ncgroups = 0;
   long nrows = 0;                     // skeleton rows (sum of ranks)
   long nnodes = 0;                    // node rows (sum of node counts)
 };
@@ -57,7 +60,8 @@ struct LevelSet {
   int nlev = 0;
   LevelView lv[kMaxLevels];
   long row0[kMaxLevels + 1] = {0};
-  long grp0[kMaxLevels + 1] = {0};  // prefix of row-group counts
+  long grp0[kMaxLevels + 1] = {0};   // prefix of row-group counts
+  long cgrp0[kMaxLevels + 1] = {0};  // prefix of row-chunk counts
 };
 
 // Leaf-level data for the near field.
