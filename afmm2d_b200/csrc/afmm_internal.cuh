@@ -184,6 +184,9 @@ struct LevelDev {
   int32_t* cgrp_box = nullptr;  // row chunk (<= 32 rows of one box) -> box
   int32_t* cgrp_row = nullptr;  // row chunk -> first skeleton row
   long ncgroups = 0;
+  int32_t* ncgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
+  int32_t* ncgrp_row = nullptr;  // node-row chunk -> first node row
+  long nncgroups = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)

@@ -354,13 +354,67 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
   }
 }
 
+// FP64 tensor-core product of one warp's row chunk: for NT tiles of 8 rows,
+// c[u] += A[rows of tile u][0:K] * B[0:K][0:RC], A column-major with leading
+// dimension lda (A points at the lane's row of tile 0: base + first row +
+// trow), B point-major (k, col) at k*RC + col.  Each 4-column step issues all
+// of its A and B loads before its MMAs; for lda >= 32 the warp's A loads are
+// four contiguous runs of up to 32 rows.
+template <int RC, int NT>
+__device__ __forceinline__ void mma_rows(double (&c)[NT][RC / 8][2], const double* __restrict__ A, int lda, int K,
+                                         const double* __restrict__ B, const bool (&rowok)[NT], int trow, int tsrc) {
+#pragma unroll 2
+  for (int k0 = 0; k0 < K; k0 += 4) {
+    const int k = k0 + tsrc;
+    const bool vk = k < K;
+    const double* Ak = A + (long)k * lda;
+    double a[NT], bq[RC / 8];
+#pragma unroll
+    for (int u = 0; u < NT; ++u) a[u] = (vk && rowok[u]) ? Ak[u * 8] : 0.0;
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) bq[t] = vk ? B[(long)k * RC + t * 8 + trow] : 0.0;
+#pragma unroll
+    for (int u = 0; u < NT; ++u)
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) mma_f64_8x8x4(c[u][t][0], c[u][t][1], a[u], bq[t]);
+  }
+}
+
+template <int RC, int NT>
+__device__ __forceinline__ void zero_tiles(double (&c)[NT][RC / 8][2]) {
+#pragma unroll
+  for (int u = 0; u < NT; ++u)
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) c[u][t][0] = c[u][t][1] = 0.0;
+}
+
+// Writes (or adds) the chunk's rows: out points at row 0 of the chunk.
+template <int RC, int NT, bool ADD>
+__device__ __forceinline__ void store_tiles(const double (&c)[NT][RC / 8][2], double* __restrict__ out,
+                                            const bool (&rowok)[NT], int trow, int tsrc) {
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    if (rowok[u]) {
+      double2* o = reinterpret_cast<double2*>(out + (long)(u * 8 + trow) * RC + 2 * tsrc);
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) {
+        double2 w = make_double2(c[u][t][0], c[u][t][1]);
+        if (ADD) {
+          const double2 cur = o[t * 4];
+          w.x += cur.x;
+          w.y += cur.y;
+        }
+        o[t * 4] = w;
+      }
+    }
+  }
+}
+
 // M2L from the stored FP64 blocks (the same blocks the FP64 path applies)
 // with FP64 tensor-core tiles: one warp per chunk of up to 32 skeleton rows of
-// one box, i.e. NT <= 4 tiles of 8 rows that share every B fragment.  For a
-// 4-column step of a column-major block the warp's A loads are four
-// contiguous runs of up to 32 rows, all issued before the step's MMAs.  The
-// 40 slots' rank and skeleton offset are fetched once per warp and broadcast
-// by shuffles.
+// one box, i.e. NT <= 4 tiles of 8 rows that share every B fragment.  The 40
+// slots' rank and skeleton offset are fetched once per warp and broadcast by
+// shuffles.
 template <int RC, int NT>
 __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const double* __restrict__ qh,
                                                  double* __restrict__ yb, int b, int r0, int lane) {
@@ -378,40 +432,97 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
   const double* M = v.m2l + v.m2l_off[b] + i0 + trow;
   double c[NT][RC / 8][2];
-#pragma unroll
-  for (int u = 0; u < NT; ++u)
-#pragma unroll
-    for (int t = 0; t < RC / 8; ++t) c[u][t][0] = c[u][t][1] = 0.0;
+  zero_tiles<RC, NT>(c);
   for (int s = 0; s < 40; ++s) {
     const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
     if (rc == 0) continue;  // empty slot or rank-0 box: no block stored
     const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
-#pragma unroll 2
-    for (int cc0 = 0; cc0 < rc; cc0 += 4) {
-      const int cs = cc0 + tsrc;
-      const bool vs = cs < rc;
-      const double* Mc = M + (long)cs * r;
-      double a[NT], bq[RC / 8];
-#pragma unroll
-      for (int u = 0; u < NT; ++u) a[u] = (vs && rowok[u]) ? Mc[u * 8] : 0.0;
-#pragma unroll
-      for (int t = 0; t < RC / 8; ++t) bq[t] = vs ? qh[(long)(sc + cs) * RC + t * 8 + trow] : 0.0;
-#pragma unroll
-      for (int u = 0; u < NT; ++u)
-#pragma unroll
-        for (int t = 0; t < RC / 8; ++t) mma_f64_8x8x4(c[u][t][0], c[u][t][1], a[u], bq[t]);
-    }
+    mma_rows<RC, NT>(c, M, r, rc, qh + (long)sc * RC, rowok, trow, tsrc);
     M += (long)r * rc;
   }
+  store_tiles<RC, NT, false>(c, yb + (long)r0 * RC, rowok, trow, tsrc);
+}
+
+// M2M on FP64 tensor-core tiles: qhat rows of box b = L2P_b^T src_b, one warp
+// per chunk of up to 32 skeleton rows (the row-major L2P copy is the
+// column-major A with lda = rank).
+template <int RC, int NT>
+__device__ __forceinline__ void m2m_chunk(const LevelView& v, const double* __restrict__ src_all, int leaf,
+                                          double* __restrict__ qhat, int b, int r0, int lane) {
+  const int r = v.rank[b];
+  const int i0 = r0 - v.skel_off[b];
+  const int nrow = min(8 * NT, r - i0);
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const int trow = lane >> 2, tsrc = lane & 3;
+  bool rowok[NT];
 #pragma unroll
-  for (int u = 0; u < NT; ++u) {
-    if (rowok[u]) {
-      double* out = yb + (long)(r0 + u * 8 + trow) * RC;
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  const double* src = src_all + (long)(leaf ? v.leaf_start[b] : v.node_off[b]) * RC;
+  double c[NT][RC / 8][2];
+  zero_tiles<RC, NT>(c);
+  mma_rows<RC, NT>(c, v.l2p_rm + v.l2p_off[b] + i0 + trow, r, n, src, rowok, trow, tsrc);
+  store_tiles<RC, NT, false>(c, qhat + (long)r0 * RC, rowok, trow, tsrc);
+}
+
+// L2L on FP64 tensor-core tiles: node rows of box b get L2P_b yhat_b, added
+// to the child's incoming potential, or written as the leaf potential; one
+// warp per chunk of up to 32 node rows.
+template <int RC, int NT>
+__device__ __forceinline__ void l2l_chunk(const LevelView& v, const double* __restrict__ yhat,
+                                          double* __restrict__ child_yhat, double* __restrict__ ys, int leaf, int b,
+                                          int g0, int lane) {
+  const int r = v.rank[b];
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const int i0 = g0 - v.node_off[b];
+  const int nrow = min(8 * NT, n - i0);
+  const int trow = lane >> 2, tsrc = lane & 3;
+  bool rowok[NT];
 #pragma unroll
-      for (int t = 0; t < RC / 8; ++t)
-        *reinterpret_cast<double2*>(out + t * 8 + 2 * tsrc) = make_double2(c[u][t][0], c[u][t][1]);
-    }
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  double c[NT][RC / 8][2];
+  zero_tiles<RC, NT>(c);
+  mma_rows<RC, NT>(c, v.l2p + v.l2p_off[b] + i0 + trow, n, r, yhat + (long)v.skel_off[b] * RC, rowok, trow, tsrc);
+  if (leaf)
+    store_tiles<RC, NT, false>(c, ys + (long)(v.leaf_start[b] + i0) * RC, rowok, trow, tsrc);
+  else
+    store_tiles<RC, NT, true>(c, child_yhat + (long)g0 * RC, rowok, trow, tsrc);
+}
+
+// Number of 8-row tiles of a chunk of at most 32 rows (warp-uniform).
+__device__ __forceinline__ int chunk_tiles(int rows_left) { return (min(32, rows_left) + 7) >> 3; }
+
+#define AFMM_NT_SWITCH(nt, CALL) \
+  switch (nt) {                  \
+    case 1: CALL(1); break;      \
+    case 2: CALL(2); break;      \
+    case 3: CALL(3); break;      \
+    default: CALL(4); break;     \
   }
+
+template <int RC>
+__global__ void __launch_bounds__(128) k_m2m_mma(LevelView v, const double* __restrict__ src_all, int leaf,
+                                                 double* __restrict__ qhat) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= v.ncgroups) return;  // whole warps only
+  const int b = v.cgrp_box[g];
+  const int r0 = v.cgrp_row[g];
+#define AFMM_M2M(NT) m2m_chunk<RC, NT>(v, src_all, leaf, qhat, b, r0, lane)
+  AFMM_NT_SWITCH(chunk_tiles(v.skel_off[b] + v.rank[b] - r0), AFMM_M2M)
+#undef AFMM_M2M
+}
+
+template <int RC>
+__global__ void __launch_bounds__(128) k_l2l_mma(LevelView v, const double* __restrict__ yhat,
+                                                 double* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= v.nncgroups) return;  // whole warps only
+  const int b = v.ncgrp_box[g];
+  const int g0 = v.ncgrp_row[g];
+#define AFMM_L2L(NT) l2l_chunk<RC, NT>(v, yhat, child_yhat, ys, leaf, b, g0, lane)
+  AFMM_NT_SWITCH(chunk_tiles(v.node_off[b + 1] - g0), AFMM_L2L)
+#undef AFMM_L2L
 }
 
 template <int RC>
@@ -426,13 +537,9 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
   const long g = gw - ls.cgrp0[j];
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
-  const int nt = (min(32, v.skel_off[b] + v.rank[b] - r0) + 7) >> 3;  // warp-uniform
-  switch (nt) {
-    case 1: m2l_stored_chunk<RC, 1>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
-    case 2: m2l_stored_chunk<RC, 2>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
-    case 3: m2l_stored_chunk<RC, 3>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
-    default: m2l_stored_chunk<RC, 4>(v, qhat_lv[j], yhat_lv[j], b, r0, lane); break;
-  }
+#define AFMM_M2L(NT) m2l_stored_chunk<RC, NT>(v, qhat_lv[j], yhat_lv[j], b, r0, lane)
+  AFMM_NT_SWITCH(chunk_tiles(v.skel_off[b] + v.rank[b] - r0), AFMM_M2L)
+#undef AFMM_M2L
 }
 
 // Near field with TF32 tensor-core tiles in a three-term split
@@ -605,6 +712,7 @@ struct Pass {
 
   static void run(const MatvecPlan& p, BatchState& bs, const NearView& nv, const double* q, int64_t ldq, double* y,
                   int64_t ldy, int ncols, cudaStream_t s, StageTimer* tm, int64_t* launches) {
+    constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
     k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhi, bs.qlo);
@@ -614,7 +722,11 @@ struct Pass {
     for (int j = p.L; j >= 2; --j) {
       const LevelView& v = p.lv[j];
       if (v.nrows == 0) continue;
-      k_m2m_b<RC><<<nbk(v.nrows, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L, bs.qhat[j]);
+      if (RC >= 8)
+        k_m2m_mma<RM><<<nbk(v.ncgroups * 32, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
+                                                               bs.qhat[j]);
+      else
+        k_m2m_b<RC><<<nbk(v.nrows, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L, bs.qhat[j]);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
@@ -625,8 +737,12 @@ struct Pass {
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];
       if (v.nnodes == 0) continue;
-      k_l2l_b<RC><<<nbk(v.nnodes, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr, bs.ys,
-                                                     j == p.L);
+      if (RC >= 8)
+        k_l2l_mma<RM><<<nbk(v.nncgroups * 32, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
+                                                                bs.ys, j == p.L);
+      else
+        k_l2l_b<RC><<<nbk(v.nnodes, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr, bs.ys,
+                                                       j == p.L);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }

@@ -241,6 +241,9 @@ void build_plan(afmm_handle* h) {
     v.cgrp_box = d.cgrp_box;
     v.cgrp_row = d.cgrp_row;
     v.ncgroups = d.ncgroups;
+    v.ncgrp_box = d.ncgrp_box;
+    v.ncgrp_row = d.ncgrp_row;
+    v.nncgroups = d.nncgroups;
     v.nrows = d.total_rank;
     v.nnodes = d.h_node_off.empty() ? 0 : d.h_node_off[d.nbox];
   }
@@ -441,14 +444,18 @@ void do_assemble(afmm_handle* h) {
     fill_box_map(v.node_off, v.nbox, v.node_box, s);
     h->launches += 2;
     // row groups of at most 8 (and chunks of at most 32) skeleton rows of one
-    // box: the tensor-core M2L tiles
-    for (int span : {8, 32}) {
+    // box: the tensor-core M2L / M2M tiles;
+    // and chunks of at most 32 node rows (tensor-core L2L tiles)
+    for (int span : {8, 32, -32}) {
       std::vector<int32_t> gb, gr;
-      for (long b = 0; b < v.nbox; ++b)
-        for (int i = 0; i < v.h_rank[b]; i += span) {
+      for (long b = 0; b < v.nbox; ++b) {
+        const int rows = span > 0 ? v.h_rank[b] : v.h_node_off[b + 1] - v.h_node_off[b];
+        const int first = span > 0 ? v.h_skel_off[b] : v.h_node_off[b];
+        for (int i = 0; i < rows; i += std::abs(span)) {
           gb.push_back((int32_t)b);
-          gr.push_back(v.h_skel_off[b] + i);
+          gr.push_back(first + i);
         }
+      }
       int32_t* db = h->arena.alloc<int32_t>(gb.size());
       int32_t* dr = h->arena.alloc<int32_t>(gr.size());
       if (!gb.empty()) {
@@ -460,10 +467,14 @@ void do_assemble(afmm_handle* h) {
         v.ngroups = (long)gb.size();
         v.grp_box = db;
         v.grp_row = dr;
-      } else {
+      } else if (span == 32) {
         v.ncgroups = (long)gb.size();
         v.cgrp_box = db;
         v.cgrp_row = dr;
+      } else {
+        v.nncgroups = (long)gb.size();
+        v.ncgrp_box = db;
+        v.ncgrp_row = dr;
       }
     }
   }
