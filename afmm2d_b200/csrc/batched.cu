@@ -542,20 +542,33 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
 #undef AFMM_M2L
 }
 
+// TF32 high / low parts of an FP32 value by masking (the tensor cores read
+// the top 19 bits of a TF32 operand): hi keeps 11 significant bits, lo the
+// next 11 of the exact remainder; |x - hi - lo| <= 2^-21 |x|.
+__device__ __forceinline__ void split_tf32_mask(float x, uint32_t& hi, uint32_t& lo) {
+  hi = __float_as_uint(x) & 0xffffe000u;
+  lo = __float_as_uint(x - __uint_as_float(hi)) & 0xffffe000u;
+}
+
+// Far-away stand-ins for padded source slots and absent targets: their
+// entries are finite for every kernel and never below a fallback threshold;
+// padded sources get zero charges and absent targets are not stored.
+constexpr float kPadSrc = 1.0e15f, kPadTgt = -1.0e15f;
+
 // Near field with TF32 tensor-core tiles in a three-term split
-// (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy): one CTA per leaf, the
-// source leaves' coordinates (relative to their leaf anchor) staged in shared
-// memory, the charges' TF32 high / low parts read from L2 (split once per
-// pass by the gather).  Each warp takes
-// tiles of 16 targets; for every 8 sources each lane evaluates the four FP32
-// entries of its A fragment (FP64 fallback for close pairs), and the 16 x 8
-// tile is multiplied with the 8 x RC charge block.  Tile sums per source leaf
-// are accumulated in FP64.
+// (A_hi B_hi + A_hi B_lo + A_lo B_hi, ~FP32 accuracy).  One CTA per leaf, one
+// warp per 32 targets (two 16 x 8 tiles sharing every charge fragment).  The
+// source leaves (neighbours 0..7, then the leaf itself) are staged in shared
+// memory in the target leaf's frame (each source leaf's anchor offset folded
+// in FP64), padded to multiples of 8; the charges' TF32 high / low parts
+// (split once per pass by the gather) come from L2.  Each lane evaluates 8
+// FP32 entries per 8-source step; a warp vote sends the rare close pairs to
+// the FP64 fallback.  Tile sums per source leaf are accumulated in FP64.
 template <class K, int RC>
-__global__ void k_p2p_mma(NearView nv, KernelParams kp, const uint32_t* __restrict__ qhi,
-                          const uint32_t* __restrict__ qlo, double* __restrict__ ys) {
+__global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, const uint32_t* __restrict__ qhi,
+                                                 const uint32_t* __restrict__ qlo, double* __restrict__ ys) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
+  __shared__ int s_src[9], s_cnt[9], s_coff[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
   const long b = blockIdx.x;
   const int n = nv.leaf_cnt[b];
@@ -571,99 +584,133 @@ __global__ void k_p2p_mma(NearView nv, KernelParams kp, const uint32_t* __restri
       const double2 ac = nv.anchor[cbx];
       s_src[m] = nv.leaf_start[cbx];
       s_cnt[m] = nv.leaf_cnt[cbx];
-      s_off[m] = off;
+      s_coff[m] = off;
       s_dx[m] = (float)(ab.x - ac.x);
       s_dy[m] = (float)(ab.y - ac.y);
-      s_thr[m] = fallback_r2_b<K>(sb, nv.span[cbx]);
-      off += nv.leaf_cnt[cbx];
+      s_thr[m] = fmaxf(fallback_r2_b<K>(sb, nv.span[cbx]), 1.0e-30f);
+      off += (nv.leaf_cnt[cbx] + 7) >> 3;
       ++m;
     }
-    s_off[m] = off;
+    s_coff[m] = off;
     s_ns = m;
   }
   __syncthreads();
   const int ns = s_ns;
   float2* sx = (float2*)smem;
   for (int m = 0; m < ns; ++m) {
-    const int o = s_off[m], nc = s_cnt[m], src = s_src[m];
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) sx[o + t] = nv.rel[src + t];
+    const int o = s_coff[m] * 8, nc = s_cnt[m], src = s_src[m], np = (s_coff[m + 1] - s_coff[m]) * 8;
+    const float ddx = s_dx[m], ddy = s_dy[m];
+    for (int t = threadIdx.x; t < np; t += blockDim.x) {
+      float2 p = make_float2(kPadSrc, kPadSrc);
+      if (t < nc) {
+        p = nv.rel[src + t];
+        p.x -= ddx;
+        p.y -= ddy;
+      }
+      sx[o + t] = p;
+    }
   }
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
-  for (int tile = warp; tile * 16 < n; tile += nw) {
-    const int t0 = tile * 16 + gq, t1 = t0 + 8;
-    const bool v0 = t0 < n, v1 = t1 < n;
-    const float2 x0 = v0 ? nv.rel[s0 + t0] : make_float2(0.f, 0.f);
-    const float2 x1 = v1 ? nv.rel[s0 + t1] : make_float2(0.f, 0.f);
-    double acc[RC / 8][4];
+  for (int tg = warp; tg * 32 < n; tg += nw) {
+    // targets of this lane: rows gq, gq + 8 of tile 0 and of tile 1
+    int ti[4];
+    float2 x[4];
 #pragma unroll
-    for (int t = 0; t < RC / 8; ++t) acc[t][0] = acc[t][1] = acc[t][2] = acc[t][3] = 0.0;
+    for (int k = 0; k < 4; ++k) {
+      ti[k] = tg * 32 + k * 8 + gq;
+      x[k] = ti[k] < n ? nv.rel[s0 + ti[k]] : make_float2(kPadTgt, kPadTgt);
+    }
+    double acc[2][RC / 8][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) acc[u][t][0] = acc[u][t][1] = acc[u][t][2] = acc[u][t][3] = 0.0;
     for (int m = 0; m < ns; ++m) {
-      const int o = s_off[m], nc = s_cnt[m], src = s_src[m];
+      const int src = s_src[m], nc = s_cnt[m];
       const float thr = s_thr[m];
-      const float ox0 = x0.x + s_dx[m], oy0 = x0.y + s_dy[m], ox1 = x1.x + s_dx[m], oy1 = x1.y + s_dy[m];
-      float cf[RC / 8][4];
+      float cf[2][RC / 8][4];
 #pragma unroll
-      for (int t = 0; t < RC / 8; ++t) cf[t][0] = cf[t][1] = cf[t][2] = cf[t][3] = 0.0f;
-      for (int k0 = 0; k0 < nc; k0 += 8) {
-        const int sa = k0 + tq, sb2 = k0 + tq + 4;
-        const bool va = sa < nc, vb = sb2 < nc;
-        float kv[4];  // A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]
-        const bool vv[4] = {v0 && va, v1 && va, v0 && vb, v1 && vb};
-        const int tgt[4] = {t0, t1, t0, t1}, srs[4] = {sa, sa, sb2, sb2};
+      for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          kv[e] = 0.0f;
-          if (vv[e]) {
-            const float2 p = sx[o + srs[e]];
-            const float ox = (e & 1) ? ox1 : ox0, oy = (e & 1) ? oy1 : oy0;
-            const float dx = ox - p.x, dy = oy - p.y;
-            const float R2 = fmaf(dx, dx, dy * dy);
-            if (R2 < thr) {
-              const int pi = s0 + tgt[e], qi = src + srs[e];
-              if (pi == qi) {
-                kv[e] = (float)K::at_zero();
-              } else {
-                const double2 a = nv.pts[pi], c2 = nv.pts[qi];
-                kv[e] = (float)K::eval_exact(r2_exact(a.x, a.y, c2.x, c2.y), kp);
-              }
-            } else {
-              kv[e] = K::eval32(R2, a32, p32);
-            }
+        for (int t = 0; t < RC / 8; ++t) cf[u][t][0] = cf[u][t][1] = cf[u][t][2] = cf[u][t][3] = 0.0f;
+      for (int c = s_coff[m]; c < s_coff[m + 1]; ++c) {
+        const int j0 = (c - s_coff[m]) * 8;
+        const float2 ps[2] = {sx[c * 8 + tq], sx[c * 8 + tq + 4]};
+        float kv[4][2], r2[4][2];
+        bool close = false;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float dx = x[k].x - ps[h].x, dy = x[k].y - ps[h].y;
+            r2[k][h] = fmaf(dx, dx, dy * dy);
+            close |= r2[k][h] < thr;
+            kv[k][h] = K::eval32(r2[k][h], a32, p32);
           }
-        }
-        uint32_t ah[4], al[4];
+        if (__any_sync(0xffffffffu, close)) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) split_tf32(kv[e], ah[e], al[e]);
+          for (int k = 0; k < 4; ++k)
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+              if (r2[k][h] < thr) {  // both points are real (stand-ins are never close)
+                const int pi = s0 + ti[k], qi = src + j0 + tq + 4 * h;
+                if (pi == qi) {
+                  kv[k][h] = (float)K::at_zero();
+                } else {
+                  const double2 pa = nv.pts[pi], pc = nv.pts[qi];
+                  kv[k][h] = (float)K::eval_exact(r2_exact(pa.x, pa.y, pc.x, pc.y), kp);
+                }
+              }
+        }
+        // A fragments: tile u rows (gq, gq + 8) = targets 2u, 2u + 1
+        uint32_t ah[2][4], al[2][4];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          split_tf32_mask(kv[2 * u][0], ah[u][0], al[u][0]);
+          split_tf32_mask(kv[2 * u + 1][0], ah[u][1], al[u][1]);
+          split_tf32_mask(kv[2 * u][1], ah[u][2], al[u][2]);
+          split_tf32_mask(kv[2 * u + 1][1], ah[u][3], al[u][3]);
+        }
+        const bool va = j0 + tq < nc, vb = j0 + tq + 4 < nc;
+        const long ra = (long)(src + j0 + tq) * RC + gq, rb = ra + 4 * RC;
 #pragma unroll
         for (int t = 0; t < RC / 8; ++t) {
-          const long ra = (long)(src + sa) * RC + t * 8 + gq, rb = (long)(src + sb2) * RC + t * 8 + gq;
-          const uint32_t bh0 = va ? qhi[ra] : 0u, bl0 = va ? qlo[ra] : 0u;
-          const uint32_t bh1 = vb ? qhi[rb] : 0u, bl1 = vb ? qlo[rb] : 0u;
-          mma_tf32_16x8x8(cf[t], ah, bh0, bh1);
-          mma_tf32_16x8x8(cf[t], ah, bl0, bl1);
-          mma_tf32_16x8x8(cf[t], al, bh0, bh1);
+          const uint32_t bh0 = va ? qhi[ra + t * 8] : 0u, bl0 = va ? qlo[ra + t * 8] : 0u;
+          const uint32_t bh1 = vb ? qhi[rb + t * 8] : 0u, bl1 = vb ? qlo[rb + t * 8] : 0u;
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            mma_tf32_16x8x8(cf[u][t], ah[u], bh0, bh1);
+            mma_tf32_16x8x8(cf[u][t], ah[u], bl0, bl1);
+            mma_tf32_16x8x8(cf[u][t], al[u], bh0, bh1);
+          }
         }
       }
 #pragma unroll
-      for (int t = 0; t < RC / 8; ++t)
+      for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int e = 0; e < 4; ++e) acc[t][e] += (double)cf[t][e];
-    }
+        for (int t = 0; t < RC / 8; ++t)
 #pragma unroll
-    for (int t = 0; t < RC / 8; ++t) {
-      if (v0) {
-        double* out = ys + (long)(s0 + t0) * RC + t * 8 + 2 * tq;
-        out[0] += acc[t][0];
-        out[1] += acc[t][1];
-      }
-      if (v1) {
-        double* out = ys + (long)(s0 + t1) * RC + t * 8 + 2 * tq;
-        out[0] += acc[t][2];
-        out[1] += acc[t][3];
-      }
+          for (int e = 0; e < 4; ++e) acc[u][t][e] += (double)cf[u][t][e];
     }
+    // D fragment of tile u: rows gq (e = 0, 1) and gq + 8 (e = 2, 3), columns 2tq, 2tq + 1
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int hr = 0; hr < 2; ++hr) {
+        const int t_ = ti[2 * u + hr];
+        if (t_ < n) {
+#pragma unroll
+          for (int t = 0; t < RC / 8; ++t) {
+            double2* o = reinterpret_cast<double2*>(ys + (long)(s0 + t_) * RC + t * 8 + 2 * tq);
+            double2 w = *o;
+            w.x += acc[u][t][2 * hr];
+            w.y += acc[u][t][2 * hr + 1];
+            *o = w;
+          }
+        }
+      }
   }
 }
 
@@ -695,9 +742,9 @@ struct Pass {
     static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint32_t* qhi,
                     const uint32_t* qlo, double* ys, cudaStream_t s) {
       constexpr int RM = RC >= 8 ? RC : 8;
-      const size_t smem_mma = (size_t)9 * nv.nmax * sizeof(float2);
+      const size_t smem_mma = (size_t)9 * ((nv.nmax + 7) / 8 * 8) * sizeof(float2);
       if (RC >= 8) {
-        const int warps = std::min(8, (nv.nmax + 15) / 16);
+        const int warps = std::min(4, (nv.nmax + 31) / 32);
         allow_smem(k_p2p_mma<K, RM>, smem_mma);
         k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qhi, qlo, ys);
       } else {
