@@ -39,6 +39,9 @@ struct Error {
 // wherever results steer pivoting (ACA, L2P, M2L blocks).  `eval` is the fast FP64 form for the matvec, `eval32` the FP32
 // form for the mixed-precision matvec (R2 formed from coordinates relative to
 // box anchors; the third argument is the Gaussian parameter).
+// `eval32_pos` is `eval32` for R2 at or above the near-field fallback
+// threshold (R2 > 0 and normal): hardware approximations (flush-to-zero
+// rsqrt, lg2, ex2) with relative error near FP32 rounding.
 struct KernelParams {
   int id;
   double a;      // 2^-L
@@ -66,7 +69,16 @@ struct KOneOverRScaled {
     float R = sqrtf(R2);
     return (R < a) ? __fdiv_rn(R, a) : __fdiv_rn(a, R);
   }
+  __device__ __forceinline__ static float eval32_pos(float R2, float a, float p) { return eval32(R2, a, p); }
 };
+
+// rsqrt.approx.ftz.f32 refined by one Newton-Raphson step y += y/2 (1 - x y^2).
+__device__ __forceinline__ float rsqrt_nr_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  const float e = fmaf(-x * y, y, 1.0f);
+  return fmaf(0.5f * y, e, y);
+}
 
 // log(r) with the diagonal convention (examples/tutorial.cpp:22-35).
 struct KLog {
@@ -89,6 +101,13 @@ struct KLog {
     if (R2 < a * a) return __fdiv_rn(0.5f * R2 * l, a * a);
     return 0.5f * l;
   }
+  // ln(R2) = lg2(R2) ln 2; lg2.approx has absolute error ~2^-22
+  __device__ __forceinline__ static float eval32_pos(float R2, float a, float) {
+    if (R2 < 1e-10f) return 0.0f;
+    const float l = __log2f(R2) * 0.693147180559945309f;
+    if (R2 < a * a) return __fdividef(0.5f * R2 * l, a * a);
+    return 0.5f * l;
+  }
 };
 
 // 1/r with 0 at r = 0.
@@ -109,6 +128,7 @@ struct KOneOverR {
     float e = fmaf(-R2 * y, y, 1.0f);
     return fmaf(0.5f * y, e, y);
   }
+  __device__ __forceinline__ static float eval32_pos(float R2, float, float) { return rsqrt_nr_ftz(R2); }
 };
 
 // Gaussian exp(-R2/param) (1 on the diagonal).
@@ -121,6 +141,9 @@ struct KGaussian {
   __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return exp(-R2 / p.param); }
   __device__ __forceinline__ static float eval32(float R2, float, float param) {
     return expf(-__fdiv_rn(R2, param));
+  }
+  __device__ __forceinline__ static float eval32_pos(float R2, float, float param) {
+    return __expf(-__fdividef(R2, param));
   }
 };
 

@@ -43,7 +43,7 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
 // once per pass).
 template <int RC>
 __global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int32_t* __restrict__ iperm,
-                           int N, double* qs, float* qs32, uint32_t* qhi, uint32_t* qlo) {
+                           int N, double* qs, float* qs32, uint2* qhl) {
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (long)N * RC) return;
   const int j = (int)(t / RC), c = (int)(t % RC);
@@ -52,10 +52,9 @@ __global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols,
   qs[d] = v;
   const float f = (float)v;
   qs32[d] = f;
-  uint32_t h, l;
-  split_tf32(f, h, l);
-  qhi[d] = h;
-  qlo[d] = l;
+  uint2 hl;
+  split_tf32(f, hl.x, hl.y);
+  qhl[d] = hl;
 }
 
 // Scatter: thread (j, c) reads the sorted row of j and writes y[c][j].
@@ -560,13 +559,17 @@ constexpr float kPadSrc = 1.0e15f, kPadTgt = -1.0e15f;
 // warp per 32 targets (two 16 x 8 tiles sharing every charge fragment).  The
 // source leaves (neighbours 0..7, then the leaf itself) are staged in shared
 // memory in the target leaf's frame (each source leaf's anchor offset folded
-// in FP64), padded to multiples of 8; the charges' TF32 high / low parts
-// (split once per pass by the gather) come from L2.  Each lane evaluates 8
-// FP32 entries per 8-source step; a warp vote sends the rare close pairs to
-// the FP64 fallback.  Tile sums per source leaf are accumulated in FP64.
+// in FP64), padded to multiples of 8; the charges' interleaved TF32 high / low
+// parts (split once per pass by the gather) come from L2, one 8-byte load per
+// fragment element.  Each lane evaluates 8 FP32 entries per 8-source step; a
+// warp vote sends the rare close pairs to the FP64 fallback.  The high*high
+// products and the two correction products accumulate in separate FP32 tiles
+// (independent MMA chains), which are added per source leaf into FP64 sums
+// kept in shared memory.
 template <class K, int RC>
-__global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, const uint32_t* __restrict__ qhi,
-                                                 const uint32_t* __restrict__ qlo, double* __restrict__ ys) {
+__global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, const uint2* __restrict__ qhl,
+                                                 double* __restrict__ ys) {
+  constexpr int NE = 2 * (RC / 8) * 4;  // FP64 sums per lane
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_coff[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
@@ -596,7 +599,9 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
   }
   __syncthreads();
   const int ns = s_ns;
-  float2* sx = (float2*)smem;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  double* sacc = (double*)smem + (long)warp * NE * 32;  // lane-major: sum e of lane l at e*32 + l
+  float2* sx = (float2*)((double*)smem + (long)nw * NE * 32);
   for (int m = 0; m < ns; ++m) {
     const int o = s_coff[m] * 8, nc = s_cnt[m], src = s_src[m], np = (s_coff[m + 1] - s_coff[m]) * 8;
     const float ddx = s_dx[m], ddy = s_dy[m];
@@ -611,51 +616,49 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
     }
   }
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const int gq = lane >> 2, tq = lane & 3;
   for (int tg = warp; tg * 32 < n; tg += nw) {
-    // targets of this lane: rows gq, gq + 8 of tile 0 and of tile 1
-    int ti[4];
+    // targets of this lane: rows gq, gq + 8 of tile 0 (k = 0, 1) and of tile 1 (k = 2, 3)
     float2 x[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      ti[k] = tg * 32 + k * 8 + gq;
-      x[k] = ti[k] < n ? nv.rel[s0 + ti[k]] : make_float2(kPadTgt, kPadTgt);
+      const int ti = tg * 32 + k * 8 + gq;
+      x[k] = ti < n ? nv.rel[s0 + ti] : make_float2(kPadTgt, kPadTgt);
     }
-    double acc[2][RC / 8][4];
 #pragma unroll
-    for (int u = 0; u < 2; ++u)
-#pragma unroll
-      for (int t = 0; t < RC / 8; ++t) acc[u][t][0] = acc[u][t][1] = acc[u][t][2] = acc[u][t][3] = 0.0;
+    for (int e = 0; e < NE; ++e) sacc[e * 32 + lane] = 0.0;
     for (int m = 0; m < ns; ++m) {
       const int src = s_src[m], nc = s_cnt[m];
       const float thr = s_thr[m];
-      float cf[2][RC / 8][4];
+      float cm[2][RC / 8][4], cc[2][RC / 8][4];
 #pragma unroll
       for (int u = 0; u < 2; ++u)
 #pragma unroll
-        for (int t = 0; t < RC / 8; ++t) cf[u][t][0] = cf[u][t][1] = cf[u][t][2] = cf[u][t][3] = 0.0f;
+        for (int t = 0; t < RC / 8; ++t)
+#pragma unroll
+          for (int e = 0; e < 4; ++e) cm[u][t][e] = cc[u][t][e] = 0.0f;
       for (int c = s_coff[m]; c < s_coff[m + 1]; ++c) {
         const int j0 = (c - s_coff[m]) * 8;
         const float2 ps[2] = {sx[c * 8 + tq], sx[c * 8 + tq + 4]};
-        float kv[4][2], r2[4][2];
+        float kv[4][2];
         bool close = false;
 #pragma unroll
         for (int k = 0; k < 4; ++k)
 #pragma unroll
           for (int h = 0; h < 2; ++h) {
             const float dx = x[k].x - ps[h].x, dy = x[k].y - ps[h].y;
-            r2[k][h] = fmaf(dx, dx, dy * dy);
-            close |= r2[k][h] < thr;
-            kv[k][h] = K::eval32(r2[k][h], a32, p32);
+            const float r2 = fmaf(dx, dx, dy * dy);
+            close |= r2 < thr;
+            kv[k][h] = K::eval32_pos(fmaxf(r2, thr), a32, p32);
           }
         if (__any_sync(0xffffffffu, close)) {
 #pragma unroll
           for (int k = 0; k < 4; ++k)
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-              if (r2[k][h] < thr) {  // both points are real (stand-ins are never close)
-                const int pi = s0 + ti[k], qi = src + j0 + tq + 4 * h;
+            for (int h = 0; h < 2; ++h) {
+              const float dx = x[k].x - ps[h].x, dy = x[k].y - ps[h].y;
+              if (fmaf(dx, dx, dy * dy) < thr) {  // both points are real (stand-ins are never close)
+                const int pi = s0 + tg * 32 + k * 8 + gq, qi = src + j0 + tq + 4 * h;
                 if (pi == qi) {
                   kv[k][h] = (float)K::at_zero();
                 } else {
@@ -663,6 +666,7 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
                   kv[k][h] = (float)K::eval_exact(r2_exact(pa.x, pa.y, pc.x, pc.y), kp);
                 }
               }
+            }
         }
         // A fragments: tile u rows (gq, gq + 8) = targets 2u, 2u + 1
         uint32_t ah[2][4], al[2][4];
@@ -674,16 +678,17 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
           split_tf32_mask(kv[2 * u + 1][1], ah[u][3], al[u][3]);
         }
         const bool va = j0 + tq < nc, vb = j0 + tq + 4 < nc;
-        const long ra = (long)(src + j0 + tq) * RC + gq, rb = ra + 4 * RC;
+        const uint2* ra = qhl + (long)(src + j0 + tq) * RC + gq;
+        const uint2* rb = ra + 4 * RC;
 #pragma unroll
         for (int t = 0; t < RC / 8; ++t) {
-          const uint32_t bh0 = va ? qhi[ra + t * 8] : 0u, bl0 = va ? qlo[ra + t * 8] : 0u;
-          const uint32_t bh1 = vb ? qhi[rb + t * 8] : 0u, bl1 = vb ? qlo[rb + t * 8] : 0u;
+          const uint2 b0 = va ? ra[t * 8] : make_uint2(0u, 0u);
+          const uint2 b1 = vb ? rb[t * 8] : make_uint2(0u, 0u);
 #pragma unroll
           for (int u = 0; u < 2; ++u) {
-            mma_tf32_16x8x8(cf[u][t], ah[u], bh0, bh1);
-            mma_tf32_16x8x8(cf[u][t], ah[u], bl0, bl1);
-            mma_tf32_16x8x8(cf[u][t], al[u], bh0, bh1);
+            mma_tf32_16x8x8(cm[u][t], ah[u], b0.x, b1.x);
+            mma_tf32_16x8x8(cc[u][t], ah[u], b0.y, b1.y);
+            mma_tf32_16x8x8(cc[u][t], al[u], b0.x, b1.x);
           }
         }
       }
@@ -692,21 +697,22 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
 #pragma unroll
         for (int t = 0; t < RC / 8; ++t)
 #pragma unroll
-          for (int e = 0; e < 4; ++e) acc[u][t][e] += (double)cf[u][t][e];
+          for (int e = 0; e < 4; ++e)
+            sacc[((u * (RC / 8) + t) * 4 + e) * 32 + lane] += (double)cm[u][t][e] + (double)cc[u][t][e];
     }
     // D fragment of tile u: rows gq (e = 0, 1) and gq + 8 (e = 2, 3), columns 2tq, 2tq + 1
 #pragma unroll
     for (int u = 0; u < 2; ++u)
 #pragma unroll
       for (int hr = 0; hr < 2; ++hr) {
-        const int t_ = ti[2 * u + hr];
-        if (t_ < n) {
+        const int ti = tg * 32 + (2 * u + hr) * 8 + gq;
+        if (ti < n) {
 #pragma unroll
           for (int t = 0; t < RC / 8; ++t) {
-            double2* o = reinterpret_cast<double2*>(ys + (long)(s0 + t_) * RC + t * 8 + 2 * tq);
+            double2* o = reinterpret_cast<double2*>(ys + (long)(s0 + ti) * RC + t * 8 + 2 * tq);
             double2 w = *o;
-            w.x += acc[u][t][2 * hr];
-            w.y += acc[u][t][2 * hr + 1];
+            w.x += sacc[((u * (RC / 8) + t) * 4 + 2 * hr) * 32 + lane];
+            w.y += sacc[((u * (RC / 8) + t) * 4 + 2 * hr + 1) * 32 + lane];
             *o = w;
           }
         }
@@ -739,14 +745,15 @@ struct Pass {
   };
   template <class K>
   struct P2p {
-    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint32_t* qhi,
-                    const uint32_t* qlo, double* ys, cudaStream_t s) {
+    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint2* qhl, double* ys,
+                    cudaStream_t s) {
       constexpr int RM = RC >= 8 ? RC : 8;
-      const size_t smem_mma = (size_t)9 * ((nv.nmax + 7) / 8 * 8) * sizeof(float2);
+      const int warps = std::min(4, (nv.nmax + 31) / 32);
+      const size_t smem_mma =
+          (size_t)9 * ((nv.nmax + 7) / 8 * 8) * sizeof(float2) + (size_t)warps * RM * 32 * sizeof(double);
       if (RC >= 8) {
-        const int warps = std::min(4, (nv.nmax + 31) / 32);
         allow_smem(k_p2p_mma<K, RM>, smem_mma);
-        k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qhi, qlo, ys);
+        k_p2p_mma<K, RM><<<(int)nv.nleaf, 32 * warps, smem_mma, s>>>(nv, kp, qhl, ys);
       } else {
         const int T = (nv.nmax + 31) / 32 * 32;
         size_t smem = (size_t)9 * nv.nmax * (sizeof(float) * RC + sizeof(float2));
@@ -762,7 +769,7 @@ struct Pass {
     constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhi, bs.qlo);
+    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
@@ -794,7 +801,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "p2p");
-    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhi, bs.qlo, bs.ys, s);
+    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhl, bs.ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
     k_scatter_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
@@ -810,8 +817,7 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
   const int RC = kBatchMax;
   bs.qs = arena.alloc<double>((size_t)p.N * RC);
   bs.qs32 = arena.alloc<float>((size_t)p.N * RC);
-  bs.qhi = arena.alloc<uint32_t>((size_t)p.N * RC);
-  bs.qlo = arena.alloc<uint32_t>((size_t)p.N * RC);
+  bs.qhl = arena.alloc<uint2>((size_t)p.N * RC);
   bs.ys = arena.alloc<double>((size_t)p.N * RC);
   std::vector<const double*> hq(kMaxLevels, nullptr);
   std::vector<double*> hy(kMaxLevels, nullptr);

@@ -29,8 +29,7 @@ struct BatchState {
   bool ready = false;
   double* qs = nullptr;     // sorted charges, point-major N x kBatchMax
   float* qs32 = nullptr;
-  uint32_t* qhi = nullptr;  // TF32 high / low parts of qs32
-  uint32_t* qlo = nullptr;
+  uint2* qhl = nullptr;     // TF32 high / low parts of qs32, interleaved
   double* ys = nullptr;     // sorted potentials, point-major
   double* qhat[kMaxLevels] = {nullptr};
   double* yhat[kMaxLevels] = {nullptr};
