@@ -192,6 +192,9 @@ struct DevArena {
 
 // ------------------------------------------------------------- tree layout
 // Per level j (4^j boxes, quadtree numbering k: parent k/4, children 4k+c).
+// Rows per warp of the FP64 tensor-core sweeps (five 8-row tiles).
+constexpr int kChunkRows = 40;
+
 struct LevelDev {
   long nbox = 0;
   int32_t* il = nullptr;        // nbox*40: inner slots 0..15 then outer 0..23, -1 = none
@@ -204,10 +207,10 @@ struct LevelDev {
   int32_t* grp_box = nullptr;   // row group (<= 8 rows of one box) -> box
   int32_t* grp_row = nullptr;   // row group -> first skeleton row
   long ngroups = 0;
-  int32_t* cgrp_box = nullptr;  // row chunk (<= 32 rows of one box) -> box
+  int32_t* cgrp_box = nullptr;  // row chunk (<= kChunkRows rows of one box) -> box
   int32_t* cgrp_row = nullptr;  // row chunk -> first skeleton row
   long ncgroups = 0;
-  int32_t* ncgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
+  int32_t* ncgrp_box = nullptr;  // node-row chunk (<= kChunkRows node rows of one box) -> box
   int32_t* ncgrp_row = nullptr;  // node-row chunk -> first node row
   long nncgroups = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks

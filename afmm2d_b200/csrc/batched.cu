@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
 // dimension lda (A points at the lane's row of tile 0: base + first row +
 // trow), B point-major (k, col) at k*RC + col.  Each 4-column step issues all
 // of its A and B loads before its MMAs; for lda >= 32 the warp's A loads are
-// four contiguous runs of up to 32 rows.
+// five contiguous runs of up to 40 rows.
 template <int RC, int NT>
 __device__ __forceinline__ void mma_rows(double (&c)[NT][RC / 8][2], const double* __restrict__ A, int lda, int K,
                                          const double* __restrict__ B, const bool (&rowok)[NT], int trow, int tsrc) {
@@ -410,8 +410,8 @@ __device__ __forceinline__ void store_tiles(const double (&c)[NT][RC / 8][2], do
 }
 
 // M2L from the stored FP64 blocks (the same blocks the FP64 path applies)
-// with FP64 tensor-core tiles: one warp per chunk of up to 32 skeleton rows of
-// one box, i.e. NT <= 4 tiles of 8 rows that share every B fragment.  The 40
+// with FP64 tensor-core tiles: one warp per chunk of up to kChunkRows skeleton rows of
+// one box, i.e. NT <= 5 tiles of 8 rows that share every B fragment.  The 40
 // slots' rank and skeleton offset are fetched once per warp and broadcast by
 // shuffles.
 template <int RC, int NT>
@@ -443,7 +443,7 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
 }
 
 // M2M on FP64 tensor-core tiles: qhat rows of box b = L2P_b^T src_b, one warp
-// per chunk of up to 32 skeleton rows (the row-major L2P copy is the
+// per chunk of up to kChunkRows skeleton rows (the row-major L2P copy is the
 // column-major A with lda = rank).
 template <int RC, int NT>
 __device__ __forceinline__ void m2m_chunk(const LevelView& v, const double* __restrict__ src_all, int leaf,
@@ -465,7 +465,7 @@ __device__ __forceinline__ void m2m_chunk(const LevelView& v, const double* __re
 
 // L2L on FP64 tensor-core tiles: node rows of box b get L2P_b yhat_b, added
 // to the child's incoming potential, or written as the leaf potential; one
-// warp per chunk of up to 32 node rows.
+// warp per chunk of up to kChunkRows node rows.
 template <int RC, int NT>
 __device__ __forceinline__ void l2l_chunk(const LevelView& v, const double* __restrict__ yhat,
                                           double* __restrict__ child_yhat, double* __restrict__ ys, int leaf, int b,
@@ -487,15 +487,20 @@ __device__ __forceinline__ void l2l_chunk(const LevelView& v, const double* __re
     store_tiles<RC, NT, true>(c, child_yhat + (long)g0 * RC, rowok, trow, tsrc);
 }
 
-// Number of 8-row tiles of a chunk of at most 32 rows (warp-uniform).
-__device__ __forceinline__ int chunk_tiles(int rows_left) { return (min(32, rows_left) + 7) >> 3; }
+// Number of 8-row tiles of a chunk: rows up to the next chunk's first row
+// (the chunk tables cut boxes into equal chunks of at most kChunkRows rows).
+__device__ __forceinline__ int chunk_tiles(const int32_t* chunk_first, long g, long nchunks, int box_end) {
+  const int next = g + 1 < nchunks ? min(box_end, chunk_first[g + 1]) : box_end;
+  return (next - chunk_first[g] + 7) >> 3;
+}
 
 #define AFMM_NT_SWITCH(nt, CALL) \
   switch (nt) {                  \
     case 1: CALL(1); break;      \
     case 2: CALL(2); break;      \
     case 3: CALL(3); break;      \
-    default: CALL(4); break;     \
+    case 4: CALL(4); break;      \
+    default: CALL(5); break;     \
   }
 
 template <int RC>
@@ -507,7 +512,7 @@ __global__ void __launch_bounds__(128) k_m2m_mma(LevelView v, const double* __re
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
 #define AFMM_M2M(NT) m2m_chunk<RC, NT>(v, src_all, leaf, qhat, b, r0, lane)
-  AFMM_NT_SWITCH(chunk_tiles(v.skel_off[b] + v.rank[b] - r0), AFMM_M2M)
+  AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2M)
 #undef AFMM_M2M
 }
 
@@ -520,7 +525,7 @@ __global__ void __launch_bounds__(128) k_l2l_mma(LevelView v, const double* __re
   const int b = v.ncgrp_box[g];
   const int g0 = v.ncgrp_row[g];
 #define AFMM_L2L(NT) l2l_chunk<RC, NT>(v, yhat, child_yhat, ys, leaf, b, g0, lane)
-  AFMM_NT_SWITCH(chunk_tiles(v.node_off[b + 1] - g0), AFMM_L2L)
+  AFMM_NT_SWITCH(chunk_tiles(v.ncgrp_row, g, v.nncgroups, v.node_off[b + 1]), AFMM_L2L)
 #undef AFMM_L2L
 }
 
@@ -537,7 +542,7 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
 #define AFMM_M2L(NT) m2l_stored_chunk<RC, NT>(v, qhat_lv[j], yhat_lv[j], b, r0, lane)
-  AFMM_NT_SWITCH(chunk_tiles(v.skel_off[b] + v.rank[b] - r0), AFMM_M2L)
+  AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2L)
 #undef AFMM_M2L
 }
 

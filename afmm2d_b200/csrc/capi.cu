@@ -443,15 +443,18 @@ void do_assemble(afmm_handle* h) {
     fill_box_map(v.skel_off, v.nbox, v.skel_box, s);
     fill_box_map(v.node_off, v.nbox, v.node_box, s);
     h->launches += 2;
-    // row groups of at most 8 (and chunks of at most 32) skeleton rows of one
-    // box: the tensor-core M2L / M2M tiles;
-    // and chunks of at most 32 node rows (tensor-core L2L tiles)
-    for (int span : {8, 32, -32}) {
+    // row groups of at most 8 skeleton rows of one box (on-the-fly M2L
+    // tiles), and balanced chunks of at most kChunkRows skeleton rows
+    // (M2L / M2M tiles) or node rows (L2L tiles): a box of n rows is cut into
+    // ceil(n / kChunkRows) chunks of equal size rounded up to 8 rows
+    for (int span : {8, kChunkRows, -kChunkRows}) {
       std::vector<int32_t> gb, gr;
       for (long b = 0; b < v.nbox; ++b) {
         const int rows = span > 0 ? v.h_rank[b] : v.h_node_off[b + 1] - v.h_node_off[b];
         const int first = span > 0 ? v.h_skel_off[b] : v.h_node_off[b];
-        for (int i = 0; i < rows; i += std::abs(span)) {
+        const int nch = (rows + std::abs(span) - 1) / std::abs(span);
+        const int step = nch > 0 ? ((rows + nch - 1) / nch + 7) / 8 * 8 : 0;
+        for (int i = 0; i < rows; i += (span == 8 ? 8 : step)) {
           gb.push_back((int32_t)b);
           gr.push_back(first + i);
         }
@@ -467,7 +470,7 @@ void do_assemble(afmm_handle* h) {
         v.ngroups = (long)gb.size();
         v.grp_box = db;
         v.grp_row = dr;
-      } else if (span == 32) {
+      } else if (span == kChunkRows) {
         v.ncgroups = (long)gb.size();
         v.cgrp_box = db;
         v.cgrp_row = dr;

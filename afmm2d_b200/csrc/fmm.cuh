@@ -47,10 +47,10 @@ struct LevelView {
   const int32_t* grp_box = nullptr;   // row group (<= 8 rows of one box) -> box
   const int32_t* grp_row = nullptr;   // row group -> first skeleton row
   long ngroups = 0;
-  const int32_t* cgrp_box = nullptr;  // row chunk (<= 32 rows of one box) -> box
+  const int32_t* cgrp_box = nullptr;  // row chunk (<= kChunkRows rows of one box) -> box
   const int32_t* cgrp_row = nullptr;  // row chunk -> first skeleton row
   long ncgroups = 0;
-  const int32_t* ncgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
+  const int32_t* ncgrp_box = nullptr;  // node-row chunk (<= kChunkRows node rows of one box) -> box
   const int32_t* ncgrp_row = nullptr;  // node-row chunk -> first node row
   long nncgroups = 0;
   long nrows = 0;                     // skeleton rows (sum of ranks)
