@@ -36,35 +36,66 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
   lo = to_tf32(x - __uint_as_float(hi));
 }
 
-// Gather: thread (j, c) reads q[c][j] (original order; a block's consecutive j
-// share sectors of every column) and writes the sorted point-major block
-// qs[iperm[j]][c] (16 lanes fill one 128-byte row), also as FP32 and as the
-// TF32 high / low parts the tensor-core near field multiplies with (split
-// once per pass).
+// Gather through a shared-memory transpose: a block takes kTileJ consecutive
+// points, reads each column of q as one contiguous run, and writes each
+// point's sorted row qs[iperm[j]][0:RC] (one 128-byte line for RC = 16).
+// With RC >= 8 the row is also written as interleaved TF32 high / low parts
+// (the tensor-core near field's charges), otherwise as FP32.
+constexpr int kTileJ = 64;
+
 template <int RC>
-__global__ void k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols, const int32_t* __restrict__ iperm,
-                           int N, double* qs, float* qs32, uint2* qhl) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)N * RC) return;
-  const int j = (int)(t / RC), c = (int)(t % RC);
-  const double v = c < ncols ? q[(long)c * ldq + j] : 0.0;
-  const long d = (long)iperm[j] * RC + c;
-  qs[d] = v;
-  const float f = (float)v;
-  qs32[d] = f;
-  uint2 hl;
-  split_tf32(f, hl.x, hl.y);
-  qhl[d] = hl;
+__global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols,
+                                                  const int32_t* __restrict__ iperm, int N, double* qs, float* qs32,
+                                                  uint2* qhl) {
+  __shared__ double tile[RC][kTileJ + 1];
+  const long j0 = (long)blockIdx.x * kTileJ;
+  for (int idx = threadIdx.x; idx < RC * kTileJ; idx += blockDim.x) {
+    const int c = idx / kTileJ, jj = idx % kTileJ;
+    const long j = j0 + jj;
+    tile[c][jj] = (c < ncols && j < N) ? q[(long)c * ldq + j] : 0.0;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < (RC / 2) * kTileJ; idx += blockDim.x) {
+    const int jj = idx / (RC / 2), cp = idx % (RC / 2);
+    const long j = j0 + jj;
+    if (j >= N) continue;
+    const double v0 = tile[2 * cp][jj], v1 = tile[2 * cp + 1][jj];
+    const long d = (long)iperm[j] * RC + 2 * cp;
+    *reinterpret_cast<double2*>(qs + d) = make_double2(v0, v1);
+    const float f0 = (float)v0, f1 = (float)v1;
+    if (RC >= 8) {
+      uint4 hl;
+      split_tf32(f0, hl.x, hl.y);
+      split_tf32(f1, hl.z, hl.w);
+      *reinterpret_cast<uint4*>(qhl + d) = hl;
+    } else {
+      *reinterpret_cast<float2*>(qs32 + d) = make_float2(f0, f1);
+    }
+  }
 }
 
-// Scatter: thread (j, c) reads the sorted row of j and writes y[c][j].
+// Scatter through a shared-memory transpose: a block takes kTileJ consecutive
+// points, reads their sorted rows ys[iperm[j]][0:RC], and writes each column
+// of y as one contiguous run.
 template <int RC>
-__global__ void k_scatter_b(const double* __restrict__ ys, const int32_t* __restrict__ iperm, int N, int ncols,
-                            double* y, int64_t ldy) {
-  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= (long)N * RC) return;
-  const int j = (int)(t / RC), c = (int)(t % RC);
-  if (c < ncols) y[(long)c * ldy + j] = ys[(long)iperm[j] * RC + c];
+__global__ void __launch_bounds__(256) k_scatter_b(const double* __restrict__ ys, const int32_t* __restrict__ iperm,
+                                                   int N, int ncols, double* y, int64_t ldy) {
+  __shared__ double tile[RC][kTileJ + 1];
+  const long j0 = (long)blockIdx.x * kTileJ;
+  for (int idx = threadIdx.x; idx < (RC / 2) * kTileJ; idx += blockDim.x) {
+    const int jj = idx / (RC / 2), cp = idx % (RC / 2);
+    const long j = j0 + jj;
+    if (j >= N) continue;
+    const double2 v = *reinterpret_cast<const double2*>(ys + (long)iperm[j] * RC + 2 * cp);
+    tile[2 * cp][jj] = v.x;
+    tile[2 * cp + 1][jj] = v.y;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < RC * kTileJ; idx += blockDim.x) {
+    const int c = idx / kTileJ, jj = idx % kTileJ;
+    const long j = j0 + jj;
+    if (c < ncols && j < N) y[(long)c * ldy + j] = tile[c][jj];
+  }
 }
 
 template <int RC>
@@ -774,7 +805,7 @@ struct Pass {
     constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl);
+    k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
@@ -809,7 +840,7 @@ struct Pass {
     dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhl, bs.ys, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
-    k_scatter_b<RC><<<nbk((long)N * RC, 256), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
+    k_scatter_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
@@ -821,8 +852,10 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
   if (bs.ready) return;
   const int RC = kBatchMax;
   bs.qs = arena.alloc<double>((size_t)p.N * RC);
-  bs.qs32 = arena.alloc<float>((size_t)p.N * RC);
+  // FP32 charges (passes of fewer than 8 columns) and TF32 parts (8 or more)
+  // are never needed by the same pass: one buffer holds either
   bs.qhl = arena.alloc<uint2>((size_t)p.N * RC);
+  bs.qs32 = reinterpret_cast<float*>(bs.qhl);
   bs.ys = arena.alloc<double>((size_t)p.N * RC);
   std::vector<const double*> hq(kMaxLevels, nullptr);
   std::vector<double*> hy(kMaxLevels, nullptr);

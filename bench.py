@@ -209,7 +209,11 @@ def run_ours(args):
             call(name)
         torch.cuda.synchronize()
         return
-    # per-stage device times (separate, untimed passes)
+    # per-stage device times (separate, untimed passes after one warm call of
+    # each path, so lazy kernel loading and first-touch allocations are not
+    # counted)
+    for name in paths:
+        call(name)
     a.set_profiling(True)
     stages = {}
     for name in paths:
