@@ -104,6 +104,19 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def scaled_traffic(kernel, algorithmic_bytes):
+    """DRAM bytes per launch for `kernel`, scaled from an ncu capture of a
+    smaller case of the same workload (profiles/traffic.json holds the
+    captured dram__bytes_read.sum + dram__bytes_write.sum and the capture's
+    algorithmic bytes); None if no capture is recorded."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)[kernel]
+        return algorithmic_bytes * d["dram_bytes"] / d["algorithmic_bytes"]
+    except (OSError, KeyError, ValueError, ZeroDivisionError):
+        return None
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -189,10 +202,16 @@ def run_ours(args):
         prec, nr = paths[name]
         a.matvec_device(dQ.data_ptr(), dY.data_ptr(), nr, N, prec)
 
-    def timed(name, steps, warm):
+    def timed(name, steps, warm, stage_acc=None):
+        """Mean device ms per step (CUDA events on the handle's stream, L2
+        flushed before every step).  With stage_acc, the library's per-stage
+        events (one pair of marks around every kernel stage, on the same
+        stream) are recorded inside the timed steps and summed into it."""
         for _ in range(warm):
             call(name)
         ms = []
+        if stage_acc is not None:
+            a.set_profiling(True)
         for _ in range(steps):
             with torch.cuda.stream(stream):
                 flush.zero_()
@@ -202,6 +221,11 @@ def run_ours(args):
             e1.record(stream)
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
+            if stage_acc is not None:
+                for k, v in a.stage_times().items():
+                    stage_acc[k] = stage_acc.get(k, 0.0) + v / steps
+        if stage_acc is not None:
+            a.set_profiling(False)
         return float(np.mean(ms))
 
     if args.profile_once:
@@ -209,17 +233,6 @@ def run_ours(args):
             call(name)
         torch.cuda.synchronize()
         return
-    # per-stage device times (separate, untimed passes after one warm call of
-    # each path, so lazy kernel loading and first-touch allocations are not
-    # counted)
-    for name in paths:
-        call(name)
-    a.set_profiling(True)
-    stages = {}
-    for name in paths:
-        call(name)
-        stages[name] = a.stage_times()
-    a.set_profiling(False)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -227,9 +240,11 @@ def run_ours(args):
     clk.start()
     t_dev = {}
     launches = {}
+    stages = {}
     for name in paths:
         l0 = a.launch_count()
-        t_dev[name] = timed(name, args.steps, args.warmup)
+        stages[name] = {}
+        t_dev[name] = timed(name, args.steps, args.warmup, stages[name])
         launches[name] = (a.launch_count() - l0) // (args.steps + args.warmup)
     torch.cuda.synchronize()
     clocks = clk.stop()
@@ -262,32 +277,35 @@ def run_ours(args):
     value = world * N * R / (t_dev["batched"] * 1e-3)
     hbm, bf16, peak_kind = load_peaks()
     fp64_peak, fp32_peak = A.measure_fma_peaks()
-    # roofline of the dominant kernel of the headline (batched) path
+    # roofline of the dominant kernel of the headline (batched) path, its
+    # duration averaged over the timed steps (stage events on the launching
+    # stream); algorithmic bytes / flops per launch from the assembled counts
     sb = stages["batched"]
     dom = max((k for k in sb if k not in ("end", "h2d", "d2h")), key=lambda k: sb[k])
+    rows = counts["sum_rank"]
     if dom == "m2l":
-        flops = 2.0 * R * counts["m2l_entries"]
-        roof = {"bound": "fp64", "kernel": "k_m2l_b (M2L on the fly, FP64)", "unit": "TFLOP/s",
-                "achieved": flops / (sb[dom] * 1e-3) / 1e12, "peak": fp64_peak,
-                "peak_kind": "measured live (register-only FP64 FMA loop)", "traffic": None,
-                "algorithmic_flops": flops, "flop_definition": "2*nrhs FP64 FMA flops per M2L entry",
+        byts = counts["m2l_entries"] * 8 + 2 * rows * R * 8
+        roof = {"bound": "hbm", "kernel": "k_m2l_stored_mma (stored FP64 M2L blocks, FP64 tensor-core tiles)",
+                "unit": "GB/s", "achieved": byts / (sb[dom] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
+                "algorithmic_bytes": byts,
+                "byte_definition": "8 B per stored M2L entry (read once) + nrhs*8 B per skeleton row in and out",
                 "ms": sb[dom]}
+        roof["traffic"] = scaled_traffic("k_m2l_stored_mma", byts)
     elif dom == "p2p":
         flops = 2.0 * R * counts["near_evals"]
-        roof = {"bound": "fp32", "kernel": "k_p2p_b (near field, FP32)", "unit": "TFLOP/s",
-                "achieved": flops / (sb[dom] * 1e-3) / 1e12, "peak": fp32_peak,
+        roof = {"bound": "fp32", "kernel": "k_p2p_mma (near field, FP32 entries on TF32x3 tensor-core tiles)",
+                "unit": "TFLOP/s", "achieved": flops / (sb[dom] * 1e-3) / 1e12, "peak": fp32_peak,
                 "peak_kind": "measured live (register-only FP32 FMA loop)", "traffic": None,
-                "algorithmic_flops": flops, "flop_definition": "2*nrhs FP32 FMA flops per near-field pair",
-                "ms": sb[dom]}
+                "algorithmic_flops": flops, "flop_definition": "2*nrhs flops per near-field pair", "ms": sb[dom]}
     else:
-        byts = counts["l2p_entries"] * 8 * 2
+        byts = counts["l2p_entries"] * 8 + 2 * rows * R * 8
         roof = {"bound": "hbm", "kernel": dom, "unit": "GB/s", "achieved": byts / (sb[dom] * 1e-3) / 1e9,
-                "peak": hbm, "peak_kind": peak_kind, "traffic": None, "ms": sb[dom]}
+                "peak": hbm, "peak_kind": peak_kind, "traffic": None, "algorithmic_bytes": byts, "ms": sb[dom]}
     roof["frac"] = roof["achieved"] / roof["peak"] if roof.get("peak") else None
     # the FP64 path's stored M2L is HBM-bound
     s64 = stages["fp64"]
     m2l_bytes = counts["m2l_entries"] * 8
-    roof64 = {"bound": "hbm", "kernel": "k_m2l_apply (stored FP64 M2L)", "unit": "GB/s",
+    roof64 = {"bound": "hbm", "kernel": "k_m2l_apply (stored FP64 M2L, one RHS)", "unit": "GB/s",
               "achieved": m2l_bytes / (s64["m2l"] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
               "algorithmic_bytes": m2l_bytes, "ms": s64["m2l"]}
     roof64["frac"] = roof64["achieved"] / hbm
