@@ -440,11 +440,40 @@ __device__ __forceinline__ void store_tiles(const double (&c)[NT][RC / 8][2], do
   }
 }
 
+// L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned
+// start, size a multiple of 16).  Issued by one lane.
+__device__ __forceinline__ void prefetch_l2_bulk(uintptr_t p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Streams a box's contiguous M2L region into L2 ahead of the warp that
+// consumes it in order: `advance(pos)` keeps the prefetched front kAhead bytes
+// beyond `pos`, in kStep pieces (the last piece may extend < 16 bytes past the
+// region; the block allocation is padded for that).
+struct L2Stream {
+  static constexpr uintptr_t kAhead = 24 * 1024, kStep = 4096;
+  uintptr_t front, end;
+  __device__ __forceinline__ L2Stream(const double* begin, const double* stop)
+      : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop) {}
+  __device__ __forceinline__ void advance(const double* pos, int lane) {
+    uintptr_t upto = (uintptr_t)pos + kAhead;
+    if (upto > end) upto = end;
+    while (front < upto) {  // warp-uniform
+      if (lane == 0) {
+        const uintptr_t left = (end - front + 15) & ~(uintptr_t)15;
+        prefetch_l2_bulk(front, (uint32_t)(left < kStep ? left : kStep));
+      }
+      front += kStep;
+    }
+  }
+};
+
 // M2L from the stored FP64 blocks (the same blocks the FP64 path applies)
-// with FP64 tensor-core tiles: one warp per chunk of up to kChunkRows skeleton rows of
-// one box, i.e. NT <= 5 tiles of 8 rows that share every B fragment.  The 40
-// slots' rank and skeleton offset are fetched once per warp and broadcast by
-// shuffles.
+// with FP64 tensor-core tiles: one warp per chunk of up to kChunkRows skeleton
+// rows of one box, i.e. NT <= 5 tiles of 8 rows that share every B fragment.
+// The 40 slots' rank and skeleton offset are fetched once per warp and
+// broadcast by shuffles; the box's contiguous block region is streamed into
+// L2 ahead of the loads.
 template <int RC, int NT>
 __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const double* __restrict__ qh,
                                                  double* __restrict__ yb, int b, int r0, int lane) {
@@ -460,15 +489,17 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
   bool rowok[NT];
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
-  const double* M = v.m2l + v.m2l_off[b] + i0 + trow;
+  const double* Mb = v.m2l + v.m2l_off[b];  // block of the current slot
+  L2Stream pf(Mb, v.m2l + v.m2l_off[b + 1]);
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   for (int s = 0; s < 40; ++s) {
     const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
     if (rc == 0) continue;  // empty slot or rank-0 box: no block stored
     const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
-    mma_rows<RC, NT>(c, M, r, rc, qh + (long)sc * RC, rowok, trow, tsrc);
-    M += (long)r * rc;
+    pf.advance(Mb, lane);
+    mma_rows<RC, NT>(c, Mb + i0 + trow, r, rc, qh + (long)sc * RC, rowok, trow, tsrc);
+    Mb += (long)r * rc;
   }
   store_tiles<RC, NT, false>(c, yb + (long)r0 * RC, rowok, trow, tsrc);
 }

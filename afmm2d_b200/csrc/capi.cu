@@ -434,7 +434,7 @@ void do_assemble(afmm_handle* h) {
     m2l_total += v.h_m2l_off[v.nbox];
     v.m2l_off = h->arena.alloc<int64_t>(v.nbox + 1);
     AFMM_CUDA(cudaMemcpyAsync(v.m2l_off, v.h_m2l_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
-    v.m2l = h->arena.alloc<double>(v.h_m2l_off[v.nbox]);
+    v.m2l = h->arena.alloc<double>(v.h_m2l_off[v.nbox] + 32);  // + 256 B for whole-piece L2 prefetches
     v.qhat = h->arena.alloc<double>(v.total_rank);
     v.yhat = h->arena.alloc<double>(v.total_rank);
     // row -> box maps for the thread-per-row sweeps
