@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--N", type=int, default=None, help="override N (same distribution)")
     ap.add_argument("--nrhs", type=int, default=16, help="right-hand sides of the batched (headline) path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=CPU_SAMPLE_N,
+                    help="points of the reference CPU run (the workload's N: full size, with a parity check of the "
+                         "FP64 GPU result against the reference's output)")
     ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
     return ap.parse_args()
 
@@ -133,6 +136,8 @@ def cpu_reference(name, n, steps, warmup):
     if not RefLib.available():
         return None
     pts, q, p = workloads.make(name, N=n)
+    if q.ndim > 1:
+        q = np.ascontiguousarray(q[:, 0])
     t0 = time.perf_counter()
     r = RefLib(pts, p["M"], p["tol"], p["kernel"])
     r.assemble()
@@ -141,13 +146,13 @@ def cpu_reference(name, n, steps, warmup):
         r.matvec(q)
     t0 = time.perf_counter()
     for _ in range(steps):
-        r.matvec(q)
+        y = r.matvec(q)
     dt = (time.perf_counter() - t0) / steps
     threads = r.lib.ref_num_threads()
     return {"value": n / dt, "unit": UNIT, "cores": int(threads), "kind": "reference",
             "sample": f"{name} at N={n} (same distribution, kernel, M, TOL), {steps} matvecs after {warmup} "
                       f"warm-up, OpenMP {threads} threads; reference setup {setup:.1f} s",
-            "ms_per_step": dt * 1e3, "setup_s": setup}
+            "ms_per_step": dt * 1e3, "setup_s": setup, "y": y}
 
 
 def run_reference(args):
@@ -327,9 +332,16 @@ def run_ours(args):
             "e2e": {"value": world * N * R / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N * R,
                     "d2h_bytes_per_step": 8 * N * R, "ms_per_step": t_e2e * 1e3, "nrhs": R}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_reference(args.workload, CPU_SAMPLE_N, 5, 1)
+        full = args.cpu_sample >= N
+        # a bounded sample: a few matvecs of the 65,536-point default; one at full size
+        cb = cpu_reference(args.workload, min(args.cpu_sample, N), 1 if full else 5, 0 if full else 1)
         if cb:
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            line["cpu_baseline"]["setup_s"] = cb["setup_s"]
+            line["fp64_gpu_vs_cpu_reference_matvec"] = (N / (t_dev["fp64"] * 1e-3)) / cb["value"]
+            if full:
+                yr = cb["y"]
+                line["rel_err_fp64_vs_reference"] = float(np.linalg.norm(y64[:, 0] - yr) / np.linalg.norm(yr))
     if dist:
         dist.barrier()
         dist.destroy_process_group()
