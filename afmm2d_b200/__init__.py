@@ -18,7 +18,7 @@ import os
 
 import numpy as np
 
-__all__ = ["AFMM", "AFMMError", "KERNELS", "PRECISIONS", "kernel_eval", "lib", "nlevels"]
+__all__ = ["AFMM", "AFMMError", "AFMMSet", "KERNELS", "PRECISIONS", "kernel_eval", "lib", "nlevels"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafmm2d.so")
@@ -53,6 +53,12 @@ _SIGS = {
     "afmm_measure_fma_peaks": [_vp, _vp],
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_destroy": [_vp],
+    "afmm_set_create": [_vp, _i, _vp],
+    "afmm_set_matvec": [_vp, _vp, _vp, _i],
+    "afmm_set_get_offsets": [_vp, _vp],
+    "afmm_set_get_launches": [_vp, _vp, _vp],
+    "afmm_set_get_stream": [_vp, _vp],
+    "afmm_set_destroy": [_vp],
 }
 _lib = None
 
@@ -76,6 +82,8 @@ def lib():
             f.restype = _i
         L.afmm_last_error.argtypes = [_vp]
         L.afmm_last_error.restype = ctypes.c_char_p
+        L.afmm_set_last_error.argtypes = [_vp]
+        L.afmm_set_last_error.restype = ctypes.c_char_p
         L.afmm_status_string.argtypes = [_i]
         L.afmm_status_string.restype = ctypes.c_char_p
         L.afmm_version.restype = ctypes.c_char_p
@@ -271,6 +279,65 @@ class AFMM:
         if getattr(self, "_h", None):
             lib().afmm_destroy(self._h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class AFMMSet:
+    """Many assembled ``AFMM`` problems applied in one call: every stage of
+    the FP64 matvec is one fused launch over all problems, recorded once in a
+    CUDA graph and replayed per call.  Each problem's result has the same bits
+    as its own ``computeMatVecProduct(q, "fp64")``.  The problems stay owned
+    by the caller and must outlive the set."""
+
+    def __init__(self, problems):
+        self.problems = list(problems)
+        arr = (ctypes.c_void_p * len(self.problems))(*[p._h.value for p in self.problems])
+        h = ctypes.c_void_p()
+        _check(lib().afmm_set_create(arr, len(self.problems), ctypes.byref(h)))
+        self._h = h
+        self.offsets = np.zeros(len(self.problems) + 1, np.int64)
+        self._call("afmm_set_get_offsets", _ptr(self.offsets))
+        self.total = int(self.offsets[-1])
+
+    def _call(self, name, *args):
+        st = getattr(lib(), name)(self._h, *args)
+        if st != 0:
+            raise AFMMError(st, lib().afmm_set_last_error(self._h).decode())
+
+    def matvec(self, qs):
+        """qs: list of per-problem charge vectors (original point order) or
+        one concatenated vector; returns the list of potentials."""
+        q = np.ascontiguousarray(np.concatenate(qs) if isinstance(qs, (list, tuple)) else qs, dtype=np.float64)
+        if q.shape != (self.total,):
+            raise ValueError(f"need {self.total} charges in total")
+        y = np.zeros(self.total)
+        self._call("afmm_set_matvec", _ptr(q), _ptr(y), 0)
+        return [y[self.offsets[p]:self.offsets[p + 1]] for p in range(len(self.problems))]
+
+    def matvec_device(self, q_ptr, y_ptr):
+        """Concatenated charges / potentials in device memory (raw pointers)."""
+        self._call("afmm_set_matvec", ctypes.c_void_p(q_ptr), ctypes.c_void_p(y_ptr), 1)
+
+    def launches(self):
+        """(fused launches per matvec recorded in the graph, graph launches so far)"""
+        a, b = ctypes.c_int(), ctypes.c_int64()
+        self._call("afmm_set_get_launches", ctypes.byref(a), ctypes.byref(b))
+        return a.value, b.value
+
+    def stream(self):
+        s = ctypes.c_void_p()
+        self._call("afmm_set_get_stream", ctypes.byref(s))
+        return s.value
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().afmm_set_destroy(self._h)
+            self._h = ctypes.c_void_p()
 
     def __del__(self):
         try:

@@ -11,7 +11,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libafmm2d.so")
-SOURCES = ["kd_sort.cu", "aca.cu", "fmm.cu", "mixed.cu", "batched.cu", "capi.cu"]
+SOURCES = ["kd_sort.cu", "aca.cu", "fmm.cu", "mixed.cu", "batched.cu", "set.cu", "capi.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -13,11 +13,22 @@
 #include "fmm.cuh"
 #include "kd_sort.cuh"
 #include "mixed.cuh"
+#include "set.cuh"
 
 using namespace afmm;
 
+struct afmm_set {
+  SetPlan plan;
+  DevArena arena;
+  cudaStream_t stream = nullptr;
+  std::vector<int64_t> offsets;
+  int64_t graph_launches = 0;
+  std::string err;
+};
+
 struct afmm_handle {
   int N = 0, M = 0, tol_pow = 0, L = 0, kernel_id = 0;
+  int device = 0;
   KernelParams kp{};
   cudaStream_t stream = nullptr;
   DevArena arena;
@@ -289,6 +300,7 @@ void do_create(afmm_handle* h, const double* loc, int layout) {
     if (nmax > 1024) throw Error{AFMM_BAD_ARG, "leaf size " + std::to_string(nmax) + " exceeds 1024; use a smaller M"};
   }
   check_device();
+  AFMM_CUDA(cudaGetDevice(&h->device));
   AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   cudaStream_t s = h->stream;
   double* d_xy = h->arena.alloc<double>(2 * (size_t)N);
@@ -842,6 +854,89 @@ afmm_status afmm_destroy(afmm_handle* h) {
   if (s) cudaStreamDestroy(s);
   return AFMM_OK;
 }
+
+afmm_status afmm_set_create(afmm_handle* const* handles, int n, afmm_set** out) {
+  if (!out) return AFMM_BAD_ARG;
+  *out = nullptr;
+  afmm_set* st = nullptr;
+  afmm_status rc = guard(nullptr, [&] {
+    check_device();
+    if (!handles || n < 1) throw Error{AFMM_BAD_ARG, "afmm_set_create: need n >= 1 handles"};
+    std::vector<SetProblem> probs;
+    int dev = -1;
+    AFMM_CUDA(cudaGetDevice(&dev));
+    for (int p = 0; p < n; ++p) {
+      afmm_handle* h = handles[p];
+      if (!h) throw Error{AFMM_BAD_ARG, "afmm_set_create: null handle"};
+      if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_set_create: handle not assembled"};
+      if (h->kernel_id != handles[0]->kernel_id) throw Error{AFMM_BAD_ARG, "afmm_set_create: mixed kernel ids"};
+      if (h->device != dev) throw Error{AFMM_BAD_ARG, "afmm_set_create: handle on another device"};
+      probs.push_back({&h->plan, p2p_shape(h->plan.near.nmax)});
+    }
+    st = new afmm_set();
+    AFMM_CUDA(cudaStreamCreateWithFlags(&st->stream, cudaStreamNonBlocking));
+    for (int p = 0; p < n; ++p) AFMM_CUDA(cudaStreamSynchronize(handles[p]->stream));
+    st->plan.kernel_id = handles[0]->kernel_id;
+    set_build(st->plan, probs, st->arena, st->stream);
+    st->offsets.resize(n + 1, 0);
+    for (int p = 0; p < n; ++p) st->offsets[p + 1] = st->offsets[p] + handles[p]->N;
+  });
+  if (rc != AFMM_OK) {
+    if (st) afmm_set_destroy(st);
+    return rc;
+  }
+  *out = st;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_matvec(afmm_set* st, const double* q, double* y, int mem_device) {
+  if (!st) return AFMM_BAD_ARG;
+  try {
+    if (!q || !y) throw Error{AFMM_BAD_ARG, "afmm_set_matvec: null q/y"};
+    cudaStream_t s = st->stream;
+    const size_t bytes = sizeof(double) * (size_t)st->plan.total_points;
+    AFMM_CUDA(cudaMemcpyAsync(st->plan.q, q, bytes, mem_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s));
+    set_matvec(st->plan, s);
+    ++st->graph_launches;
+    AFMM_CUDA(cudaMemcpyAsync(y, st->plan.y, bytes, mem_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
+    AFMM_CUDA(cudaStreamSynchronize(s));
+    return AFMM_OK;
+  } catch (const Error& e) {
+    st->err = e.msg;
+    return e.status;
+  }
+}
+
+afmm_status afmm_set_get_offsets(afmm_set* st, int64_t* offsets) {
+  if (!st || !offsets) return AFMM_BAD_ARG;
+  std::copy(st->offsets.begin(), st->offsets.end(), offsets);
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_get_launches(afmm_set* st, int* per_matvec, int64_t* graph_launches) {
+  if (!st) return AFMM_BAD_ARG;
+  if (per_matvec) *per_matvec = st->plan.launches_per_matvec;
+  if (graph_launches) *graph_launches = st->graph_launches;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_get_stream(afmm_set* st, void** stream) {
+  if (!st || !stream) return AFMM_BAD_ARG;
+  *stream = (void*)st->stream;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_destroy(afmm_set* st) {
+  if (!st) return AFMM_OK;
+  if (st->stream) cudaStreamSynchronize(st->stream);
+  set_release(st->plan);
+  cudaStream_t s = st->stream;
+  delete st;
+  if (s) cudaStreamDestroy(s);
+  return AFMM_OK;
+}
+
+const char* afmm_set_last_error(afmm_set* st) { return st ? st->err.c_str() : g_err.c_str(); }
 
 const char* afmm_status_string(afmm_status s) {
   switch (s) {

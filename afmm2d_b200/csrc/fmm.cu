@@ -141,29 +141,12 @@ __global__ void k_scatter(const double* __restrict__ ys, const int64_t* __restri
   if (i < n) y[perm[i]] = ys[i];
 }
 
-// M2M (src/AFMM2DTree.cpp:1129-1154): qhat_b = L2P_b^T src_b.  One thread per
-// output (skeleton row of the level), summing over the box's node rows on
-// the row-major copy of L2P (a warp's consecutive outputs read contiguously).
-// src_b = leaf charges, or the concatenated outgoing charges of children 0..3.
+// M2M (src/AFMM2DTree.cpp:1129-1154): one thread per output (skeleton row of
+// the level), a warp's consecutive outputs reading the row-major L2P
+// contiguously.
 __global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
   const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= v.nrows) return;
-  const int b = v.skel_box[row];
-  const int r = v.rank[b];
-  const int c = (int)(row - v.skel_off[b]);
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
-  const double* P = v.l2p_rm + v.l2p_off[b] + c;  // (i, c) at i*r + c
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int i = 0;
-  for (; i + 3 < n; i += 4) {
-    a0 += P[(long)i * r] * src[i];
-    a1 += P[(long)(i + 1) * r] * src[i + 1];
-    a2 += P[(long)(i + 2) * r] * src[i + 2];
-    a3 += P[(long)(i + 3) * r] * src[i + 3];
-  }
-  for (; i < n; ++i) a0 += P[(long)i * r] * src[i];
-  v.qhat[row] = (a0 + a1) + (a2 + a3);
+  if (row < v.nrows) m2m_row(v, src_all, leaf, row);
 }
 
 // Row-major copy of L2P (per box, r fastest) for the M2M sweep.
@@ -193,135 +176,27 @@ __device__ __forceinline__ int level_of_row(const LevelSet& ls, long g) {
 }
 
 // M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch, one thread
-// per skeleton row (upper levels first): row i of box b sums, slot by slot in
-// the reference's order (inner 0..15, outer 0..23), row i of the stored block
-// M2L[b][c] (column-major: a warp's consecutive rows read contiguously) times
-// the outgoing charges of c.
+// per skeleton row (upper levels first); the column-major blocks let a warp's
+// consecutive rows read contiguously.
 __global__ void k_m2l_apply(LevelSet ls) {
   const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= ls.row0[ls.nlev]) return;
-  const LevelView& v = ls.lv[level_of_row(ls, g)];
-  const long row = g - ls.row0[level_of_row(ls, g)];
-  const int b = v.skel_box[row];
-  const int r = v.rank[b];
-  const int i = (int)(row - v.skel_off[b]);
-  const double* M = v.m2l + v.m2l_off[b] + i;
-  double acc = 0.0;
-  for (int s = 0; s < 40; ++s) {
-    const int c = v.il[(long)b * 40 + s];
-    if (c < 0) continue;
-    const int rc = v.rank[c];
-    const double* qc = v.qhat + v.skel_off[c];
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int cc = 0;
-    for (; cc + 3 < rc; cc += 4) {
-      a0 += M[(long)cc * r] * qc[cc];
-      a1 += M[(long)(cc + 1) * r] * qc[cc + 1];
-      a2 += M[(long)(cc + 2) * r] * qc[cc + 2];
-      a3 += M[(long)(cc + 3) * r] * qc[cc + 3];
-    }
-    for (; cc < rc; ++cc) a0 += M[(long)cc * r] * qc[cc];
-    acc += (a0 + a1) + (a2 + a3);
-    M += (long)r * rc;
-  }
-  v.yhat[row] = acc;
+  const int j = level_of_row(ls, g);
+  m2l_row(ls.lv[j], g - ls.row0[j]);
 }
 
-// L2L (src/AFMM2DTree.cpp:1180-1197): t = L2P_b yhat_b, one thread per node
-// row of the level (column-major L2P: a warp's consecutive rows read
-// contiguously); added to the child's incoming potential (node row g of
-// level j is skeleton row g of level j+1), or written as the leaf potential.
+// L2L (src/AFMM2DTree.cpp:1180-1197): one thread per node row of the level.
 __global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
   const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= v.nnodes) return;
-  const int b = v.node_box[g];
-  const int r = v.rank[b];
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const int i = (int)(g - v.node_off[b]);
-  const double* P = v.l2p + v.l2p_off[b] + i;  // (i, c) at c*n + i
-  const double* yb = v.yhat + v.skel_off[b];
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-  int c = 0;
-  for (; c + 3 < r; c += 4) {
-    a0 += P[(long)c * n] * yb[c];
-    a1 += P[(long)(c + 1) * n] * yb[c + 1];
-    a2 += P[(long)(c + 2) * n] * yb[c + 2];
-    a3 += P[(long)(c + 3) * n] * yb[c + 3];
-  }
-  for (; c < r; ++c) a0 += P[(long)c * n] * yb[c];
-  const double t = (a0 + a1) + (a2 + a3);
-  if (leaf) ys[v.leaf_start[b] + i] = t;
-  else child_yhat[g] += t;
+  if (g < v.nnodes) l2l_row(v, child_yhat, ys, leaf, g);
 }
 
-// Near field (src/AFMM2DTree.cpp:1199-1213): per leaf, neighbours 0..7 and
-// the leaf itself, kernel evaluated on the fly.  One CTA per leaf; all source
-// leaves are staged in shared memory at once; G groups of NT threads split
-// the source leaves (group g takes leaves g, g+G, ...), each thread owns one
-// target, and the groups' sums are added in group order.
+// Near field (src/AFMM2DTree.cpp:1199-1213): one CTA per leaf.
 template <class K>
 __global__ void k_p2p64(NearView nv, KernelParams kp, const double* __restrict__ qs, double* __restrict__ ys, int NT,
                         int G) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
-  const long b = blockIdx.x;
-  const int n = nv.leaf_cnt[b];
-  const int s0 = nv.leaf_start[b];
-  if (threadIdx.x == 0) {
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (c < 0) continue;
-      s_src[m] = nv.leaf_start[c];
-      s_cnt[m] = nv.leaf_cnt[c];
-      s_off[m] = off;
-      off += nv.leaf_cnt[c];
-      ++m;
-    }
-    s_off[m] = off;
-    s_ns = m;
-  }
-  __syncthreads();
-  const int ns = s_ns, tot = s_off[ns];
-  double2* sx = (double2*)smem;
-  double* sq = (double*)(sx + 9 * nv.nmax);
-  double* red = sq + 9 * nv.nmax;  // G x NT
-  for (int m = 0; m < ns; ++m)
-    for (int t = threadIdx.x; t < s_cnt[m]; t += blockDim.x) {
-      sx[s_off[m] + t] = nv.pts[s_src[m] + t];
-      sq[s_off[m] + t] = qs[s_src[m] + t];
-    }
-  __syncthreads();
-  (void)tot;
-  const int i = threadIdx.x % NT, g = threadIdx.x / NT;
-  double acc = 0.0;
-  if (i < n) {
-    const double2 xi = nv.pts[s0 + i];
-    for (int m = g; m < ns; m += G) {
-      const int o = s_off[m], nc = s_cnt[m];
-      double a0 = 0.0, a1 = 0.0;
-      int t = 0;
-      for (; t + 1 < nc; t += 2) {
-        const double2 p0 = sx[o + t], p1 = sx[o + t + 1];
-        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y, dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
-        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
-        a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * sq[o + t + 1];
-      }
-      if (t < nc) {
-        const double2 p0 = sx[o + t];
-        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
-        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
-      }
-      acc += a0 + a1;
-    }
-  }
-  red[g * NT + i] = acc;
-  __syncthreads();
-  if (g == 0 && i < n) {
-    double s = ys[s0 + i];
-    for (int h = 0; h < G; ++h) s += red[h * NT + i];
-    ys[s0 + i] = s;
-  }
+  p2p64_leaf<K>(nv, kp, qs, ys, NT, G, blockIdx.x, smem);
 }
 
 template <class K>

@@ -11,11 +11,6 @@
 namespace afmm {
 
 constexpr int kMaxLevels = 16;
-// CTA shape of the per-box sweep kernels.
-constexpr int SW_T = 256;
-constexpr int SW_WARPS = SW_T / 32;
-// threads for a per-box kernel whose work runs over up to n rows
-inline int sweep_threads(int n) { return n <= 64 ? 64 : (n <= 128 ? 128 : 256); }
 
 // Allows `bytes` of dynamic shared memory for kernel `fn` (needed above 48 KB).
 template <class F>
@@ -129,20 +124,6 @@ struct MatvecPlan {
   NearView near;
 };
 
-// M2L kernels work on (slot, row) items; rows are processed in chunks of at
-// most M2L_RCH so that the per-slot partial sums (40 x M2L_RCH doubles) fit
-// in shared memory.
-constexpr int M2L_RCH = 256;
-
-// Valid interaction-list slots of a box, staged by one thread.
-struct SlotTable {
-  int n;
-  int box[40];
-  int rank[40];
-  int skel[40];
-  long off[40];  // block offset within the box's M2L data (stored form)
-};
-
 // Near-field launch shape: NT threads per target group (targets rounded up to
 // a warp multiple), G groups splitting the (up to 9) source leaves.
 struct P2pShape {
@@ -154,6 +135,156 @@ inline P2pShape p2p_shape(int nmax) {
   p.g = std::max(1, std::min(9, 256 / p.nt));
   p.threads = p.nt * p.g;
   return p;
+}
+
+// ------------------------------------------------ FP64 sweep rows
+// The arithmetic of one output of each FP64 sweep, shared by the
+// single-problem kernels (fmm.cu) and the fused many-problem kernels (set.cu)
+// so both give the same bits.
+
+// M2M (src/AFMM2DTree.cpp:1129-1154): qhat[row] = (L2P_b^T src_b)[row] over
+// the row-major L2P copy; src_b = leaf charges, or the concatenated outgoing
+// charges of children 0..3.
+__device__ __forceinline__ void m2m_row(const LevelView& v, const double* __restrict__ src_all, int leaf, long row) {
+  const int b = v.skel_box[row];
+  const int r = v.rank[b];
+  const int c = (int)(row - v.skel_off[b]);
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
+  const double* P = v.l2p_rm + v.l2p_off[b] + c;  // (i, c) at i*r + c
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int i = 0;
+  for (; i + 3 < n; i += 4) {
+    a0 += P[(long)i * r] * src[i];
+    a1 += P[(long)(i + 1) * r] * src[i + 1];
+    a2 += P[(long)(i + 2) * r] * src[i + 2];
+    a3 += P[(long)(i + 3) * r] * src[i + 3];
+  }
+  for (; i < n; ++i) a0 += P[(long)i * r] * src[i];
+  v.qhat[row] = (a0 + a1) + (a2 + a3);
+}
+
+// M2L (src/AFMM2DTree.cpp:1156-1178): row i of box b sums, slot by slot in
+// the reference's order (inner 0..15, outer 0..23), row i of the stored block
+// M2L[b][c] (column-major) times the outgoing charges of c.
+__device__ __forceinline__ void m2l_row(const LevelView& v, long row) {
+  const int b = v.skel_box[row];
+  const int r = v.rank[b];
+  const int i = (int)(row - v.skel_off[b]);
+  const double* M = v.m2l + v.m2l_off[b] + i;
+  double acc = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int c = v.il[(long)b * 40 + s];
+    if (c < 0) continue;
+    const int rc = v.rank[c];
+    const double* qc = v.qhat + v.skel_off[c];
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int cc = 0;
+    for (; cc + 3 < rc; cc += 4) {
+      a0 += M[(long)cc * r] * qc[cc];
+      a1 += M[(long)(cc + 1) * r] * qc[cc + 1];
+      a2 += M[(long)(cc + 2) * r] * qc[cc + 2];
+      a3 += M[(long)(cc + 3) * r] * qc[cc + 3];
+    }
+    for (; cc < rc; ++cc) a0 += M[(long)cc * r] * qc[cc];
+    acc += (a0 + a1) + (a2 + a3);
+    M += (long)r * rc;
+  }
+  v.yhat[row] = acc;
+}
+
+// L2L (src/AFMM2DTree.cpp:1180-1197): t = (L2P_b yhat_b)[node row g] over the
+// column-major L2P, added to the child's incoming potential (node row g of
+// level j is skeleton row g of level j+1), or written as the leaf potential.
+__device__ __forceinline__ void l2l_row(const LevelView& v, double* __restrict__ child_yhat, double* __restrict__ ys,
+                                        int leaf, long g) {
+  const int b = v.node_box[g];
+  const int r = v.rank[b];
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const int i = (int)(g - v.node_off[b]);
+  const double* P = v.l2p + v.l2p_off[b] + i;  // (i, c) at c*n + i
+  const double* yb = v.yhat + v.skel_off[b];
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  int c = 0;
+  for (; c + 3 < r; c += 4) {
+    a0 += P[(long)c * n] * yb[c];
+    a1 += P[(long)(c + 1) * n] * yb[c + 1];
+    a2 += P[(long)(c + 2) * n] * yb[c + 2];
+    a3 += P[(long)(c + 3) * n] * yb[c + 3];
+  }
+  for (; c < r; ++c) a0 += P[(long)c * n] * yb[c];
+  const double t = (a0 + a1) + (a2 + a3);
+  if (leaf) ys[v.leaf_start[b] + i] = t;
+  else child_yhat[g] += t;
+}
+
+// Near field (src/AFMM2DTree.cpp:1199-1213) of leaf b: neighbours 0..7 and the
+// leaf itself, kernel evaluated on the fly.  Run by one CTA of at least
+// NT * G threads: all source leaves are staged in shared memory (`smem`:
+// 9 * nmax double2 + 9 * nmax double + NT * G double); G groups of NT
+// threads split the source leaves (group g takes leaves g, g+G, ...), each
+// thread owns one target, and the groups' sums are added in group order.
+template <class K>
+__device__ __forceinline__ void p2p64_leaf(const NearView& nv, const KernelParams& kp, const double* __restrict__ qs,
+                                           double* __restrict__ ys, int NT, int G, long b, unsigned char* smem) {
+  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
+  const int n = nv.leaf_cnt[b];
+  const int s0 = nv.leaf_start[b];
+  if (threadIdx.x == 0) {
+    int m = 0, off = 0;
+    for (int slot = 0; slot < 9; ++slot) {
+      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
+      if (c < 0) continue;
+      s_src[m] = nv.leaf_start[c];
+      s_cnt[m] = nv.leaf_cnt[c];
+      s_off[m] = off;
+      off += nv.leaf_cnt[c];
+      ++m;
+    }
+    s_off[m] = off;
+    s_ns = m;
+  }
+  __syncthreads();
+  const int ns = s_ns;
+  double2* sx = (double2*)smem;
+  double* sq = (double*)(sx + 9 * nv.nmax);
+  double* red = sq + 9 * nv.nmax;  // G x NT
+  for (int m = 0; m < ns; ++m)
+    for (int t = threadIdx.x; t < s_cnt[m]; t += blockDim.x) {
+      sx[s_off[m] + t] = nv.pts[s_src[m] + t];
+      sq[s_off[m] + t] = qs[s_src[m] + t];
+    }
+  __syncthreads();
+  const bool active = (int)threadIdx.x < NT * G;
+  const int i = threadIdx.x % NT, g = threadIdx.x / NT;
+  double acc = 0.0;
+  if (active && i < n) {
+    const double2 xi = nv.pts[s0 + i];
+    for (int m = g; m < ns; m += G) {
+      const int o = s_off[m], nc = s_cnt[m];
+      double a0 = 0.0, a1 = 0.0;
+      int t = 0;
+      for (; t + 1 < nc; t += 2) {
+        const double2 p0 = sx[o + t], p1 = sx[o + t + 1];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y, dx1 = xi.x - p1.x, dy1 = xi.y - p1.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
+        a1 += K::eval(dx1 * dx1 + dy1 * dy1, kp) * sq[o + t + 1];
+      }
+      if (t < nc) {
+        const double2 p0 = sx[o + t];
+        const double dx0 = xi.x - p0.x, dy0 = xi.y - p0.y;
+        a0 += K::eval(dx0 * dx0 + dy0 * dy0, kp) * sq[o + t];
+      }
+      acc += a0 + a1;
+    }
+  }
+  if (active) red[g * NT + i] = acc;
+  __syncthreads();
+  if (active && g == 0 && i < n) {
+    double s = ys[s0 + i];
+    for (int h = 0; h < G; ++h) s += red[h * NT + i];
+    ys[s0 + i] = s;
+  }
 }
 
 void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);

@@ -1,0 +1,62 @@
+// A set of independent assembled problems applied together: every stage of
+// the FP64 matvec runs as one fused launch over all problems, and the whole
+// sequence is captured once in a CUDA graph.
+#pragma once
+#include <vector>
+
+#include "fmm.cuh"
+
+namespace afmm {
+
+// Device tables of the set (pointers to device memory), passed by value.
+struct SetDev {
+  int nprob = 0;
+  const LevelView* lv = nullptr;    // nprob x kMaxLevels, level j of problem p at p*kMaxLevels + j
+  const NearView* nv = nullptr;     // nprob
+  const KernelParams* kp = nullptr; // nprob
+  const int2* p2p = nullptr;        // nprob: near-field launch shape (NT, G)
+  const int64_t* const* perm = nullptr;  // nprob: sorted -> original index
+  double* const* qs = nullptr;      // nprob: sorted charges
+  double* const* ys = nullptr;      // nprob: sorted potentials
+  const int64_t* off = nullptr;     // nprob + 1: problem p's points at [off[p], off[p+1]) of the set vectors
+};
+
+// Work items of one fused launch: segment s covers items [first[s], first[s+1])
+// of problem prob[s] at level level[s].
+struct SetSegs {
+  const int64_t* first = nullptr;  // n + 1
+  const int32_t* prob = nullptr;
+  const int32_t* level = nullptr;
+  int n = 0;
+  long total = 0;
+};
+
+// Host description of one problem of the set.
+struct SetProblem {
+  const MatvecPlan* plan;
+  P2pShape shape;
+};
+
+struct SetPlan {
+  SetDev dev;
+  int kernel_id = 0;
+  long total_points = 0;
+  int p2p_threads = 0;
+  size_t p2p_smem = 0;
+  SetSegs gather, m2l, p2p;
+  std::vector<SetSegs> m2m;  // by depth below each problem's leaf level
+  std::vector<SetSegs> l2l;  // by level 2, 3, ...
+  double* q = nullptr;       // set input (original order, problems concatenated)
+  double* y = nullptr;       // set output
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int launches_per_matvec = 0;
+};
+
+// Builds the device tables (allocated from `arena`) and the graph on stream s.
+void set_build(SetPlan& sp, const std::vector<SetProblem>& probs, DevArena& arena, cudaStream_t s);
+// One FP64 matvec of every problem: sp.q -> sp.y (graph replay on s).
+void set_matvec(SetPlan& sp, cudaStream_t s);
+void set_release(SetPlan& sp);
+
+}  // namespace afmm

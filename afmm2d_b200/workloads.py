@@ -80,3 +80,18 @@ def make(name, N=None, seed=None, nrhs=None):
 def many_sizes(count=256, nmin=2048, nmax=65536, seed=0xAF3D2D05):
     rng = np.random.Generator(np.random.PCG64(seed))
     return np.round(np.exp(rng.uniform(np.log(nmin), np.log(nmax), size=count))).astype(np.int64)
+
+
+def many_problems(count=256, nmin=2048, nmax=65536, seed=0xAF3D2D05):
+    """The many-problem workload: `count` independent problems, N log-uniform
+    in [nmin, nmax] (many_sizes), points uniform in [0,1]^2, charges N(0,1);
+    problem k draws from its own stream (seed + 1 + k).  Returns a list of
+    (points, charges) and the shared parameters (log, M = 32, TOL 8)."""
+    p = dict(WORKLOADS["many"])
+    sizes = many_sizes(count, nmin, nmax, seed)
+    probs = []
+    for k, n in enumerate(sizes):
+        rng = np.random.Generator(np.random.PCG64(seed + 1 + k))
+        pts = uniform(int(n), 0.0, 1.0, rng)
+        probs.append((np.ascontiguousarray(pts), rng.standard_normal(int(n))))
+    return probs, p

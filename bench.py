@@ -350,10 +350,151 @@ def run_ours(args):
     a.close()
 
 
+def run_many(args):
+    """The many-problem workload: 256 independent problems (N log-uniform in
+    2,048..65,536, uniform points, log, M = 32, TOL 8).  One step = one FP64
+    matvec of every problem through AFMMSet (fused launches replayed from one
+    CUDA graph); a loop of per-problem FP64 matvecs is timed beside it."""
+    import torch
+    import afmm2d_b200 as A
+    from afmm2d_b200 import workloads
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    probs, p = workloads.many_problems()
+    t0 = time.perf_counter()
+    hs = []
+    for pts, _ in probs:
+        h = A.AFMM(len(pts), p["M"], p["tol"], pts, kernel=p["kernel"])
+        h.assemble()
+        hs.append(h)
+    st = A.AFMMSet(hs)
+    setup_s = time.perf_counter() - t0
+    total = st.total
+    dev = f"cuda:{local}"
+    q = torch.from_numpy(np.concatenate([qk for _, qk in probs])).to(dev)
+    y = torch.empty_like(q)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.ExternalStream(st.stream())
+
+    def timed(fn, s):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            with torch.cuda.stream(s):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms))
+
+    if dist:
+        dist.barrier()
+    clk = ClockSampler(local)
+    clk.start()
+    t_set = timed(lambda: st.matvec_device(q.data_ptr(), y.data_ptr()), stream)
+    # per-problem loop: each handle's own FP64 matvec through the C ABI (each
+    # call runs on its handle's stream and returns when done: wall clock)
+    offs = st.offsets
+    esz = q.element_size()
+
+    def loop():
+        for k, h in enumerate(hs):
+            h.matvec_device(q.data_ptr() + esz * int(offs[k]), y.data_ptr() + esz * int(offs[k]), 1, h.N, "fp64")
+
+    for _ in range(args.warmup):
+        loop()
+    torch.cuda.synchronize()
+    tl = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loop()
+        tl.append(time.perf_counter() - t1)
+    t_loop = float(np.mean(tl)) * 1e3
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    hq = q.cpu().pin_memory()
+    hy = torch.empty_like(hq).pin_memory()
+    for _ in range(args.warmup):
+        st._call("afmm_set_matvec", ctypes.c_void_p(hq.data_ptr()), ctypes.c_void_p(hy.data_ptr()), 0)
+    e2e = []
+    for _ in range(max(args.steps, 1)):
+        t1 = time.perf_counter()
+        st._call("afmm_set_matvec", ctypes.c_void_p(hq.data_ptr()), ctypes.c_void_p(hy.data_ptr()), 0)
+        e2e.append(time.perf_counter() - t1)
+    t_e2e = float(np.mean(e2e))
+    # one problem's set output against its own FP64 matvec
+    yk = hs[0].computeMatVecProduct(probs[0][1], "fp64")
+    same = bool(np.array_equal(hy.numpy()[offs[0]:offs[1]], yk))
+    red = max_over_ranks([t_set, t_loop, t_e2e], dist, dev)
+    t_set, t_loop, t_e2e = red
+    per, _ = st.launches()
+    c = np.sum([h.counts()["m2l_entries"] for h in hs]), np.sum([h.counts()["l2p_entries"] for h in hs])
+    hbm, _, peak_kind = load_peaks()
+    byts = float(c[0] * 8 + c[1] * 8 * 2)
+    line = {"metric": "points/s per FP64 matvec of 256 independent problems (N 2,048..65,536, log, TOL 8)",
+            "value": world * total / (t_set * 1e-3), "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_set, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+            "config": {"workload": "many", "problems": len(hs), "points": total, "kernel": p["kernel"],
+                       "M": p["M"], "TOL_POW": p["tol"], "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"replicas x{world}"},
+            "loop_ms_per_step": t_loop, "loop_timing": "wall clock of 256 afmm_matvec FP64 calls",
+            "speedup_set_vs_loop": t_loop / t_set,
+            "set_output_equals_own_fp64_matvec": same, "setup_s": setup_s,
+            "gpu_launches": per, "graph_launches_per_step": 1,
+            "roofline": {"bound": "hbm", "kernel": "whole set matvec (stored M2L + both L2P copies, read once)",
+                         "unit": "GB/s", "achieved": byts / (t_set * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
+                         "algorithmic_bytes": byts, "traffic": None,
+                         "frac": byts / (t_set * 1e-3) / 1e9 / hbm},
+            "clocks": clocks,
+            "e2e": {"value": world * total / t_e2e, "unit": "points/s", "h2d_bytes_per_step": 8 * total,
+                    "d2h_bytes_per_step": 8 * total, "ms_per_step": t_e2e * 1e3}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle_lib import RefLib
+        if RefLib.available():
+            done, spent, tm = 0, 0.0, 0.0
+            for pts, qk in probs:
+                t1 = time.perf_counter()
+                r = RefLib(pts, p["M"], p["tol"], p["kernel"])
+                r.assemble()
+                t2 = time.perf_counter()
+                r.matvec(qk)
+                t3 = time.perf_counter()
+                tm += t3 - t2
+                spent += t3 - t1
+                done += len(pts)
+                if spent > 15.0:
+                    break
+            line["cpu_baseline"] = {"value": done / tm, "unit": "points/s", "cores": int(r.lib.ref_num_threads()),
+                                    "kind": "reference",
+                                    "sample": f"the first problems of the set ({done} points), one matvec each"}
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    st.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "many":
+        run_many(args)
     else:
         run_ours(args)
 

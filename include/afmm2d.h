@@ -169,6 +169,32 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
                                         double* xy_sorted, void* stream);
 
 afmm_status afmm_destroy(afmm_handle* h);
+
+/* ---- many independent problems in one call -------------------------------
+ * No single counterpart in the reference, which applies one problem per AFMM
+ * object (AFMM::computeMatVecProduct, include/AFMM2D.hpp:30); a set replaces
+ * a loop of that call over many objects.  afmm_set_create takes n assembled
+ * handles on the current device with one kernel id (the handles stay owned
+ * by the caller and must outlive the set) and records, once, a CUDA graph in
+ * which every stage of the FP64 matvec is one fused launch over all problems
+ * (gather, M2M per depth below the leaves, M2L of all levels, L2L per level,
+ * near field, scatter).  afmm_set_matvec replays it: q and y hold the
+ * problems' charges / potentials back to back in handle order (problem p at
+ * offsets[p] .. offsets[p+1], each in its own original point order), host or
+ * device memory.  Each problem's result has the same bits as its own FP64
+ * afmm_matvec.  The set uses the handles' FP64 work buffers: do not run a
+ * set and one of its handles concurrently. */
+typedef struct afmm_set afmm_set;
+afmm_status afmm_set_create(afmm_handle* const* handles, int n, afmm_set** out);
+afmm_status afmm_set_matvec(afmm_set* s, const double* q, double* y, int mem_device);
+/* offsets: n + 1 entries (prefix of the problems' N). */
+afmm_status afmm_set_get_offsets(afmm_set* s, int64_t* offsets);
+/* Fused launches recorded in the graph per matvec, and graph launches so far. */
+afmm_status afmm_set_get_launches(afmm_set* s, int* launches_per_matvec, int64_t* graph_launches);
+afmm_status afmm_set_get_stream(afmm_set* s, void** stream);
+afmm_status afmm_set_destroy(afmm_set* s);
+const char* afmm_set_last_error(afmm_set* s);
+
 const char* afmm_status_string(afmm_status s);
 const char* afmm_last_error(afmm_handle* h);
 /* Library version string. */
