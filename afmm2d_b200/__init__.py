@@ -58,6 +58,7 @@ _SIGS = {
     "afmm_set_get_offsets": [_vp, _vp],
     "afmm_set_get_launches": [_vp, _vp, _vp],
     "afmm_set_get_stream": [_vp, _vp],
+    "afmm_set_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_set_destroy": [_vp],
 }
 _lib = None
@@ -333,6 +334,14 @@ class AFMMSet:
         s = ctypes.c_void_p()
         self._call("afmm_set_get_stream", ctypes.byref(s))
         return s.value
+
+    def stage_times(self):
+        """Device milliseconds per stage of the last matvec."""
+        n = ctypes.c_int()
+        names = (ctypes.c_char_p * 16)()
+        ms = (ctypes.c_double * 16)()
+        self._call("afmm_set_get_stage_times", 16, names, ms, ctypes.byref(n))
+        return {names[i].decode(): ms[i] for i in range(min(n.value, 16))}
 
     def close(self):
         if getattr(self, "_h", None) is not None and self._h.value:

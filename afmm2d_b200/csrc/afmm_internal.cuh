@@ -44,9 +44,15 @@ struct Error {
 // rsqrt, lg2, ex2) with relative error near FP32 rounding.
 struct KernelParams {
   int id;
-  double a;      // 2^-L
-  double param;  // Gaussian: exp(-R2 / param)
+  double a;       // 2^-L
+  double param;   // Gaussian: exp(-R2 / param)
+  double a2;      // a * a
+  double inv_a2;  // 1 / (a * a)
 };
+
+inline KernelParams make_kernel_params(int id, double a, double param) {
+  return KernelParams{id, a, param, a * a, 1.0 / (a * a)};
+}
 
 __device__ __forceinline__ double r2_exact(double xi, double yi, double xj, double yj) {
   double dx = __dsub_rn(xi, xj), dy = __dsub_rn(yi, yj);
@@ -90,10 +96,14 @@ struct KLog {
     if (R2 < __dmul_rn(p.a, p.a)) return __ddiv_rn(__ddiv_rn(__dmul_rn(__dmul_rn(0.5, R2), l), p.a), p.a);
     return __dmul_rn(0.5, l);
   }
+  // a = 2^-L, so dividing by a twice is the exact scaling by 1/a^2: both
+  // branches are evaluated without divergence and selected (same bits as
+  // 0.5*R2*log(R2)/a/a and 0.5*log(R2))
   __device__ __forceinline__ static double eval(double R2, const KernelParams& p) {
-    if (R2 < 1e-10) return 0.0;
-    if (R2 < p.a * p.a) return 0.5 * R2 * log(R2) / p.a / p.a;
-    return 0.5 * log(R2);
+    const double l = log(R2);
+    const double near = ((0.5 * R2) * l) * p.inv_a2;
+    const double r = R2 < p.a2 ? near : 0.5 * l;
+    return R2 < 1e-10 ? 0.0 : r;
   }
   __device__ __forceinline__ static float eval32(float R2, float a, float) {
     if (R2 < 1e-10f) return 0.0f;

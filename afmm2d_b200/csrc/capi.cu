@@ -23,6 +23,7 @@ struct afmm_set {
   cudaStream_t stream = nullptr;
   std::vector<int64_t> offsets;
   int64_t graph_launches = 0;
+  std::vector<std::pair<std::string, double>> stage_ms;
   std::string err;
 };
 
@@ -565,7 +566,7 @@ afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const dou
     // a = boxRadius[L], halving from 1 (src/AFMM2DTree.cpp:14-19)
     double a = 1.0;
     for (int j = 0; j < L; ++j) a *= 0.5;
-    h->kp = KernelParams{kernel_id, a, param};
+    h->kp = make_kernel_params(kernel_id, a, param);
     double t0 = now_s();
     do_create(h, loc, loc_layout);
     h->t_create = now_s() - t0;
@@ -818,7 +819,7 @@ afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, c
     double* dout = tmp.alloc<double>(n);
     AFMM_CUDA(cudaMemcpy(da, xy1, sizeof(double2) * n, cudaMemcpyHostToDevice));
     AFMM_CUDA(cudaMemcpy(db, xy2, sizeof(double2) * n, cudaMemcpyHostToDevice));
-    dispatch_kernel<PairsRun>(kernel_id, da, db, (long)n, KernelParams{kernel_id, a, param}, mode, dout);
+    dispatch_kernel<PairsRun>(kernel_id, da, db, (long)n, make_kernel_params(kernel_id, a, param), mode, dout);
     AFMM_CUDA(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
   });
 }
@@ -918,6 +919,24 @@ afmm_status afmm_set_get_launches(afmm_set* st, int* per_matvec, int64_t* graph_
   if (per_matvec) *per_matvec = st->plan.launches_per_matvec;
   if (graph_launches) *graph_launches = st->graph_launches;
   return AFMM_OK;
+}
+
+afmm_status afmm_set_get_stage_times(afmm_set* st, int cap, const char** names, double* ms, int* n) {
+  if (!st || !n) return AFMM_BAD_ARG;
+  try {
+    if (st->stream) AFMM_CUDA(cudaStreamSynchronize(st->stream));
+    if (st->graph_launches == 0) throw Error{AFMM_BAD_ARG, "afmm_set_get_stage_times before afmm_set_matvec"};
+    set_stage_times(st->plan, st->stage_ms);
+    *n = (int)st->stage_ms.size();
+    for (int i = 0; i < *n && i < cap; ++i) {
+      if (names) names[i] = st->stage_ms[i].first.c_str();
+      if (ms) ms[i] = st->stage_ms[i].second;
+    }
+    return AFMM_OK;
+  } catch (const Error& e) {
+    st->err = e.msg;
+    return e.status;
+  }
 }
 
 afmm_status afmm_set_get_stream(afmm_set* st, void** stream) {

@@ -143,30 +143,47 @@ T* upload(const std::vector<T>& h, DevArena& arena, cudaStream_t s) {
 }
 
 void record(SetPlan& sp, cudaStream_t s) {
-  int n = 0;
+  int n = 0, m = 0;
+  auto mark = [&](const char* name) {
+    if ((size_t)m == sp.marks.size()) {
+      cudaEvent_t e;
+      AFMM_CUDA(cudaEventCreate(&e));
+      sp.marks.push_back({name, e});
+    }
+    // an external record becomes an event-record node of the graph
+    AFMM_CUDA(cudaEventRecordWithFlags(sp.marks[m].second, s, cudaEventRecordExternal));
+    ++m;
+  };
+  mark("gather");
   k_set_gather<<<nb(sp.gather.total, 256), 256, 0, s>>>(sp.dev, sp.gather, sp.q);
   AFMM_LAUNCH_CHECK();
   ++n;
+  mark("m2m");
   for (const SetSegs& sg : sp.m2m) {
     k_set_m2m<<<nb(sg.total, 128), 128, 0, s>>>(sp.dev, sg);
     AFMM_LAUNCH_CHECK();
     ++n;
   }
+  mark("m2l");
   if (sp.m2l.total > 0) {
     k_set_m2l<<<nb(sp.m2l.total, 128), 128, 0, s>>>(sp.dev, sp.m2l);
     AFMM_LAUNCH_CHECK();
     ++n;
   }
+  mark("l2l");
   for (const SetSegs& sg : sp.l2l) {
     k_set_l2l<<<nb(sg.total, 128), 128, 0, s>>>(sp.dev, sg);
     AFMM_LAUNCH_CHECK();
     ++n;
   }
+  mark("p2p");
   dispatch_kernel<SetP2pLaunch>(sp.kernel_id, sp, s);
   ++n;
+  mark("scatter");
   k_set_scatter<<<nb(sp.gather.total, 256), 256, 0, s>>>(sp.dev, sp.gather, sp.y);
   AFMM_LAUNCH_CHECK();
   ++n;
+  mark("end");
   sp.launches_per_matvec = n;
 }
 
@@ -257,9 +274,20 @@ void set_build(SetPlan& sp, const std::vector<SetProblem>& probs, DevArena& aren
 
 void set_matvec(SetPlan& sp, cudaStream_t s) { AFMM_CUDA(cudaGraphLaunch(sp.exec, s)); }
 
+void set_stage_times(const SetPlan& sp, std::vector<std::pair<std::string, double>>& out) {
+  out.clear();
+  for (size_t i = 0; i + 1 < sp.marks.size(); ++i) {
+    float ms = 0;
+    AFMM_CUDA(cudaEventElapsedTime(&ms, sp.marks[i].second, sp.marks[i + 1].second));
+    out.push_back({sp.marks[i].first, ms});
+  }
+}
+
 void set_release(SetPlan& sp) {
   if (sp.exec) cudaGraphExecDestroy(sp.exec);
   if (sp.graph) cudaGraphDestroy(sp.graph);
+  for (auto& m : sp.marks) cudaEventDestroy(m.second);
+  sp.marks.clear();
   sp.exec = nullptr;
   sp.graph = nullptr;
 }

@@ -51,7 +51,12 @@ struct SetPlan {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int launches_per_matvec = 0;
+  // events recorded inside the graph between stages (per-stage device time)
+  std::vector<std::pair<std::string, cudaEvent_t>> marks;
 };
+
+// Per-stage milliseconds of the last replay, accumulated by stage name.
+void set_stage_times(const SetPlan& sp, std::vector<std::pair<std::string, double>>& out);
 
 // Builds the device tables (allocated from `arena`) and the graph on stream s.
 void set_build(SetPlan& sp, const std::vector<SetProblem>& probs, DevArena& arena, cudaStream_t s);

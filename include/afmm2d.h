@@ -191,6 +191,9 @@ afmm_status afmm_set_matvec(afmm_set* s, const double* q, double* y, int mem_dev
 afmm_status afmm_set_get_offsets(afmm_set* s, int64_t* offsets);
 /* Fused launches recorded in the graph per matvec, and graph launches so far. */
 afmm_status afmm_set_get_launches(afmm_set* s, int* launches_per_matvec, int64_t* graph_launches);
+/* Device milliseconds per stage of the last afmm_set_matvec (events recorded
+ * inside the graph between stages); names stay valid until the next call. */
+afmm_status afmm_set_get_stage_times(afmm_set* s, int cap, const char** names, double* ms, int* n);
 afmm_status afmm_set_get_stream(afmm_set* s, void** stream);
 afmm_status afmm_set_destroy(afmm_set* s);
 const char* afmm_set_last_error(afmm_set* s);

@@ -271,3 +271,25 @@ def test_batched_host_device_and_kernels():
     for c in (0, 15):
         y64 = a.computeMatVecProduct(Q[:, c])
         assert np.linalg.norm(Yh[:, c] - y64) / np.linalg.norm(y64) <= MIXED_TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["one_over_r_scaled", "log", "one_over_r", "gaussian"])
+def test_fp64_matvec_kernel_form_tracks_the_exact_form(kernel):
+    """The matvec's fast FP64 entries (libdevice sqrt/log/exp, the log kernel's
+    near-leaf branch as an exact power-of-two scaling, both branches selected
+    without divergence) stay within a few ulp of the reference arithmetic,
+    across both sides of R = a, R2 = 1e-10 and at R = 0."""
+    rng = np.random.default_rng(11)
+    a = 2.0 ** -7
+    n = 1 << 16
+    xy1 = rng.uniform(0, 1, (n, 2))
+    r = np.exp(rng.uniform(np.log(1e-7), np.log(4 * a), n))
+    t = rng.uniform(0, 2 * np.pi, n)
+    xy2 = xy1 + np.stack([r * np.cos(t), r * np.sin(t)], axis=1)
+    xy2[:64] = xy1[:64]  # R = 0
+    g = A.kernel_eval(kernel, a, xy1, xy2, mode="exact")
+    f = A.kernel_eval(kernel, a, xy1, xy2, mode="fp64")
+    assert np.all(np.isfinite(f) == np.isfinite(g))
+    ok = np.isfinite(g)
+    assert np.all(np.abs(f[ok] - g[ok]) <= 8e-16 * np.maximum(np.abs(g[ok]), 1e-300))
