@@ -230,6 +230,13 @@ void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launche
   }
 }
 
+void m2l_apply_stored(const MatvecPlan& p, cudaStream_t s) {
+  const long rows = p.levels.row0[p.levels.nlev];
+  if (rows == 0) return;
+  k_m2l_apply<<<(int)((rows + 127) / 128), 128, 0, s>>>(p.levels);
+  AFMM_LAUNCH_CHECK();
+}
+
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches) {
   const int N = p.N;
   const int gb = (N + 255) / 256;
@@ -240,12 +247,8 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   if (tm) tm->mark(s, "m2m");
   sweep_m2m(p, p.qs, s, launches);
   if (tm) tm->mark(s, "m2l");
-  {
-    const long rows = p.levels.row0[p.levels.nlev];
-    k_m2l_apply<<<(int)((rows + 127) / 128), 128, 0, s>>>(p.levels);
-    AFMM_LAUNCH_CHECK();
-    ++*launches;
-  }
+  m2l_apply_stored(p, s);
+  ++*launches;
   if (tm) tm->mark(s, "l2l");
   sweep_l2l(p, p.ys, s, launches);
   if (tm) tm->mark(s, "p2p");

@@ -283,8 +283,34 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     if (tm) tm->mark(s, "m2m");
     sweep_m2m(p, ms.qs, s, launches);
     if (tm) tm->mark(s, "m2l");
-    dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
-    ++*launches;
+    const bool stored = p.levels.nlev > 0 && p.levels.lv[0].m2l != nullptr;
+    if (ms.m2l_form < 0 && stored) {
+      // one-time choice: both forms write the same yhat (to FP64 rounding);
+      // time each once on this problem and keep the faster
+      cudaEvent_t e[3];
+      for (auto& x : e) AFMM_CUDA(cudaEventCreate(&x));
+      AFMM_CUDA(cudaEventRecord(e[0], s));
+      dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
+      AFMM_CUDA(cudaEventRecord(e[1], s));
+      m2l_apply_stored(p, s);
+      AFMM_CUDA(cudaEventRecord(e[2], s));
+      AFMM_CUDA(cudaEventSynchronize(e[2]));
+      AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[0], e[0], e[1]));
+      AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[1], e[1], e[2]));
+      for (auto& x : e) cudaEventDestroy(x);
+      ms.m2l_form = ms.m2l_ms[1] < ms.m2l_ms[0] ? 1 : 0;
+      *launches += 2;
+      if (ms.m2l_form == 0) {  // the result must come from the chosen form
+        dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
+        ++*launches;
+      }
+    } else if (ms.m2l_form == 1 && stored) {
+      m2l_apply_stored(p, s);
+      ++*launches;
+    } else {
+      dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
+      ++*launches;
+    }
     if (tm) tm->mark(s, "l2l");
     sweep_l2l(p, ms.ys, s, launches);
     if (tm) tm->mark(s, "p2p");
