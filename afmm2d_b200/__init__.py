@@ -24,7 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafmm2d.so")
 
 KERNELS = {"one_over_r_scaled": 0, "log": 1, "one_over_r": 2, "gaussian": 3}
-PRECISIONS = {"fp64": 0, "mixed": 1}
+PRECISIONS = {"fp64": 0, "mixed": 1, "fp64_batched": 2}
 STATUS = {0: "ok", 1: "bad argument", 2: "out of device memory", 3: "CUDA error", 4: "device wait timed out",
           5: "non-finite values", 6: "not assembled", 7: "no sm_100 device"}
 

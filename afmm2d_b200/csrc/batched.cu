@@ -40,13 +40,14 @@ __device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) 
 // points, reads each column of q as one contiguous run, and writes each
 // point's sorted row qs[iperm[j]][0:RC] (one 128-byte line for RC = 16).
 // With RC >= 8 the row is also written as interleaved TF32 high / low parts
-// (the tensor-core near field's charges), otherwise as FP32.
+// (the tensor-core near field's charges), otherwise as FP32; neither when the
+// pass is FP64 throughout.
 constexpr int kTileJ = 64;
 
 template <int RC>
 __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols,
                                                   const int32_t* __restrict__ iperm, int N, double* qs, float* qs32,
-                                                  uint2* qhl) {
+                                                  uint2* qhl, int fp64_only) {
   __shared__ double tile[RC][kTileJ + 1];
   const long j0 = (long)blockIdx.x * kTileJ;
   for (int idx = threadIdx.x; idx < RC * kTileJ; idx += blockDim.x) {
@@ -62,6 +63,7 @@ __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, 
     const double v0 = tile[2 * cp][jj], v1 = tile[2 * cp + 1][jj];
     const long d = (long)iperm[j] * RC + 2 * cp;
     *reinterpret_cast<double2*>(qs + d) = make_double2(v0, v1);
+    if (fp64_only) continue;
     const float f0 = (float)v0, f1 = (float)v1;
     if (RC >= 8) {
       uint4 hl;
@@ -787,6 +789,100 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
   }
 }
 
+// Stand-in coordinates of padded source slots and absent targets of the FP64
+// near field (finite entries for every kernel, never stored).
+constexpr double kPadSrc64 = 1.0e100, kPadTgt64 = -1.0e100;
+
+// Near field in FP64 on the FP64 tensor cores (AFMM_PREC_FP64_BATCHED): one
+// CTA per leaf, one warp per 32 targets (four 8-row tiles sharing every charge
+// fragment).  Source leaves (neighbours 0..7, then the leaf itself) are staged
+// in shared memory with their exact coordinates, padded to multiples of 4 with
+// far stand-ins; each lane evaluates one FP64 entry per tile and 4-source step
+// with the FP64 matvec form K::eval (the diagonal included, as in the FP64
+// path), and the 8 x 4 entry tiles multiply the 4 x RC FP64 charge blocks
+// (mma.sync m8n8k4, FP64 accumulation).
+template <class K, int RC>
+__global__ void __launch_bounds__(128) k_p2p_dmma(NearView nv, KernelParams kp, const double* __restrict__ qs,
+                                                  double* __restrict__ ys) {
+  constexpr int NTT = 4;  // 8-row target tiles per warp
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_src[9], s_cnt[9], s_coff[10], s_ns;
+  const long b = blockIdx.x;
+  const int n = nv.leaf_cnt[b];
+  const int s0 = nv.leaf_start[b];
+  if (threadIdx.x == 0) {
+    int m = 0, off = 0;
+    for (int slot = 0; slot < 9; ++slot) {
+      const long cbx = slot < 8 ? nv.nbr[b * 8 + slot] : b;
+      if (cbx < 0) continue;
+      s_src[m] = nv.leaf_start[cbx];
+      s_cnt[m] = nv.leaf_cnt[cbx];
+      s_coff[m] = off;
+      off += (nv.leaf_cnt[cbx] + 3) >> 2;
+      ++m;
+    }
+    s_coff[m] = off;
+    s_ns = m;
+  }
+  __syncthreads();
+  const int ns = s_ns;
+  double2* sx = (double2*)smem;
+  for (int m = 0; m < ns; ++m) {
+    const int o = s_coff[m] * 4, nc = s_cnt[m], src = s_src[m], np = (s_coff[m + 1] - s_coff[m]) * 4;
+    for (int t = threadIdx.x; t < np; t += blockDim.x)
+      sx[o + t] = t < nc ? nv.pts[src + t] : make_double2(kPadSrc64, kPadSrc64);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int trow = lane >> 2, tsrc = lane & 3;
+  for (int tg = warp; tg * 32 < n; tg += nw) {
+    double2 x[NTT];
+#pragma unroll
+    for (int u = 0; u < NTT; ++u) {
+      const int ti = tg * 32 + u * 8 + trow;
+      x[u] = ti < n ? nv.pts[s0 + ti] : make_double2(kPadTgt64, kPadTgt64);
+    }
+    double c[NTT][RC / 8][2];
+#pragma unroll
+    for (int u = 0; u < NTT; ++u)
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) c[u][t][0] = c[u][t][1] = 0.0;
+    for (int m = 0; m < ns; ++m) {
+      const int src = s_src[m], nc = s_cnt[m];
+      for (int st = s_coff[m]; st < s_coff[m + 1]; ++st) {
+        const int j = (st - s_coff[m]) * 4 + tsrc;
+        const double2 p = sx[st * 4 + tsrc];
+        const bool vj = j < nc;
+        double bq[RC / 8];
+#pragma unroll
+        for (int t = 0; t < RC / 8; ++t) bq[t] = vj ? qs[(long)(src + j) * RC + t * 8 + trow] : 0.0;
+#pragma unroll
+        for (int u = 0; u < NTT; ++u) {
+          const double dx = x[u].x - p.x, dy = x[u].y - p.y;
+          const double a = K::eval(dx * dx + dy * dy, kp);
+#pragma unroll
+          for (int t = 0; t < RC / 8; ++t) mma_f64_8x8x4(c[u][t][0], c[u][t][1], a, bq[t]);
+        }
+      }
+    }
+    // D fragment: row trow, columns 2*tsrc, 2*tsrc + 1 of each 8-column block
+#pragma unroll
+    for (int u = 0; u < NTT; ++u) {
+      const int ti = tg * 32 + u * 8 + trow;
+      if (ti < n) {
+#pragma unroll
+        for (int t = 0; t < RC / 8; ++t) {
+          double2* o = reinterpret_cast<double2*>(ys + (long)(s0 + ti) * RC + t * 8 + 2 * tsrc);
+          double2 w = *o;
+          w.x += c[u][t][0];
+          w.y += c[u][t][1];
+          *o = w;
+        }
+      }
+    }
+  }
+}
+
 inline int nbk(long n, int t) { return (int)((n + t - 1) / t); }
 
 template <int RC>
@@ -812,9 +908,18 @@ struct Pass {
   };
   template <class K>
   struct P2p {
-    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint2* qhl, double* ys,
-                    cudaStream_t s) {
+    static void run(const NearView& nv, const KernelParams& kp, const float* qs32, const uint2* qhl,
+                    const double* qs, double* ys, int fp64, cudaStream_t s) {
       constexpr int RM = RC >= 8 ? RC : 8;
+      if (fp64) {
+        if (RC < 8) throw Error{AFMM_BAD_ARG, "FP64 batched passes take 8 or 16 columns"};
+        const int warps = std::min(4, (nv.nmax + 31) / 32);
+        const size_t smem = (size_t)9 * ((nv.nmax + 3) / 4 * 4) * sizeof(double2);
+        allow_smem(k_p2p_dmma<K, RM>, smem);
+        k_p2p_dmma<K, RM><<<(int)nv.nleaf, 32 * warps, smem, s>>>(nv, kp, qs, ys);
+        AFMM_LAUNCH_CHECK();
+        return;
+      }
       const int warps = std::min(4, (nv.nmax + 31) / 32);
       const size_t smem_mma =
           (size_t)9 * ((nv.nmax + 7) / 8 * 8) * sizeof(float2) + (size_t)warps * RM * 32 * sizeof(double);
@@ -832,11 +937,11 @@ struct Pass {
   };
 
   static void run(const MatvecPlan& p, BatchState& bs, const NearView& nv, const double* q, int64_t ldq, double* y,
-                  int64_t ldy, int ncols, cudaStream_t s, StageTimer* tm, int64_t* launches) {
+                  int64_t ldy, int ncols, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
     constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl);
+    k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl, fp64);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     if (tm) tm->mark(s, "m2m");
@@ -868,7 +973,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "p2p");
-    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhl, bs.ys, s);
+    dispatch_kernel<P2p>(p.kp.id, nv, p.kp, bs.qs32, bs.qhl, bs.qs, bs.ys, fp64, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
     k_scatter_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
@@ -907,7 +1012,7 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
 }
 
 void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const double* q, int64_t ldq, double* y,
-                    int64_t ldy, int nrhs, cudaStream_t s, StageTimer* tm, int64_t* launches) {
+                    int64_t ldy, int nrhs, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
   if (!ms.ready || !bs.ready) throw Error{AFMM_BAD_ARG, "batched operators are not set up"};
   NearView nv = p.near;
   nv.anchor = ms.leaf_anchor;
@@ -915,13 +1020,14 @@ void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const d
   nv.span = ms.leaf_span;
   for (int c0 = 0; c0 < nrhs;) {
     const int left = nrhs - c0;
-    const int rc = left > 8 ? 16 : (left > 4 ? 8 : 4);
+    // FP64 passes take 8 or 16 columns (tensor-core tiles; unused columns are zero)
+    const int rc = left > 8 ? 16 : (left > 4 || fp64 ? 8 : 4);
     const int nc = std::min(left, rc);
     const double* qc = q + (long)c0 * ldq;
     double* yc = y + (long)c0 * ldy;
-    if (rc == 16) Pass<16>::run(p, bs, nv, qc, ldq, yc, ldy, nc, s, tm, launches);
-    else if (rc == 8) Pass<8>::run(p, bs, nv, qc, ldq, yc, ldy, nc, s, tm, launches);
-    else Pass<4>::run(p, bs, nv, qc, ldq, yc, ldy, nc, s, tm, launches);
+    if (rc == 16) Pass<16>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
+    else if (rc == 8) Pass<8>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
+    else Pass<4>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
     c0 += nc;
   }
 }

@@ -595,16 +595,20 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
   return guard(h, [&] {
     if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_matvec before afmm_assemble"};
     if (!q || !y || nrhs < 1 || ld < h->N) throw Error{AFMM_BAD_ARG, "bad q/y/nrhs/ld"};
-    if (precision != AFMM_PREC_FP64 && precision != AFMM_PREC_MIXED) throw Error{AFMM_BAD_ARG, "bad precision"};
+    if (precision != AFMM_PREC_FP64 && precision != AFMM_PREC_MIXED && precision != AFMM_PREC_FP64_BATCHED)
+      throw Error{AFMM_BAD_ARG, "bad precision"};
+    // one column in FP64 batched mode is the plain FP64 apply
+    if (precision == AFMM_PREC_FP64_BATCHED && nrhs == 1) precision = AFMM_PREC_FP64;
     cudaStream_t s = h->stream;
     const size_t bytes = sizeof(double) * (size_t)h->N;
     if (h->profiling) h->timer.reset();
     StageTimer* tm = h->profiling ? &h->timer : nullptr;
-    if (precision == AFMM_PREC_MIXED) {
+    if (precision == AFMM_PREC_MIXED || precision == AFMM_PREC_FP64_BATCHED) {
+      const int fp64 = precision == AFMM_PREC_FP64_BATCHED;
       mixed_reserve(h->mixed, h->N, 1, h->arena);
       if (nrhs > 1) batch_reserve(h->plan, h->batch, h->arena, s);
       auto run = [&](const double* qq, int64_t ldq, double* yy, int64_t ldy) {
-        if (nrhs > 1) matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nrhs, s, tm, &h->launches);
+        if (nrhs > 1) matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nrhs, fp64, s, tm, &h->launches);
         else matvec_mixed(h->plan, h->mixed, qq, ldq, yy, ldy, nrhs, s, tm, &h->launches);
       };
       if (!mem_device) {

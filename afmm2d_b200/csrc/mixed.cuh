@@ -42,8 +42,10 @@ struct BatchState {
 };
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s);
 // y = K q for nrhs > 1 columns in passes of 4, 8 or 16 right-hand sides.
+// fp64 = 1: FP64 throughout (FP64 near field on the tensor cores), passes of 8
+// or 16 columns.
 void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const double* q, int64_t ldq, double* y,
-                    int64_t ldy, int nrhs, cudaStream_t s, StageTimer* tm, int64_t* launches);
+                    int64_t ldy, int nrhs, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches);
 
 // Builds the FP32 operators and anchors after assembly.
 void mixed_setup(MatvecPlan& p, std::vector<LevelDev>& lv, MixedState& ms, DevArena& arena, cudaStream_t s,

@@ -201,7 +201,7 @@ def run_ours(args):
     dY = torch.empty_like(dQ)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    paths = {"fp64": ("fp64", 1), "mixed": ("mixed", 1), "batched": ("mixed", R)}
+    paths = {"fp64": ("fp64", 1), "mixed": ("mixed", 1), "batched": ("mixed", R), "fp64_batched": ("fp64_batched", R)}
 
     def call(name):
         prec, nr = paths[name]
@@ -264,6 +264,9 @@ def run_ours(args):
     err_batched = float(np.max([np.linalg.norm(yb[:, c] - y64[:, c]) / np.linalg.norm(y64[:, c]) for c in range(R)]))
     call("mixed")
     err_mixed = float(np.linalg.norm(dY[0].cpu().numpy() - y64[:, 0]) / np.linalg.norm(y64[:, 0]))
+    call("fp64_batched")
+    yb64 = dY.cpu().numpy().T
+    err_fp64b = float(np.max([np.linalg.norm(yb64[:, c] - y64[:, c]) / np.linalg.norm(y64[:, c]) for c in range(R)]))
     # end to end through the C ABI with pinned host buffers (the headline workload)
     hQ = torch.from_numpy(np.asfortranarray(Q).T.copy()).pin_memory()
     hY = torch.empty_like(hQ).pin_memory()
@@ -325,6 +328,7 @@ def run_ours(args):
                              "gpu_launches": launches[name]} for name in paths},
             "speedup_batched_vs_fp64": (N * R / t_dev["batched"]) / (N / t_dev["fp64"]),
             "rel_err_batched_vs_fp64_max_col": err_batched, "rel_err_mixed_vs_fp64": err_mixed,
+            "rel_err_fp64_batched_vs_fp64_max_col": err_fp64b,
             "rel_err_fp64_vs_dense_16_leaves": err_dense,
             "setup_s": setup_s, "setup": a.setup_times(), "stages_ms": stages, "counts": counts,
             "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},

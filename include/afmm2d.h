@@ -70,8 +70,11 @@ typedef enum {
 } afmm_kernel_id;
 
 typedef enum {
-  AFMM_PREC_FP64 = 0,  /* plain FP64 apply (stored operators) */
-  AFMM_PREC_MIXED = 1  /* FP32 apply with FP64 where it matters */
+  AFMM_PREC_FP64 = 0,        /* plain FP64 apply (stored operators), column by column */
+  AFMM_PREC_MIXED = 1,       /* FP32 apply with FP64 where it matters */
+  AFMM_PREC_FP64_BATCHED = 2 /* FP64 throughout, 8 or 16 columns per pass on the FP64 tensor
+                                cores; agrees with AFMM_PREC_FP64 to FP64 rounding (the
+                                summation order differs) */
 } afmm_precision;
 
 /* Layout of the `loc` array given to afmm_create. */

@@ -293,3 +293,30 @@ def test_fp64_matvec_kernel_form_tracks_the_exact_form(kernel):
     assert np.all(np.isfinite(f) == np.isfinite(g))
     ok = np.isfinite(g)
     assert np.all(np.abs(f[ok] - g[ok]) <= 8e-16 * np.maximum(np.abs(g[ok]), 1e-300))
+
+
+# FP64 throughout; only the summation order differs, and the L2P weights
+# (large, mixed-sign) amplify FP64 rounding to ~1e-13 on the log kernel -- the
+# level at which the FP64 path itself meets the reference's CPU result
+FP64_BATCHED_TOL = 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,nrhs", [("one_over_r", 3), ("log", 16), ("gaussian", 21), ("one_over_r_scaled", 8)])
+def test_fp64_batched_matches_fp64_columns(kernel, nrhs):
+    """AFMM_PREC_FP64_BATCHED (FP64 tensor-core tiles in every sweep and in the
+    near field, passes of 8 or 16 columns with zero-padded remainders) against
+    the plain FP64 apply column by column, on a clustered tree."""
+    torch = pytest.importorskip("torch")
+    pts, _, _ = workloads.make("mixture4m", N=32768)
+    a = A.AFMM(32768, 64, 8, pts, kernel=kernel)
+    a.assemble()
+    Q = np.random.default_rng(nrhs).standard_normal((32768, nrhs))
+    Yb = a.computeMatVecProduct(Q, precision="fp64_batched")
+    for c in range(nrhs):
+        y64 = a.computeMatVecProduct(Q[:, c])
+        assert np.linalg.norm(Yb[:, c] - y64) / np.linalg.norm(y64) <= FP64_BATCHED_TOL, c
+    dq = torch.tensor(Q.T.copy(), device="cuda")
+    dy = torch.zeros_like(dq)
+    a.matvec_device(dq.data_ptr(), dy.data_ptr(), nrhs, 32768, precision="fp64_batched")
+    np.testing.assert_array_equal(dy.cpu().numpy().T, Yb)
