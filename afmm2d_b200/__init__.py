@@ -44,6 +44,8 @@ _SIGS = {
     "afmm_get_charge_points": [_vp, _i, _vp, _vp],
     "afmm_get_l2p": [_vp, _i, _i, _vp, _vp, _vp],
     "afmm_set_profiling": [_vp, _i],
+    "afmm_set_m2l_storage": [_vp, _i],
+    "afmm_get_m2l_stored": [_vp, _vp],
     "afmm_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_setup_times": [_vp, _vp],
     "afmm_get_counts": [_vp, _vp],
@@ -159,6 +161,18 @@ class AFMM:
         """ACA skeletons, L2P and M2L blocks of every box (src/AFMM2D.cpp:41-44)."""
         _check(lib().afmm_assemble(self._h), self._h)
         self.assembled = True
+
+    M2L_STORAGE = {"auto": 0, "store": 1, "on_the_fly": 2}
+
+    def set_m2l_storage(self, mode):
+        """M2L block storage before assemble(): "auto" (store when they fit),
+        "store", or "on_the_fly" (entries evaluated in FP64 by every matvec)."""
+        _check(lib().afmm_set_m2l_storage(self._h, self.M2L_STORAGE[mode]), self._h)
+
+    def m2l_stored(self):
+        v = ctypes.c_int()
+        _check(lib().afmm_get_m2l_stored(self._h, ctypes.byref(v)), self._h)
+        return bool(v.value)
 
     def computeMatVecProduct(self, b, precision="fp64"):
         """y = K b in the original point order (src/AFMM2D.cpp:46-65)."""

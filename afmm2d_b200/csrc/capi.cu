@@ -30,6 +30,8 @@ struct afmm_set {
 struct afmm_handle {
   int N = 0, M = 0, tol_pow = 0, L = 0, kernel_id = 0;
   int device = 0;
+  int m2l_mode = AFMM_M2L_AUTO;  // afmm_m2l_storage
+  bool m2l_stored = false;
   KernelParams kp{};
   cudaStream_t stream = nullptr;
   DevArena arena;
@@ -430,8 +432,8 @@ void do_assemble(afmm_handle* h) {
     v.rmax = out.rmax;
     v.total_rank = out.h_skel_off[v.nbox];
   }
-  // M2L blocks, levels 2..L
-  int64_t m2l_total = 0;
+  // M2L blocks, levels 2..L: sizes first, then the storage decision
+  int64_t m2l_total = 0, l2p_total = 0, rows_total = 0;
   for (int j = 2; j <= L; ++j) {
     LevelDev& v = h->lv[j];
     const std::vector<int32_t>& il = h->h_il[j];
@@ -445,9 +447,27 @@ void do_assemble(afmm_handle* h) {
       v.h_m2l_off[b + 1] = v.h_m2l_off[b] + e;
     }
     m2l_total += v.h_m2l_off[v.nbox];
+    l2p_total += v.h_l2p_off[v.nbox];
+    rows_total += v.total_rank;
+  }
+  {
+    // AUTO stores the blocks when they fit beside what the matvecs still
+    // allocate (the row-major L2P copy, the mixed and 16-column batched
+    // buffers) with 2 GB to spare
+    size_t free_b = 0, total_b = 0;
+    AFMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double need = 8.0 * (double)m2l_total;
+    const double reserve = 8.0 * (double)l2p_total + (double)h->N * (16 * 8 * 4 + 64) +
+                           (double)rows_total * 16 * 8 * 2 + 2e9;
+    h->m2l_stored = h->m2l_mode == AFMM_M2L_STORE ||
+                    (h->m2l_mode == AFMM_M2L_AUTO && need <= (double)free_b - reserve);
+  }
+  for (int j = 2; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
     v.m2l_off = h->arena.alloc<int64_t>(v.nbox + 1);
     AFMM_CUDA(cudaMemcpyAsync(v.m2l_off, v.h_m2l_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
-    v.m2l = h->arena.alloc<double>(v.h_m2l_off[v.nbox] + 32);  // + 256 B for whole-piece L2 prefetches
+    // + 256 B for whole-piece L2 prefetches
+    v.m2l = h->m2l_stored ? h->arena.alloc<double>(v.h_m2l_off[v.nbox] + 32) : nullptr;
     v.qhat = h->arena.alloc<double>(v.total_rank);
     v.yhat = h->arena.alloc<double>(v.total_rank);
     // row -> box maps for the thread-per-row sweeps
@@ -500,9 +520,12 @@ void do_assemble(afmm_handle* h) {
   }
   build_plan(h);
   for (int j = 2; j <= L; ++j) {
-    m2l_assemble(h->plan.lv[j], h->kp, s);
+    if (h->m2l_stored) {
+      m2l_assemble(h->plan.lv[j], h->kp, s);
+      ++h->launches;
+    }
     l2p_transpose(h->plan.lv[j], h->lv[j].l2p, h->lv[j].l2p_rm, s);
-    h->launches += 2;
+    ++h->launches;
   }
   mixed_setup(h->plan, h->lv, h->mixed, h->arena, s, &h->launches);
   build_plan(h);
@@ -769,6 +792,26 @@ afmm_status afmm_get_l2p(afmm_handle* h, int level, int k, int32_t* rows, int32_
   });
 }
 
+afmm_status afmm_set_m2l_storage(afmm_handle* h, int mode) {
+  if (!h) return AFMM_BAD_ARG;
+  if (mode != AFMM_M2L_AUTO && mode != AFMM_M2L_STORE && mode != AFMM_M2L_ON_THE_FLY) {
+    h->err = "bad M2L storage mode";
+    return AFMM_BAD_ARG;
+  }
+  if (h->assembled) {
+    h->err = "afmm_set_m2l_storage after afmm_assemble";
+    return AFMM_BAD_ARG;
+  }
+  h->m2l_mode = mode;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored) {
+  if (!h || !stored) return AFMM_BAD_ARG;
+  *stored = h->m2l_stored ? 1 : 0;
+  return AFMM_OK;
+}
+
 afmm_status afmm_set_profiling(afmm_handle* h, int on) {
   if (!h) return AFMM_BAD_ARG;
   h->profiling = on != 0;
@@ -875,6 +918,7 @@ afmm_status afmm_set_create(afmm_handle* const* handles, int n, afmm_set** out) 
       if (!h) throw Error{AFMM_BAD_ARG, "afmm_set_create: null handle"};
       if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_set_create: handle not assembled"};
       if (h->kernel_id != handles[0]->kernel_id) throw Error{AFMM_BAD_ARG, "afmm_set_create: mixed kernel ids"};
+      if (!h->m2l_stored) throw Error{AFMM_BAD_ARG, "afmm_set_create: a handle has no stored M2L blocks"};
       if (h->device != dev) throw Error{AFMM_BAD_ARG, "afmm_set_create: handle on another device"};
       probs.push_back({&h->plan, p2p_shape(h->plan.near.nmax)});
     }

@@ -230,9 +230,13 @@ void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launche
   }
 }
 
-void m2l_apply_stored(const MatvecPlan& p, cudaStream_t s) {
+void m2l_apply(const MatvecPlan& p, cudaStream_t s) {
   const long rows = p.levels.row0[p.levels.nlev];
   if (rows == 0) return;
+  if (p.levels.lv[0].m2l == nullptr) {  // blocks not stored: entries on the fly
+    m2l_apply_otf(p, s);
+    return;
+  }
   k_m2l_apply<<<(int)((rows + 127) / 128), 128, 0, s>>>(p.levels);
   AFMM_LAUNCH_CHECK();
 }
@@ -247,7 +251,7 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   if (tm) tm->mark(s, "m2m");
   sweep_m2m(p, p.qs, s, launches);
   if (tm) tm->mark(s, "m2l");
-  m2l_apply_stored(p, s);
+  m2l_apply(p, s);
   ++*launches;
   if (tm) tm->mark(s, "l2l");
   sweep_l2l(p, p.ys, s, launches);

@@ -295,8 +295,11 @@ void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
 void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
-// M2L of every level from the stored FP64 blocks (one thread per skeleton row).
-void m2l_apply_stored(const MatvecPlan& p, cudaStream_t s);
+// M2L of every level in FP64: the stored blocks (one thread per skeleton row),
+// or m2l_apply_otf when no blocks are stored.
+void m2l_apply(const MatvecPlan& p, cudaStream_t s);
+// M2L of every level with the entries evaluated on the fly in FP64 (mixed.cu).
+void m2l_apply_otf(const MatvecPlan& p, cudaStream_t s);
 // The FP64 sweeps shared by both precisions (leaf charges qs in FP64).
 void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches);
 void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches);

@@ -240,6 +240,12 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
+void m2l_apply_otf(const MatvecPlan& p, cudaStream_t s) {
+  if (p.levels.row0[p.levels.nlev] == 0) return;
+  dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
+}
+
+
 void mixed_setup(MatvecPlan& p, std::vector<LevelDev>&, MixedState& ms, DevArena& arena, cudaStream_t s,
                  int64_t* launches) {
   NearView& nv = p.near;
@@ -292,7 +298,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
       AFMM_CUDA(cudaEventRecord(e[0], s));
       dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
       AFMM_CUDA(cudaEventRecord(e[1], s));
-      m2l_apply_stored(p, s);
+      m2l_apply(p, s);
       AFMM_CUDA(cudaEventRecord(e[2], s));
       AFMM_CUDA(cudaEventSynchronize(e[2]));
       AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[0], e[0], e[1]));
@@ -305,7 +311,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
         ++*launches;
       }
     } else if (ms.m2l_form == 1 && stored) {
-      m2l_apply_stored(p, s);
+      m2l_apply(p, s);
       ++*launches;
     } else {
       dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);

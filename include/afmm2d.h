@@ -77,6 +77,13 @@ typedef enum {
                                 summation order differs) */
 } afmm_precision;
 
+/* Storage of the M2L blocks K(R_b, R_c) (src/AFMM2DTree.cpp:1070-1097). */
+typedef enum {
+  AFMM_M2L_AUTO = 0,      /* store them when they fit in device memory (default) */
+  AFMM_M2L_STORE = 1,     /* always store them (AFMM_OOM if they do not fit) */
+  AFMM_M2L_ON_THE_FLY = 2 /* never store them: every matvec evaluates the entries in FP64 */
+} afmm_m2l_storage;
+
 /* Layout of the `loc` array given to afmm_create. */
 typedef enum {
   AFMM_LOC_COLMAJOR = 0,   /* N x 2 column-major, as Eigen::MatrixXd loc(N,2) */
@@ -93,6 +100,16 @@ afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const dou
 
 /* ACA skeletonisation of every box (levels L..2), L2P, and M2L blocks. */
 afmm_status afmm_assemble(afmm_handle* h);
+
+/* M2L storage policy (afmm_m2l_storage), before afmm_assemble.  No reference
+ * counterpart: the reference always stores the blocks in std::maps
+ * (src/AFMM2DTree.cpp:1070-1097), which at 16M points and TOL 12 needs
+ * ~190 GB.  Without stored blocks the M2L entries are evaluated on the fly in
+ * FP64 (the matvec's fast FP64 kernel form) by every precision; results
+ * agree with the stored blocks to FP64 rounding.  Sets need stored blocks. */
+afmm_status afmm_set_m2l_storage(afmm_handle* h, int mode);
+/* 1 when the assembled handle stores its M2L blocks. */
+afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored);
 
 /* y = K q for nrhs right-hand sides.  q and y are N x nrhs, column j at
  * offset j*ld (ld >= N), in the caller's ORIGINAL point order.

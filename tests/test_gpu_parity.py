@@ -320,3 +320,38 @@ def test_fp64_batched_matches_fp64_columns(kernel, nrhs):
     dy = torch.zeros_like(dq)
     a.matvec_device(dq.data_ptr(), dy.data_ptr(), nrhs, 32768, precision="fp64_batched")
     np.testing.assert_array_equal(dy.cpu().numpy().T, Yb)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["log", "one_over_r"])
+def test_m2l_on_the_fly_matches_stored_blocks(kernel):
+    """Without stored M2L blocks every precision evaluates the entries on the
+    fly in FP64; the results agree with the stored-block handle to FP64
+    rounding (FP64) or within the mixed tolerance."""
+    pts, _, _ = workloads.make("mixture4m", N=32768)
+    st = A.AFMM(32768, 64, 8, pts, kernel=kernel)
+    st.set_m2l_storage("store")
+    st.assemble()
+    ot = A.AFMM(32768, 64, 8, pts, kernel=kernel)
+    ot.set_m2l_storage("on_the_fly")
+    ot.assemble()
+    assert st.m2l_stored() and not ot.m2l_stored()
+    assert st.counts() == ot.counts()
+    Q = np.random.default_rng(3).standard_normal((32768, 16))
+    for c in (0, 7):
+        y0 = st.computeMatVecProduct(Q[:, c])
+        y1 = ot.computeMatVecProduct(Q[:, c])
+        assert np.linalg.norm(y1 - y0) / np.linalg.norm(y0) <= FP64_BATCHED_TOL
+    Yb = ot.computeMatVecProduct(Q, precision="fp64_batched")
+    Ym = ot.computeMatVecProduct(Q, precision="mixed")
+    ym1 = ot.computeMatVecProduct(Q[:, 5], precision="mixed")
+    for c in (0, 5, 15):
+        y0 = st.computeMatVecProduct(Q[:, c])
+        assert np.linalg.norm(Yb[:, c] - y0) / np.linalg.norm(y0) <= FP64_BATCHED_TOL
+        assert np.linalg.norm(Ym[:, c] - y0) / np.linalg.norm(y0) <= MIXED_TOL
+    y5 = st.computeMatVecProduct(Q[:, 5])
+    assert np.linalg.norm(ym1 - y5) / np.linalg.norm(y5) <= MIXED_TOL
+    with pytest.raises(A.AFMMError):
+        A.AFMMSet([ot])
+    with pytest.raises(A.AFMMError):
+        st.set_m2l_storage("auto")  # after assemble
