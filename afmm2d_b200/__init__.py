@@ -49,6 +49,7 @@ _SIGS = {
     "afmm_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_setup_times": [_vp, _vp],
     "afmm_get_counts": [_vp, _vp],
+    "afmm_get_setup_phases": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_launch_count": [_vp, _vp],
     "afmm_get_stream": [_vp, _vp],
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
@@ -272,7 +273,13 @@ class AFMM:
     def setup_times(self):
         t = np.zeros(2)
         _check(lib().afmm_get_setup_times(self._h, _ptr(t)), self._h)
-        return {"create_s": t[0], "assemble_s": t[1]}
+        out = {"create_s": t[0], "assemble_s": t[1]}
+        n = ctypes.c_int()
+        names = (ctypes.c_char_p * 16)()
+        secs = (ctypes.c_double * 16)()
+        _check(lib().afmm_get_setup_phases(self._h, 16, names, secs, ctypes.byref(n)), self._h)
+        out.update({"assemble_" + names[i].decode() + "_s": secs[i] for i in range(min(n.value, 16))})
+        return out
 
     def counts(self):
         c = np.zeros(7, np.int64)

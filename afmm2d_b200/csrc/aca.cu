@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cfloat>
 
 #include "afmm_internal.cuh"
@@ -716,6 +717,7 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   int32_t* colpiv = scratch.alloc<int32_t>((size_t)in.nbox * rcap);
   a.rowpiv = rowpiv;
   a.colpiv = colpiv;
+  const auto t0 = std::chrono::steady_clock::now();
   dispatch_kernel<AcaRun>(in.kp.id, a, C, ncl, smem, s);
   *launches += 1;
   out.cluster = C;
@@ -724,6 +726,8 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   std::vector<int32_t> h_rank(in.nbox);
   AFMM_CUDA(cudaMemcpyAsync(h_rank.data(), in.rank_out, sizeof(int32_t) * in.nbox, cudaMemcpyDeviceToHost, s));
   AFMM_CUDA(cudaStreamSynchronize(s));
+  const auto t1 = std::chrono::steady_clock::now();
+  out.aca_s = std::chrono::duration<double>(t1 - t0).count();
   out.h_rank = h_rank;
   out.h_skel_off.assign(in.nbox + 1, 0);
   out.h_l2p_off.assign(in.nbox + 1, 0);
@@ -781,6 +785,7 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     *launches += 1;
   }
   AFMM_CUDA(cudaStreamSynchronize(s));
+  out.l2p_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
 }
 
 }  // namespace afmm

@@ -32,6 +32,7 @@ struct AcaLevelOut {
   double* l2p = nullptr;  // per box n x r, column-major
   std::vector<int32_t> h_rank, h_skel_off;
   std::vector<int64_t> h_l2p_off;
+  double aca_s = 0, l2p_s = 0;  // wall clock of the two phases
 };
 
 // Runs the ACA and L2P kernels for one level; outputs are allocated in

@@ -58,6 +58,9 @@ struct afmm_handle {
   double t_create = 0, t_assemble = 0;
   int64_t launches = 0;
   int64_t counts[7] = {0, 0, 0, 0, 0, 0, 0};
+  // assemble phases (wall clock, s): the rest of assemble is host work
+  std::vector<std::pair<std::string, double>> setup_phase{
+      {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}};
   bool have_last = false;
   std::string err;
 };
@@ -419,6 +422,8 @@ void do_assemble(afmm_handle* h) {
     in.rank_out = v.rank;
     AcaLevelOut out;
     aca_level(in, out, h->arena, s, &h->launches);
+    h->setup_phase[0].second += out.aca_s;
+    h->setup_phase[1].second += out.l2p_s;
     v.skel_off = out.skel_off;
     v.skel_ids = out.skel_ids;
     v.cpiv_ids = out.cpiv_ids;
@@ -519,17 +524,25 @@ void do_assemble(afmm_handle* h) {
     v.l2p_rm = h->arena.alloc<double>(v.h_l2p_off[v.nbox]);
   }
   build_plan(h);
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  double t_ph = now_s();
   for (int j = 2; j <= L; ++j) {
     if (h->m2l_stored) {
       m2l_assemble(h->plan.lv[j], h->kp, s);
       ++h->launches;
     }
+  }
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  h->setup_phase[2].second += now_s() - t_ph;
+  t_ph = now_s();
+  for (int j = 2; j <= L; ++j) {
     l2p_transpose(h->plan.lv[j], h->lv[j].l2p, h->lv[j].l2p_rm, s);
     ++h->launches;
   }
   mixed_setup(h->plan, h->lv, h->mixed, h->arena, s, &h->launches);
   build_plan(h);
   AFMM_CUDA(cudaStreamSynchronize(s));
+  h->setup_phase[3].second += now_s() - t_ph;
   // structure counts
   int64_t sum_rank = 0, l2p_entries = 0;
   for (int j = 2; j <= L; ++j) {
@@ -832,6 +845,16 @@ afmm_status afmm_get_setup_times(afmm_handle* h, double* t2) {
   if (!h || !t2) return AFMM_BAD_ARG;
   t2[0] = h->t_create;
   t2[1] = h->t_assemble;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_setup_phases(afmm_handle* h, int cap, const char** names, double* secs, int* n) {
+  if (!h || !n) return AFMM_BAD_ARG;
+  *n = (int)h->setup_phase.size();
+  for (int i = 0; i < *n && i < cap; ++i) {
+    if (names) names[i] = h->setup_phase[i].first.c_str();
+    if (secs) secs[i] = h->setup_phase[i].second;
+  }
   return AFMM_OK;
 }
 

@@ -150,6 +150,12 @@ afmm_status afmm_get_stage_times(afmm_handle* h, int cap, const char** names, do
 afmm_status afmm_get_setup_times(afmm_handle* h, double* t2);
 /* Counts of the assembled structure: [nlevels, N, sum ranks, stored L2P entries,
  * stored M2L entries, near-field kernel evaluations, far-field (M2L) entries]. */
+/* Wall-clock seconds of the assemble phases: ACA kernels ("aca"), L2P solves
+ * ("l2p"), M2L block evaluation ("m2l_blocks"), row-major L2P copy and mixed
+ * setup ("transpose_mixed"); names stay valid for the handle's lifetime.
+ * Replaces the reference's omp_get_wtime prints around assemble
+ * (examples/testAFMM2D.cpp:56-84). */
+afmm_status afmm_get_setup_phases(afmm_handle* h, int cap, const char** names, double* secs, int* n);
 afmm_status afmm_get_counts(afmm_handle* h, int64_t* c7);
 /* Number of kernels this library launched since the handle was created. */
 afmm_status afmm_get_launch_count(afmm_handle* h, int64_t* n);
