@@ -275,10 +275,10 @@ class AFMM:
         _check(lib().afmm_get_setup_times(self._h, _ptr(t)), self._h)
         out = {"create_s": t[0], "assemble_s": t[1]}
         n = ctypes.c_int()
-        names = (ctypes.c_char_p * 16)()
-        secs = (ctypes.c_double * 16)()
-        _check(lib().afmm_get_setup_phases(self._h, 16, names, secs, ctypes.byref(n)), self._h)
-        out.update({"assemble_" + names[i].decode() + "_s": secs[i] for i in range(min(n.value, 16))})
+        names = (ctypes.c_char_p * 32)()
+        secs = (ctypes.c_double * 32)()
+        _check(lib().afmm_get_setup_phases(self._h, 32, names, secs, ctypes.byref(n)), self._h)
+        out.update({"assemble_" + names[i].decode() + "_s": secs[i] for i in range(min(n.value, 32))})
         return out
 
     def counts(self):

@@ -424,6 +424,7 @@ void do_assemble(afmm_handle* h) {
     aca_level(in, out, h->arena, s, &h->launches);
     h->setup_phase[0].second += out.aca_s;
     h->setup_phase[1].second += out.l2p_s;
+    h->setup_phase.push_back({"aca_level" + std::to_string(j), out.aca_s});
     v.skel_off = out.skel_off;
     v.skel_ids = out.skel_ids;
     v.cpiv_ids = out.cpiv_ids;

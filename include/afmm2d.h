@@ -152,7 +152,8 @@ afmm_status afmm_get_setup_times(afmm_handle* h, double* t2);
  * stored M2L entries, near-field kernel evaluations, far-field (M2L) entries]. */
 /* Wall-clock seconds of the assemble phases: ACA kernels ("aca"), L2P solves
  * ("l2p"), M2L block evaluation ("m2l_blocks"), row-major L2P copy and mixed
- * setup ("transpose_mixed"); names stay valid for the handle's lifetime.
+ * setup ("transpose_mixed"), then the ACA time of each level ("aca_levelJ");
+ * names stay valid for the handle's lifetime.
  * Replaces the reference's omp_get_wtime prints around assemble
  * (examples/testAFMM2D.cpp:56-84). */
 afmm_status afmm_get_setup_phases(afmm_handle* h, int cap, const char** names, double* secs, int* n);
