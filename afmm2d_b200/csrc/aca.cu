@@ -635,12 +635,20 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   const int n2max = std::max(in.n2max, 1);
   const int rcap = std::max(1, std::min(n1max, n2max));
   // Cluster size: smallest power of two (<= 16) whose column slice keeps at
-  // least min(rcap, 48) ranks of V in shared memory.  The small per-CTA
-  // arrays go to shared memory first (argmax exchange, column and row
-  // coordinates, flags, per-rank vectors, V-dot exchange) while they fit in
-  // a quarter of the budget; whatever does not fit lives in a per-CTA slot
-  // of global memory.  U then takes up to a quarter and V the rest.
-  const size_t budget = 200 * 1024;
+  // least min(rcap, 48) ranks of V in shared memory -- unless the level has
+  // enough boxes to fill the GPU with smaller clusters (boxes x C >= two CTAs
+  // per SM), in which case boxes run side by side and the V ranks beyond the
+  // shared-memory capacity live in L2-resident global slots.  Many-box levels
+  // use half the shared-memory budget, so two CTAs share an SM.  The small
+  // per-CTA arrays go to shared memory first (argmax exchange, column and row
+  // coordinates, flags, per-rank vectors, V-dot exchange) while they fit in a
+  // quarter of the budget; whatever does not fit lives in a per-CTA slot of
+  // global memory.  U then takes up to a quarter and V the rest.
+  int dev = 0, nsm = 148;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  AFMM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  const long want_ctas = 2L * nsm;
+  const size_t budget = in.nbox >= want_ctas ? 100 * 1024 : 200 * 1024;
   int C = 1, chunk = 0, vcap = 0, ucap = 0;
   size_t smem = 0, gslot = 0;
   size_t off[AR_N] = {0};
@@ -674,7 +682,7 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     used += al(sizeof(double) * (size_t)ucap * n1max);
     size_t left = budget > used ? budget - used : 0;
     vcap = std::min<long>(rcap, (long)(left / (sizeof(double) * chunk)));
-    if (vcap >= std::min(rcap, 48) || C == 16) {
+    if (vcap >= std::min(rcap, 48) || C == 16 || in.nbox * C >= want_ctas) {
       in_smem[AR_V] = 1;
       off[AR_V] = used;
       used += al(sizeof(double) * (size_t)vcap * chunk);
