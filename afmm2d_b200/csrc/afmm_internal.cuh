@@ -41,7 +41,8 @@ struct Error {
 // box anchors; the third argument is the Gaussian parameter).
 // `eval32_pos` is `eval32` for R2 at or above the near-field fallback
 // threshold (R2 > 0 and normal): hardware approximations (flush-to-zero
-// rsqrt, lg2, ex2) with relative error near FP32 rounding.
+// rsqrt, lg2, ex2) with relative error near FP32 rounding, for the TF32x3
+// tensor-core near field (whose operand split allows 2^-21).
 struct KernelParams {
   int id;
   double a;       // 2^-L
@@ -138,7 +139,14 @@ struct KOneOverR {
     float e = fmaf(-R2 * y, y, 1.0f);
     return fmaf(0.5f * y, e, y);
   }
-  __device__ __forceinline__ static float eval32_pos(float R2, float, float) { return rsqrt_nr_ftz(R2); }
+  // rsqrt.approx alone (relative error ~2^-23): the tensor-core near field
+  // splits every entry into two 11-bit TF32 parts (error up to 2^-21), so a
+  // Newton step would not change its result
+  __device__ __forceinline__ static float eval32_pos(float R2, float, float) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(R2));
+    return y;
+  }
 };
 
 // Gaussian exp(-R2/param) (1 on the diagonal).

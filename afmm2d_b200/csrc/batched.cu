@@ -718,7 +718,8 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
             const float dx = x[k].x - ps[h].x, dy = x[k].y - ps[h].y;
             const float r2 = fmaf(dx, dx, dy * dy);
             close |= r2 < thr;
-            kv[k][h] = K::eval32_pos(fmaxf(r2, thr), a32, p32);
+            // close pairs (R2 = 0 among them) are overwritten by the FP64 fallback below
+            kv[k][h] = K::eval32_pos(r2, a32, p32);
           }
         if (__any_sync(0xffffffffu, close)) {
 #pragma unroll
