@@ -79,13 +79,6 @@ struct KOneOverRScaled {
   __device__ __forceinline__ static float eval32_pos(float R2, float a, float p) { return eval32(R2, a, p); }
 };
 
-// rsqrt.approx.ftz.f32 refined by one Newton-Raphson step y += y/2 (1 - x y^2).
-__device__ __forceinline__ float rsqrt_nr_ftz(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  const float e = fmaf(-x * y, y, 1.0f);
-  return fmaf(0.5f * y, e, y);
-}
 
 // log(r) with the diagonal convention (examples/tutorial.cpp:22-35).
 struct KLog {

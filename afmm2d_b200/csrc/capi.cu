@@ -60,7 +60,8 @@ struct afmm_handle {
   int64_t counts[7] = {0, 0, 0, 0, 0, 0, 0};
   // assemble phases (wall clock, s): the rest of assemble is host work
   std::vector<std::pair<std::string, double>> setup_phase{
-      {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}};
+      {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}, {"tables_alloc", 0.0},
+      {"m2l_cudamalloc", 0.0}, {"level_prep", 0.0}, {"aca_alloc_other", 0.0}};
   bool have_last = false;
   std::string err;
 };
@@ -386,6 +387,7 @@ void do_assemble(afmm_handle* h) {
   const int L = h->L;
   double tol = std::pow(10, -1.0 * h->tol_pow);  // src/ACA.cpp:7
   for (int j = L; j >= 2; --j) {
+    const double t_lv = now_s();
     LevelDev& v = h->lv[j];
     if (j < L) {
       // a box's nodes are its children's skeletons (src/AFMM2DTree.cpp:997-1007)
@@ -421,7 +423,10 @@ void do_assemble(afmm_handle* h) {
     v.rank = h->arena.alloc<int32_t>(v.nbox);
     in.rank_out = v.rank;
     AcaLevelOut out;
+    const double t_call = now_s();
+    h->setup_phase[6].second += t_call - t_lv;
     aca_level(in, out, h->arena, s, &h->launches);
+    h->setup_phase[7].second += now_s() - t_call - out.aca_s - out.l2p_s;
     h->setup_phase[0].second += out.aca_s;
     h->setup_phase[1].second += out.l2p_s;
     h->setup_phase.push_back({"aca_level" + std::to_string(j), out.aca_s});
@@ -439,6 +444,7 @@ void do_assemble(afmm_handle* h) {
     v.total_rank = out.h_skel_off[v.nbox];
   }
   // M2L blocks, levels 2..L: sizes first, then the storage decision
+  const double t_tab = now_s();
   int64_t m2l_total = 0, l2p_total = 0, rows_total = 0;
   for (int j = 2; j <= L; ++j) {
     LevelDev& v = h->lv[j];
@@ -473,7 +479,9 @@ void do_assemble(afmm_handle* h) {
     v.m2l_off = h->arena.alloc<int64_t>(v.nbox + 1);
     AFMM_CUDA(cudaMemcpyAsync(v.m2l_off, v.h_m2l_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
     // + 256 B for whole-piece L2 prefetches
+    const double t_al = now_s();
     v.m2l = h->m2l_stored ? h->arena.alloc<double>(v.h_m2l_off[v.nbox] + 32) : nullptr;
+    h->setup_phase[5].second += now_s() - t_al;
     v.qhat = h->arena.alloc<double>(v.total_rank);
     v.yhat = h->arena.alloc<double>(v.total_rank);
     // row -> box maps for the thread-per-row sweeps
@@ -525,6 +533,8 @@ void do_assemble(afmm_handle* h) {
     v.l2p_rm = h->arena.alloc<double>(v.h_l2p_off[v.nbox]);
   }
   build_plan(h);
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  h->setup_phase[4].second += now_s() - t_tab;
   AFMM_CUDA(cudaStreamSynchronize(s));
   double t_ph = now_s();
   for (int j = 2; j <= L; ++j) {

@@ -152,7 +152,11 @@ afmm_status afmm_get_setup_times(afmm_handle* h, double* t2);
  * stored M2L entries, near-field kernel evaluations, far-field (M2L) entries]. */
 /* Wall-clock seconds of the assemble phases: ACA kernels ("aca"), L2P solves
  * ("l2p"), M2L block evaluation ("m2l_blocks"), row-major L2P copy and mixed
- * setup ("transpose_mixed"), then the ACA time of each level ("aca_levelJ");
+ * setup ("transpose_mixed"), sizes, allocations and row tables
+ * ("tables_alloc", of which the M2L block allocation "m2l_cudamalloc"),
+ * per-level host preparation ("level_prep"), the rest of the per-level ACA
+ * call -- scratch allocation, rank offsets ("aca_alloc_other"), then the ACA
+ * time of each level ("aca_levelJ");
  * names stay valid for the handle's lifetime.
  * Replaces the reference's omp_get_wtime prints around assemble
  * (examples/testAFMM2D.cpp:56-84). */
