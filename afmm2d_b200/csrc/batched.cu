@@ -453,7 +453,7 @@ __device__ __forceinline__ void prefetch_l2_bulk(uintptr_t p, uint32_t bytes) {
 // beyond `pos`, in kStep pieces (the last piece may extend < 16 bytes past the
 // region; the block allocation is padded for that).
 struct L2Stream {
-  static constexpr uintptr_t kAhead = 24 * 1024, kStep = 4096;
+  static constexpr uintptr_t kAhead = 12 * 1024, kStep = 4096;
   uintptr_t front, end;
   __device__ __forceinline__ L2Stream(const double* begin, const double* stop)
       : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop) {}
