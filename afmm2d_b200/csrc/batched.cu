@@ -395,7 +395,7 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
 template <int RC, int NT>
 __device__ __forceinline__ void mma_rows(double (&c)[NT][RC / 8][2], const double* __restrict__ A, int lda, int K,
                                          const double* __restrict__ B, const bool (&rowok)[NT], int trow, int tsrc) {
-#pragma unroll 2
+#pragma unroll 4
   for (int k0 = 0; k0 < K; k0 += 4) {
     const int k = k0 + tsrc;
     const bool vk = k < K;
