@@ -70,6 +70,11 @@ def test_null_handle_queries_are_rejected():
     lib = A.lib()
     n = ctypes.c_int()
     assert lib.afmm_get_nlevels(None, ctypes.byref(n)) == 1
+    assert lib.afmm_set_m2l_storage(None, 0) == 1
+    assert lib.afmm_get_m2l_stored(None, ctypes.byref(n)) == 1
+    assert lib.afmm_get_setup_phases(None, 0, None, None, ctypes.byref(n)) == 1
+    assert lib.afmm_set_get_stage_times(None, 0, None, None, ctypes.byref(n)) == 1
+    assert lib.afmm_set_get_stream(None, None) == 1
     assert lib.afmm_destroy(None) == 0
 
 
