@@ -36,9 +36,26 @@ def needs_build():
 
 
 def build(force=False, verbose=False, extra=()):
+    """Compiles every source to an object under _build/ in parallel, then
+    links the shared library."""
     if not force and not needs_build():
         return OUT
-    cmd = [nvcc(), *NVCC_FLAGS, *extra, "-o", OUT] + [os.path.join(CSRC, s) for s in SOURCES]
+    objdir = os.path.join(HERE, "..", "_build")
+    os.makedirs(objdir, exist_ok=True)
+    cflags = [f for f in NVCC_FLAGS if f != "-shared"]
+    procs = []
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        objs.append(obj)
+        cmd = [nvcc(), *cflags, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((src, subprocess.Popen(cmd, cwd=CSRC)))
+    failed = [src for src, p in procs if p.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, "nvcc " + " ".join(failed))
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", OUT, *objs]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=CSRC)

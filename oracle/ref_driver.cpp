@@ -15,6 +15,9 @@
 //   3  Gaussian exp(-R2/p), p = kernel parameter (0.01 by default)
 // log and exp are correctly rounded (cr_math.h), so the entries are a
 // function of the coordinates alone, as on the device.
+//   101  the log kernel exactly as examples/tutorial.cpp:22-35 writes it,
+//        with the host libm's log (not correctly rounded): the stock kernel,
+//        for measuring how far the reference's own output moves with it.
 #include <omp.h>
 
 #include <chrono>
@@ -47,6 +50,10 @@ double userkernel::getMatrixEntry(const unsigned i, const unsigned j) {
       double R = sqrt(R2);
       return 1.0 / R;
     }
+    case 101:
+      if (R2 < 1e-10) return 0.0;
+      if (R2 < a * a) return 0.5 * R2 * log(R2) / a / a;
+      return 0.5 * log(R2);
     default:
       return crm::exp_cr(-R2 / g_kparam);
   }
