@@ -18,7 +18,8 @@ import os
 
 import numpy as np
 
-__all__ = ["AFMM", "AFMMError", "AFMMSet", "KERNELS", "PRECISIONS", "kernel_eval", "lib", "nlevels"]
+__all__ = ["AFMM", "AFMMError", "AFMMSet", "KERNELS", "PRECISIONS", "device_alloc_count", "kernel_eval", "lib",
+           "nlevels"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafmm2d.so")
@@ -55,6 +56,7 @@ _SIGS = {
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
     "afmm_measure_fma_peaks": [_vp, _vp],
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
+    "afmm_get_device_alloc_count": [_vp],
     "afmm_destroy": [_vp],
     "afmm_set_create": [_vp, _i, _vp],
     "afmm_set_matvec": [_vp, _vp, _vp, _i],
@@ -121,6 +123,13 @@ def measure_fma_peaks():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(lib().afmm_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def device_alloc_count():
+    """Device allocations (cudaMalloc) the library has made in this process."""
+    n = ctypes.c_int64()
+    _check(lib().afmm_get_device_alloc_count(ctypes.byref(n)))
+    return n.value
 
 
 def nlevels(N, M):

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -171,6 +172,10 @@ void dispatch_kernel(int id, Args&&... args) {
 }
 
 // ------------------------------------------------------------- allocation
+// Every device allocation of the library goes through DevArena::alloc, which
+// counts it here (read by afmm_get_device_alloc_count).
+std::atomic<int64_t>& device_alloc_counter();
+
 // Device allocations owned by a handle; freed together.
 struct DevArena {
   std::vector<void*> ptrs;
@@ -184,6 +189,7 @@ struct DevArena {
       cudaGetLastError();
       throw Error{AFMM_OOM, "cudaMalloc of " + std::to_string(n * sizeof(T)) + " bytes failed"};
     }
+    device_alloc_counter().fetch_add(1, std::memory_order_relaxed);
     ptrs.push_back(p);
     bytes += n * sizeof(T);
     return (T*)p;

@@ -17,6 +17,11 @@
 
 using namespace afmm;
 
+std::atomic<int64_t>& afmm::device_alloc_counter() {
+  static std::atomic<int64_t> n{0};
+  return n;
+}
+
 struct afmm_set {
   SetPlan plan;
   DevArena arena;
@@ -926,6 +931,12 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
     check_device();
     kd_sort_noalloc(xy, N, L, perm, xy_sorted, (cudaStream_t)stream);
   });
+}
+
+afmm_status afmm_get_device_alloc_count(int64_t* n) {
+  if (!n) return AFMM_BAD_ARG;
+  *n = device_alloc_counter().load();
+  return AFMM_OK;
 }
 
 afmm_status afmm_destroy(afmm_handle* h) {

@@ -19,7 +19,6 @@
 //   3. finishes segments of <= kSmallSeg points inside one CTA (bitonic sorts
 //      of (sub-segment, rank) keys in shared memory), levels down to L.
 #include <algorithm>
-#include <mutex>
 
 #include "afmm_internal.cuh"
 #include "kd_sort.cuh"
@@ -317,8 +316,10 @@ __global__ void k_finish_perm(const int32_t* __restrict__ perm32, const double* 
   if (i < n) {
     int p = perm32[i];
     perm[i] = p;
-    xy_sorted[2 * i] = xy[2 * p];
-    xy_sorted[2 * i + 1] = xy[2 * p + 1];
+    if (xy_sorted) {
+      xy_sorted[2 * i] = xy[2 * p];
+      xy_sorted[2 * i + 1] = xy[2 * p + 1];
+    }
   }
 }
 
@@ -368,97 +369,112 @@ std::vector<std::vector<int64_t>> kd_segment_sizes(int64_t N, int L) {
   return sz;
 }
 
-void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted, cudaStream_t s,
-                    int64_t* launches) {
-  DevArena tmp;
+namespace {
+
+// Device scratch of one KD sort of n points: key and id arrays of n entries
+// each, the radix-pass counts (256 per radix tile) and the segment starts
+// (starts_cap int64).  kd_sort_device takes it from a DevArena,
+// kd_sort_noalloc from the static array below; both run kd_sort_run.
+struct KdScratch {
+  uint64_t *kx = nullptr, *ky = nullptr, *k0 = nullptr, *k1 = nullptr;
+  int32_t *v0 = nullptr, *v1 = nullptr;
+  int32_t *rank_x0 = nullptr, *rank_x = nullptr, *rank_y = nullptr;
+  int32_t *perm_x0 = nullptr, *perm_x = nullptr, *perm_y = nullptr, *perm32 = nullptr;
+  int32_t *seg_of = nullptr, *half_of = nullptr;
+  uint32_t* counts = nullptr;
+  int64_t* starts = nullptr;
+  size_t starts_cap = 0;
+};
+
+// Level below which every segment has at most kSmallSeg points (the top
+// levels split by radix multi-splits, the rest finish inside one CTA).
+int kd_bottom_level(const std::vector<std::vector<int64_t>>& sizes, int L) {
+  int lb = 0;
+  while (lb < L && *std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg) ++lb;
+  if (*std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg)
+    throw Error{AFMM_BAD_ARG, "leaf segments larger than " + std::to_string(kSmallSeg) + " points"};
+  return lb;
+}
+
+// The KD permutation (src/KDTree.cpp:37-243) with the scratch of `sc`:
+// ranks under the three total orders, radix splits of the top levels, CTA
+// sorts of the small segments.  Synchronises `s` before returning.
+void kd_sort_run(const KdScratch& sc, const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted,
+                 cudaStream_t s, int64_t* launches) {
   const int T = 256;
-  uint64_t* kx = tmp.alloc<uint64_t>(N);
-  uint64_t* ky = tmp.alloc<uint64_t>(N);
   RadixCtx rc;
-  rc.k0 = tmp.alloc<uint64_t>(N);
-  rc.k1 = tmp.alloc<uint64_t>(N);
-  rc.v0 = tmp.alloc<int32_t>(N);
-  rc.v1 = tmp.alloc<int32_t>(N);
-  rc.counts = tmp.alloc<uint32_t>((size_t)256 * nblocks(N, RS_TILE));
+  rc.k0 = sc.k0;
+  rc.k1 = sc.k1;
+  rc.v0 = sc.v0;
+  rc.v1 = sc.v1;
+  rc.counts = sc.counts;
   rc.n = N;
   rc.s = s;
   rc.launches = launches;
-  int32_t* rank_x0 = tmp.alloc<int32_t>(N);
-  int32_t* rank_x = tmp.alloc<int32_t>(N);
-  int32_t* rank_y = tmp.alloc<int32_t>(N);
-  int32_t* perm_x0 = tmp.alloc<int32_t>(N);
-  int32_t* perm_x = tmp.alloc<int32_t>(N);
-  int32_t* perm_y = tmp.alloc<int32_t>(N);
-  int32_t* perm32 = tmp.alloc<int32_t>(N);
-  int gb = nblocks(N, T);
+  const int gb = nblocks(N, T);
 
-  k_make_keys<<<gb, T, 0, s>>>(d_xy, N, kx, ky);
+  k_make_keys<<<gb, T, 0, s>>>(d_xy, N, sc.kx, sc.ky);
   // (x asc, index desc)
   k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
+  k_gather_key64<<<gb, T, 0, s>>>(sc.kx, rc.v0, N, 0, rc.k0);
   *launches += 3;
   rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_x0, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  AFMM_CUDA(cudaMemcpyAsync(sc.perm_x0, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
   // (x asc, y desc, index desc)
   k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
-  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 1, rc.k0);
+  k_gather_key64<<<gb, T, 0, s>>>(sc.ky, rc.v0, N, 1, rc.k0);
   *launches += 2;
   rc.sort(0, 64);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
+  k_gather_key64<<<gb, T, 0, s>>>(sc.kx, rc.v0, N, 0, rc.k0);
   *launches += 1;
   rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_x, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  AFMM_CUDA(cudaMemcpyAsync(sc.perm_x, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
   // (y asc, x desc, index asc)
   k_iota<<<gb, T, 0, s>>>(rc.v0, N, 0);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 1, rc.k0);
+  k_gather_key64<<<gb, T, 0, s>>>(sc.kx, rc.v0, N, 1, rc.k0);
   *launches += 2;
   rc.sort(0, 64);
-  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 0, rc.k0);
+  k_gather_key64<<<gb, T, 0, s>>>(sc.ky, rc.v0, N, 0, rc.k0);
   *launches += 1;
   rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_y, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-  k_invert<<<gb, T, 0, s>>>(perm_x0, N, rank_x0);
-  k_invert<<<gb, T, 0, s>>>(perm_x, N, rank_x);
-  k_invert<<<gb, T, 0, s>>>(perm_y, N, rank_y);
+  AFMM_CUDA(cudaMemcpyAsync(sc.perm_y, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+  k_invert<<<gb, T, 0, s>>>(sc.perm_x0, N, sc.rank_x0);
+  k_invert<<<gb, T, 0, s>>>(sc.perm_x, N, sc.rank_x);
+  k_invert<<<gb, T, 0, s>>>(sc.perm_y, N, sc.rank_y);
   *launches += 3;
   AFMM_LAUNCH_CHECK();
 
   // Top levels: split while segments are larger than kSmallSeg.
   auto sizes = kd_segment_sizes(N, L);
-  int lb = 0;
-  while (lb < L && *std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg) ++lb;
-  if (*std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg)
-    throw Error{AFMM_BAD_ARG, "leaf segments larger than " + std::to_string(kSmallSeg) + " points"};
-  if ((int64_t)N >= (1LL << 28)) throw Error{AFMM_BAD_ARG, "N must be below 2^28"};
-  int32_t* seg_of = tmp.alloc<int32_t>(N);   // segment id at the current level
-  int32_t* half_of = tmp.alloc<int32_t>(N);  // half id at the current level
-  const int32_t* seq = nullptr;              // point ids grouped by level-lb segment
+  const int lb = kd_bottom_level(sizes, L);
+  if (2 * sizes[lb].size() + 2 > sc.starts_cap) throw Error{AFMM_BAD_ARG, "too many top-level segments"};
+  const int32_t* seq = nullptr;  // point ids grouped by level-lb segment
   if (lb == 0) {
-    k_iota<<<gb, T, 0, s>>>(perm32, N, 0);
+    k_iota<<<gb, T, 0, s>>>(sc.perm32, N, 0);
     *launches += 1;
-    seq = perm32;
+    seq = sc.perm32;
   }
-  int64_t* d_starts = tmp.alloc<int64_t>((size_t)2 * sizes[lb].size() + 2);
   std::vector<int64_t> h_starts;
   for (int l = 0; l < lb; ++l) {
     size_t ns = sizes[l].size();
     // x-split: group perm_x (perm_x0 at level 0) by segment, split each at n/2.
-    AFMM_CUDA(cudaMemcpyAsync(rc.v0, l == 0 ? perm_x0 : perm_x, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+    AFMM_CUDA(cudaMemcpyAsync(rc.v0, l == 0 ? sc.perm_x0 : sc.perm_x, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice,
+                              s));
     if (l == 0) {
       AFMM_CUDA(cudaMemsetAsync(rc.k0, 0, sizeof(uint64_t) * N, s));
     } else {
-      k_gather_key32<<<gb, T, 0, s>>>(seg_of, rc.v0, N, rc.k0);
+      k_gather_key32<<<gb, T, 0, s>>>(sc.seg_of, rc.v0, N, rc.k0);
       *launches += 1;
       rc.sort(0, 2 * l);
     }
     h_starts.assign(ns + 1, 0);
     for (size_t i = 0; i < ns; ++i) h_starts[i + 1] = h_starts[i] + sizes[l][i];
-    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
-    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, half_of);
+    AFMM_CUDA(cudaMemcpyAsync(sc.starts, h_starts.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
+    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, sc.starts, sc.half_of);
     *launches += 1;
     // y-split: group perm_y by half, split each half at h/2.
-    AFMM_CUDA(cudaMemcpyAsync(rc.v0, perm_y, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-    k_gather_key32<<<gb, T, 0, s>>>(half_of, rc.v0, N, rc.k0);
+    AFMM_CUDA(cudaMemcpyAsync(rc.v0, sc.perm_y, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
+    k_gather_key32<<<gb, T, 0, s>>>(sc.half_of, rc.v0, N, rc.k0);
     *launches += 1;
     rc.sort(0, 2 * l + 1);
     h_starts.assign(2 * ns + 1, 0);
@@ -467,8 +483,8 @@ void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d
       h_starts[2 * i + 1] = h_starts[2 * i] + ln;
       h_starts[2 * i + 2] = h_starts[2 * i + 1] + (sizes[l][i] - ln);
     }
-    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (2 * ns + 1), cudaMemcpyHostToDevice, s));
-    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, seg_of);
+    AFMM_CUDA(cudaMemcpyAsync(sc.starts, h_starts.data(), sizeof(int64_t) * (2 * ns + 1), cudaMemcpyHostToDevice, s));
+    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, sc.starts, sc.seg_of);
     *launches += 1;
     AFMM_CUDA(cudaStreamSynchronize(s));  // h_starts is reused
     AFMM_LAUNCH_CHECK();
@@ -477,24 +493,45 @@ void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d
   size_t nseg = sizes[lb].size();
   h_starts.assign(nseg + 1, 0);
   for (size_t i = 0; i < nseg; ++i) h_starts[i + 1] = h_starts[i] + sizes[lb][i];
-  AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s));
+  AFMM_CUDA(cudaMemcpyAsync(sc.starts, h_starts.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s));
   size_t smem = (size_t)kSmallSeg * 8 + (size_t)kSmallSeg * 4 * 3 + (size_t)(kSmallSeg + 1) * 4 +
                 (size_t)(2 * kSmallSeg + 1) * 4;
   AFMM_CUDA(cudaFuncSetAttribute(k_kd_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int32_t* out32 = (seq == perm32) ? perm_y : perm32;  // perm_y is no longer needed
-  k_kd_bottom<<<(int)nseg, BT_THREADS, smem, s>>>(seq, d_starts, lb, L, rank_x0, rank_x, rank_y, out32);
+  int32_t* out32 = (seq == sc.perm32) ? sc.perm_y : sc.perm32;  // perm_y is no longer needed
+  k_kd_bottom<<<(int)nseg, BT_THREADS, smem, s>>>(seq, sc.starts, lb, L, sc.rank_x0, sc.rank_x, sc.rank_y, out32);
   k_finish_perm<<<gb, T, 0, s>>>(out32, d_xy, N, d_perm, d_xy_sorted);
   *launches += 2;
   AFMM_LAUNCH_CHECK();
   AFMM_CUDA(cudaStreamSynchronize(s));
 }
 
+}  // namespace
+
+void kd_sort_device(const double* d_xy, int N, int L, int64_t* d_perm, double* d_xy_sorted, cudaStream_t s,
+                    int64_t* launches) {
+  if ((int64_t)N >= (1LL << 28)) throw Error{AFMM_BAD_ARG, "N must be below 2^28"};
+  DevArena tmp;
+  KdScratch sc;
+  sc.kx = tmp.alloc<uint64_t>(N);
+  sc.ky = tmp.alloc<uint64_t>(N);
+  sc.k0 = tmp.alloc<uint64_t>(N);
+  sc.k1 = tmp.alloc<uint64_t>(N);
+  for (int32_t** p : {&sc.v0, &sc.v1, &sc.rank_x0, &sc.rank_x, &sc.rank_y, &sc.perm_x0, &sc.perm_x, &sc.perm_y,
+                      &sc.perm32, &sc.seg_of, &sc.half_of})
+    *p = tmp.alloc<int32_t>(N);
+  sc.counts = tmp.alloc<uint32_t>((size_t)256 * nblocks(N, RS_TILE));
+  auto sizes = kd_segment_sizes(N, L);
+  sc.starts_cap = 2 * sizes[kd_bottom_level(sizes, L)].size() + 2;
+  sc.starts = tmp.alloc<int64_t>(sc.starts_cap);
+  kd_sort_run(sc, d_xy, N, L, d_perm, d_xy_sorted, s, launches);
+}
+
 // ------------------------------------------------- allocation-free variant
 // The KD permutation for callers that cannot allocate device memory.  All
 // scratch lives in one file-scope device array (kNoAllocScratchBytes, held by
 // every GPU that loads this library until exit); inputs and outputs are the
-// caller's.  The kernels are the ones above; only the scratch comes from the
-// array instead of cudaMalloc.
+// caller's.  The kernel sequence is kd_sort_run's; only the scratch comes
+// from the array instead of cudaMalloc.
 namespace {
 
 // Layout of the scratch for up to kNoAllocMaxPoints points (each part 256-byte
@@ -510,40 +547,19 @@ static_assert(kNaNeed <= kNoAllocScratchBytes, "scratch array too small for its 
 
 static __device__ __align__(256) unsigned char g_kd_scratch[kNoAllocScratchBytes];
 
-// Device address of g_kd_scratch per device, looked up once per device with
-// that device current (the host-side symbol is not a device address).
-std::mutex g_na_mu;
-void* g_na_addr[64] = {nullptr};
-
+// Device address of g_kd_scratch in the current context.  In host code the
+// symbol is only a host-side stand-in, so the address is looked up on every
+// call with the caller's device current (cheap, and never stale after a
+// context is torn down and recreated).
 unsigned char* scratch_address() {
-  int dev = 0;
-  AFMM_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) throw Error{AFMM_BAD_ARG, "device ordinal out of range"};
-  std::lock_guard<std::mutex> lock(g_na_mu);
-  if (!g_na_addr[dev]) {
-    void* p = nullptr;
-    AFMM_CUDA(cudaGetSymbolAddress(&p, g_kd_scratch));
-    g_na_addr[dev] = p;
-  }
-  return (unsigned char*)g_na_addr[dev];
+  void* p = nullptr;
+  AFMM_CUDA(cudaGetSymbolAddress(&p, g_kd_scratch));
+  return (unsigned char*)p;
 }
 
 __global__ void k_check_finite(const double* __restrict__ xy, int n, int* flag) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n && !(isfinite(xy[2 * i]) && isfinite(xy[2 * i + 1]))) atomicExch(flag, 1);
-}
-
-__global__ void k_finish_perm_na(const int32_t* __restrict__ perm32, const double* __restrict__ xy, int n,
-                                 int64_t* perm, double* xy_sorted) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) {
-    int p = perm32[i];
-    perm[i] = p;
-    if (xy_sorted) {
-      xy_sorted[2 * i] = xy[2 * p];
-      xy_sorted[2 * i + 1] = xy[2 * p + 1];
-    }
-  }
 }
 
 }  // namespace
@@ -559,30 +575,18 @@ void kd_sort_noalloc(const double* d_xy, int N, int L, int64_t* d_perm, double* 
     off += al256(bytes);
     return p;
   };
-  const size_t n8 = kNaPts * 8, n4 = kNaPts * 4;
-  uint64_t* kx = (uint64_t*)carve(n8);
-  uint64_t* ky = (uint64_t*)carve(n8);
-  RadixCtx rc;
-  rc.k0 = (uint64_t*)carve(n8);
-  rc.k1 = (uint64_t*)carve(n8);
-  rc.v0 = (int32_t*)carve(n4);
-  rc.v1 = (int32_t*)carve(n4);
-  int32_t* rank_x0 = (int32_t*)carve(n4);
-  int32_t* rank_x = (int32_t*)carve(n4);
-  int32_t* rank_y = (int32_t*)carve(n4);
-  int32_t* perm_x0 = (int32_t*)carve(n4);
-  int32_t* perm_x = (int32_t*)carve(n4);
-  int32_t* perm_y = (int32_t*)carve(n4);
-  int32_t* perm32 = (int32_t*)carve(n4);
-  int32_t* seg_of = (int32_t*)carve(n4);
-  int32_t* half_of = (int32_t*)carve(n4);
-  rc.counts = (uint32_t*)carve(256 * kNaCountBlocks * 4);
-  int64_t* d_starts = (int64_t*)carve(kNaStarts * 8);
+  KdScratch sc;
+  sc.kx = (uint64_t*)carve(kNaPts * 8);
+  sc.ky = (uint64_t*)carve(kNaPts * 8);
+  sc.k0 = (uint64_t*)carve(kNaPts * 8);
+  sc.k1 = (uint64_t*)carve(kNaPts * 8);
+  for (int32_t** p : {&sc.v0, &sc.v1, &sc.rank_x0, &sc.rank_x, &sc.rank_y, &sc.perm_x0, &sc.perm_x, &sc.perm_y,
+                      &sc.perm32, &sc.seg_of, &sc.half_of})
+    *p = (int32_t*)carve(kNaPts * 4);
+  sc.counts = (uint32_t*)carve(256 * kNaCountBlocks * 4);
+  sc.starts = (int64_t*)carve(kNaStarts * 8);
+  sc.starts_cap = kNaStarts;
   int* flag = (int*)carve(sizeof(int));
-  rc.n = N;
-  rc.s = s;
-  int64_t launches = 0;
-  rc.launches = &launches;
   const int T = 256, gb = nblocks(N, T);
   // the array keeps the previous call's contents: clear the flag
   AFMM_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s));
@@ -592,81 +596,8 @@ void kd_sort_noalloc(const double* d_xy, int N, int L, int64_t* d_perm, double* 
   AFMM_CUDA(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s));
   AFMM_CUDA(cudaStreamSynchronize(s));
   if (h_flag) throw Error{AFMM_BAD_ARG, "a point has a non-finite coordinate"};
-
-  k_make_keys<<<gb, T, 0, s>>>(d_xy, N, kx, ky);
-  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
-  rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_x0, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 1);
-  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 1, rc.k0);
-  rc.sort(0, 64);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 0, rc.k0);
-  rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_x, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-  k_iota<<<gb, T, 0, s>>>(rc.v0, N, 0);
-  k_gather_key64<<<gb, T, 0, s>>>(kx, rc.v0, N, 1, rc.k0);
-  rc.sort(0, 64);
-  k_gather_key64<<<gb, T, 0, s>>>(ky, rc.v0, N, 0, rc.k0);
-  rc.sort(0, 64);
-  AFMM_CUDA(cudaMemcpyAsync(perm_y, rc.v0, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-  k_invert<<<gb, T, 0, s>>>(perm_x0, N, rank_x0);
-  k_invert<<<gb, T, 0, s>>>(perm_x, N, rank_x);
-  k_invert<<<gb, T, 0, s>>>(perm_y, N, rank_y);
-  AFMM_LAUNCH_CHECK();
-
-  auto sizes = kd_segment_sizes(N, L);
-  int lb = 0;
-  while (lb < L && *std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg) ++lb;
-  if (*std::max_element(sizes[lb].begin(), sizes[lb].end()) > kSmallSeg)
-    throw Error{AFMM_BAD_ARG, "leaf segments larger than " + std::to_string(kSmallSeg) + " points"};
-  if (2 * sizes[lb].size() + 2 > kNaStarts) throw Error{AFMM_BAD_ARG, "too many top-level segments"};
-  const int32_t* seq = nullptr;
-  if (lb == 0) {
-    k_iota<<<gb, T, 0, s>>>(perm32, N, 0);
-    seq = perm32;
-  }
-  std::vector<int64_t> h_starts;
-  for (int l = 0; l < lb; ++l) {
-    size_t ns = sizes[l].size();
-    AFMM_CUDA(cudaMemcpyAsync(rc.v0, l == 0 ? perm_x0 : perm_x, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-    if (l == 0) {
-      AFMM_CUDA(cudaMemsetAsync(rc.k0, 0, sizeof(uint64_t) * N, s));
-    } else {
-      k_gather_key32<<<gb, T, 0, s>>>(seg_of, rc.v0, N, rc.k0);
-      rc.sort(0, 2 * l);
-    }
-    h_starts.assign(ns + 1, 0);
-    for (size_t i = 0; i < ns; ++i) h_starts[i + 1] = h_starts[i] + sizes[l][i];
-    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (ns + 1), cudaMemcpyHostToDevice, s));
-    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, half_of);
-    AFMM_CUDA(cudaMemcpyAsync(rc.v0, perm_y, sizeof(int32_t) * N, cudaMemcpyDeviceToDevice, s));
-    k_gather_key32<<<gb, T, 0, s>>>(half_of, rc.v0, N, rc.k0);
-    rc.sort(0, 2 * l + 1);
-    h_starts.assign(2 * ns + 1, 0);
-    for (size_t i = 0; i < ns; ++i) {
-      int64_t ln = sizes[l][i] / 2;
-      h_starts[2 * i + 1] = h_starts[2 * i] + ln;
-      h_starts[2 * i + 2] = h_starts[2 * i + 1] + (sizes[l][i] - ln);
-    }
-    AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (2 * ns + 1), cudaMemcpyHostToDevice, s));
-    k_split_assign<<<gb, T, 0, s>>>(rc.k0, rc.v0, N, d_starts, seg_of);
-    AFMM_CUDA(cudaStreamSynchronize(s));
-    AFMM_LAUNCH_CHECK();
-  }
-  if (lb > 0) seq = rc.v0;
-  size_t nseg = sizes[lb].size();
-  h_starts.assign(nseg + 1, 0);
-  for (size_t i = 0; i < nseg; ++i) h_starts[i + 1] = h_starts[i] + sizes[lb][i];
-  AFMM_CUDA(cudaMemcpyAsync(d_starts, h_starts.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s));
-  size_t smem = (size_t)kSmallSeg * 8 + (size_t)kSmallSeg * 4 * 3 + (size_t)(kSmallSeg + 1) * 4 +
-                (size_t)(2 * kSmallSeg + 1) * 4;
-  AFMM_CUDA(cudaFuncSetAttribute(k_kd_bottom, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int32_t* out32 = (seq == perm32) ? perm_y : perm32;
-  k_kd_bottom<<<(int)nseg, BT_THREADS, smem, s>>>(seq, d_starts, lb, L, rank_x0, rank_x, rank_y, out32);
-  k_finish_perm_na<<<gb, T, 0, s>>>(out32, d_xy, N, d_perm, d_xy_sorted);
-  AFMM_LAUNCH_CHECK();
-  AFMM_CUDA(cudaStreamSynchronize(s));
+  int64_t launches = 0;
+  kd_sort_run(sc, d_xy, N, L, d_perm, d_xy_sorted, s, &launches);
 }
 
 }  // namespace afmm

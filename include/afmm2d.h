@@ -30,7 +30,7 @@
  *   afmm_destroy          AFMM::~AFMM()               include/AFMM2D.hpp:32
  * The user kernel userkernel::getMatrixEntry (include/kernel.hpp:58) is
  * selected by `kernel_id` (see afmm_kernel_id); new kernels are added as
- * device functors (INTEGRATION.md).
+ * device functors.
  *
  * Errors: every call returns an afmm_status; afmm_last_error() gives a
  * message.  Where the reference aborts or has undefined behaviour the engine
@@ -189,15 +189,21 @@ afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
  * a loop that cannot afford a cudaMalloc/cudaFree pair per call (cudaFree
  * synchronises the whole device).  xy (N interleaved x,y), perm (N int64) and
  * xy_sorted (2N doubles, may be NULL) are device pointers owned by the caller;
- * stream is a cudaStream_t (NULL: the default stream); the call returns after
- * the stream has completed the work.  Limit: 1 <= N <= 65,536 points
+ * stream is a cudaStream_t (NULL: the default stream).  The call is
+ * synchronous: it reads a validity flag back from the device and returns
+ * after the stream has completed the work.  Limit: 1 <= N <= 65,536 points
  * (AFMM_BAD_ARG beyond).  Scratch is one static device array of 5 MiB that
- * every GPU loading this library keeps until the process exits; the first call
- * on a device looks up its address (make that first call before any stream
- * capture).  All calls share that array, so calls that overlap on the GPU
- * (other threads or streams) race and must be serialised by the caller. */
+ * every GPU loading this library keeps until the process exits; each call
+ * looks up its address in the current context.  All calls share that array,
+ * so calls that overlap on the GPU (other threads or streams) race and must
+ * be serialised by the caller. */
 afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const double* xy, int64_t* perm,
                                         double* xy_sorted, void* stream);
+
+/* Number of device allocations (cudaMalloc) this library has made in the
+ * process so far, over all handles and sets.  No reference counterpart: a
+ * diagnostic that lets a caller check that a call allocated nothing. */
+afmm_status afmm_get_device_alloc_count(int64_t* n);
 
 afmm_status afmm_destroy(afmm_handle* h);
 

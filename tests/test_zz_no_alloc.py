@@ -35,17 +35,24 @@ def test_no_alloc_permutation_matches_afmm_create(name, N, M):
     dxy = torch.tensor(pts, device="cuda").contiguous()
     perm = torch.empty(N, dtype=torch.int64, device="cuda")
     srt = torch.empty((N, 2), dtype=torch.float64, device="cuda")
-    free = []
     for _ in range(2):  # two calls in a row share the static scratch
         perm.fill_(-1)
         srt.zero_()
-        assert noalloc(N, M, dxy, perm, srt) == 0, A.lib().afmm_last_error(None)
         torch.cuda.synchronize()
-        free.append(torch.cuda.mem_get_info()[0])
+        allocs = A.device_alloc_count()
+        assert noalloc(N, M, dxy, perm, srt) == 0, A.lib().afmm_last_error(None)
+        # the library counts every device allocation it makes: the call made none
+        assert A.device_alloc_count() == allocs
         # integer output: exact agreement is the tolerance
         np.testing.assert_array_equal(perm.cpu().numpy(), ref)
         np.testing.assert_array_equal(srt.cpu().numpy(), pts[ref])
-    assert free[0] == free[1]  # the second call took no device memory
+
+
+def test_alloc_counter_sees_the_allocating_entry_point():
+    pts = workloads.make("uniform1m", N=8192)[0]
+    allocs = A.device_alloc_count()
+    A.AFMM(8192, 32, 6, pts, kernel="log").close()
+    assert A.device_alloc_count() > allocs
 
 
 def test_no_alloc_rejects_sizes_beyond_the_limit():
