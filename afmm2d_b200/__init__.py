@@ -47,6 +47,8 @@ _SIGS = {
     "afmm_set_profiling": [_vp, _i],
     "afmm_set_m2l_storage": [_vp, _i],
     "afmm_get_m2l_stored": [_vp, _vp],
+    "afmm_set_m2l_fixed_point": [_vp, _i],
+    "afmm_get_m2l_fixed_point": [_vp, _vp],
     "afmm_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_setup_times": [_vp, _vp],
     "afmm_get_counts": [_vp, _vp],
@@ -178,6 +180,16 @@ class AFMM:
         """M2L block storage before assemble(): "auto" (store when they fit),
         "store", or "on_the_fly" (entries evaluated in FP64 by every matvec)."""
         _check(lib().afmm_set_m2l_storage(self._h, self.M2L_STORAGE[mode]), self._h)
+
+    def set_m2l_fixed_point(self, on):
+        """Before assemble(): keep a 32-bit fixed-point copy of the stored M2L
+        blocks for the mixed-precision paths (default on, when it fits)."""
+        _check(lib().afmm_set_m2l_fixed_point(self._h, 1 if on else 0), self._h)
+
+    def m2l_fixed_point(self):
+        v = ctypes.c_int()
+        _check(lib().afmm_get_m2l_fixed_point(self._h, ctypes.byref(v)), self._h)
+        return bool(v.value)
 
     def m2l_stored(self):
         v = ctypes.c_int()

@@ -230,6 +230,9 @@ struct LevelDev {
   int32_t* ncgrp_box = nullptr;  // node-row chunk (<= kChunkRows node rows of one box) -> box
   int32_t* ncgrp_row = nullptr;  // node-row chunk -> first node row
   long nncgroups = 0;
+  int32_t* wgrp_box = nullptr;   // row chunk (<= 32 skeleton rows of one box: a warp's lanes) -> box
+  int32_t* wgrp_row = nullptr;   // row chunk -> first skeleton row
+  long nwgroups = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)
@@ -239,6 +242,12 @@ struct LevelDev {
   double* l2p_rm = nullptr;     // the same, row-major (rank index fastest)
   int64_t* m2l_off = nullptr;   // nbox+1 prefix over sum_slots r_b*r_c
   double* m2l = nullptr;        // per box, per valid slot, block r_b x r_c column-major
+  // The same blocks in 32-bit fixed point (the mixed-precision paths): entry
+  // e of block (b, slot s) is (u - 2^31) * 2^k with u = m2l_q[e] and 2^k the
+  // block's power-of-two scale; m2l_dec[b * 40 + s] = (2^k, -(2^52 + 2^31) 2^k)
+  // decodes it with one FMA (see decode_q32).
+  uint32_t* m2l_q = nullptr;
+  double2* m2l_dec = nullptr;
   double* qhat = nullptr;       // outgoing charges, skel_off layout
   double* yhat = nullptr;       // incoming potentials, skel_off layout
   // host copies

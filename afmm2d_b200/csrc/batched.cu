@@ -7,7 +7,8 @@
 // source with one broadcast load.
 //  * M2M / L2L: FP64 L2P (row-major / column-major), one thread per output
 //    row with RC FP64 accumulators.
-//  * M2L: the stored FP64 blocks (one HBM read for all RC columns), or
+//  * M2L: the stored blocks (one HBM read for all RC columns; the 32-bit
+//    fixed-point copy in mixed precision, the FP64 blocks otherwise), or
 //    entries evaluated on the fly in FP64 from the skeleton coordinates when
 //    no blocks are stored, multiplied with the RC-column charge blocks on the
 //    FP64 tensor cores (8 rows x 4 sources tiles).
@@ -412,6 +413,34 @@ __device__ __forceinline__ void mma_rows(double (&c)[NT][RC / 8][2], const doubl
   }
 }
 
+// mma_rows with the 32-bit fixed-point M2L entries of one block (decode
+// constants `dec`, decode_q32): each 4-column step loads its A entries as
+// 32-bit words (half the bytes of FP64) and decodes them exactly before the
+// FP64 products.
+template <int RC, int NT>
+__device__ __forceinline__ void mma_rows_q32(double (&c)[NT][RC / 8][2], const uint32_t* __restrict__ A, int lda,
+                                             int K, double2 dec, const double* __restrict__ B,
+                                             const bool (&rowok)[NT], int trow, int tsrc) {
+#pragma unroll 4
+  for (int k0 = 0; k0 < K; k0 += 4) {
+    const int k = k0 + tsrc;
+    const bool vk = k < K;
+    const uint32_t* Ak = A + (long)k * lda;
+    uint32_t ua[NT];
+    double bq[RC / 8];
+#pragma unroll
+    for (int u = 0; u < NT; ++u) ua[u] = (vk && rowok[u]) ? Ak[u * 8] : 0x80000000u;  // 2^31 decodes to 0
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) bq[t] = vk ? B[(long)k * RC + t * 8 + trow] : 0.0;
+#pragma unroll
+    for (int u = 0; u < NT; ++u) {
+      const double a = decode_q32(ua[u], dec);
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) mma_f64_8x8x4(c[u][t][0], c[u][t][1], a, bq[t]);
+    }
+  }
+}
+
 template <int RC, int NT>
 __device__ __forceinline__ void zero_tiles(double (&c)[NT][RC / 8][2]) {
 #pragma unroll
@@ -442,41 +471,13 @@ __device__ __forceinline__ void store_tiles(const double (&c)[NT][RC / 8][2], do
   }
 }
 
-// L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned
-// start, size a multiple of 16).  Issued by one lane.
-__device__ __forceinline__ void prefetch_l2_bulk(uintptr_t p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-// Streams a box's contiguous M2L region into L2 ahead of the warp that
-// consumes it in order: `advance(pos)` keeps the prefetched front kAhead bytes
-// beyond `pos`, in kStep pieces (the last piece may extend < 16 bytes past the
-// region; the block allocation is padded for that).
-struct L2Stream {
-  static constexpr uintptr_t kAhead = 12 * 1024, kStep = 4096;
-  uintptr_t front, end;
-  __device__ __forceinline__ L2Stream(const double* begin, const double* stop)
-      : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop) {}
-  __device__ __forceinline__ void advance(const double* pos, int lane) {
-    uintptr_t upto = (uintptr_t)pos + kAhead;
-    if (upto > end) upto = end;
-    while (front < upto) {  // warp-uniform
-      if (lane == 0) {
-        const uintptr_t left = (end - front + 15) & ~(uintptr_t)15;
-        prefetch_l2_bulk(front, (uint32_t)(left < kStep ? left : kStep));
-      }
-      front += kStep;
-    }
-  }
-};
-
 // M2L from the stored FP64 blocks (the same blocks the FP64 path applies)
 // with FP64 tensor-core tiles: one warp per chunk of up to kChunkRows skeleton
 // rows of one box, i.e. NT <= 5 tiles of 8 rows that share every B fragment.
 // The 40 slots' rank and skeleton offset are fetched once per warp and
 // broadcast by shuffles; the box's contiguous block region is streamed into
 // L2 ahead of the loads.
-template <int RC, int NT>
+template <int RC, int NT, bool Q32>
 __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const double* __restrict__ qh,
                                                  double* __restrict__ yb, int b, int r0, int lane) {
   const int r = v.rank[b];
@@ -491,17 +492,25 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
   bool rowok[NT];
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
-  const double* Mb = v.m2l + v.m2l_off[b];  // block of the current slot
-  L2Stream pf(Mb, v.m2l + v.m2l_off[b + 1]);
+  long pos = v.m2l_off[b];  // first entry of the current slot's block
+  const long stop = v.m2l_off[b + 1];
+  L2Stream pf(Q32 ? (const void*)(v.m2l_q + pos) : (const void*)(v.m2l + pos),
+              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop));
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   for (int s = 0; s < 40; ++s) {
     const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
     if (rc == 0) continue;  // empty slot or rank-0 box: no block stored
     const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
-    pf.advance(Mb, lane);
-    mma_rows<RC, NT>(c, Mb + i0 + trow, r, rc, qh + (long)sc * RC, rowok, trow, tsrc);
-    Mb += (long)r * rc;
+    if (Q32) {
+      pf.advance(v.m2l_q + pos, lane);
+      mma_rows_q32<RC, NT>(c, v.m2l_q + pos + i0 + trow, r, rc, v.m2l_dec[(long)b * 40 + s], qh + (long)sc * RC,
+                           rowok, trow, tsrc);
+    } else {
+      pf.advance(v.m2l + pos, lane);
+      mma_rows<RC, NT>(c, v.m2l + pos + i0 + trow, r, rc, qh + (long)sc * RC, rowok, trow, tsrc);
+    }
+    pos += (long)r * rc;
   }
   store_tiles<RC, NT, false>(c, yb + (long)r0 * RC, rowok, trow, tsrc);
 }
@@ -593,7 +602,7 @@ __global__ void __launch_bounds__(128) k_l2l_mma(LevelView v, const double* __re
 #undef AFMM_L2L
 }
 
-template <int RC>
+template <int RC, bool Q32>
 __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const double* const* __restrict__ qhat_lv,
                                                         double* const* __restrict__ yhat_lv) {
   const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -605,7 +614,7 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
   const long g = gw - ls.cgrp0[j];
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
-#define AFMM_M2L(NT) m2l_stored_chunk<RC, NT>(v, qhat_lv[j], yhat_lv[j], b, r0, lane)
+#define AFMM_M2L(NT) m2l_stored_chunk<RC, NT, Q32>(v, qhat_lv[j], yhat_lv[j], b, r0, lane)
   AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2L)
 #undef AFMM_M2L
 }
@@ -891,12 +900,17 @@ struct Pass {
   template <class K>
   struct M2l {
     static void run(const LevelSet& ls, const KernelParams& kp, const double* const* qh, double* const* yh,
-                    cudaStream_t s) {
+                    int fp64, cudaStream_t s) {
       constexpr int RM = RC >= 8 ? RC : 8;
-      if (RC >= 8 && ls.lv[0].m2l != nullptr) {
+      if (ls.row0[ls.nlev] == 0) return;  // every box of ACA rank 0: no far field
+      if (RC >= 8 && !fp64 && ls.lv[0].m2l_q != nullptr) {
+        // mixed precision: the 32-bit fixed-point blocks (half the bytes)
+        const long warps = ls.cgrp0[ls.nlev];
+        k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
+      } else if (RC >= 8 && ls.lv[0].m2l != nullptr) {
         // stored blocks: one HBM read of the blocks serves all RC columns
         const long warps = ls.cgrp0[ls.nlev];
-        k_m2l_stored_mma<RM><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
+        k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
       } else if (RC >= 8) {
         const long warps = ls.grp0[ls.nlev];
         k_m2l_mma<K, RM><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
@@ -958,7 +972,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "m2l");
-    dispatch_kernel<M2l>(p.kp.id, p.levels, p.kp, bs.d_qhat_lv, bs.d_yhat_lv, s);
+    dispatch_kernel<M2l>(p.kp.id, p.levels, p.kp, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
     ++*launches;
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {

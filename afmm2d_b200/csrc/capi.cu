@@ -37,6 +37,8 @@ struct afmm_handle {
   int device = 0;
   int m2l_mode = AFMM_M2L_AUTO;  // afmm_m2l_storage
   bool m2l_stored = false;
+  int m2l_q_mode = 1;            // also keep a 32-bit fixed-point copy for the mixed paths
+  bool m2l_q_stored = false;
   KernelParams kp{};
   cudaStream_t stream = nullptr;
   DevArena arena;
@@ -267,6 +269,11 @@ void build_plan(afmm_handle* h) {
     v.ncgrp_box = d.ncgrp_box;
     v.ncgrp_row = d.ncgrp_row;
     v.nncgroups = d.nncgroups;
+    v.wgrp_box = d.wgrp_box;
+    v.wgrp_row = d.wgrp_row;
+    v.nwgroups = d.nwgroups;
+    v.m2l_q = d.m2l_q;
+    v.m2l_dec = d.m2l_dec;
     v.nrows = d.total_rank;
     v.nnodes = d.h_node_off.empty() ? 0 : d.h_node_off[d.nbox];
   }
@@ -274,11 +281,13 @@ void build_plan(afmm_handle* h) {
   p.levels.row0[0] = 0;
   p.levels.grp0[0] = 0;
   p.levels.cgrp0[0] = 0;
+  p.levels.wgrp0[0] = 0;
   for (int j = 2; j <= h->L; ++j) {
     p.levels.lv[p.levels.nlev] = p.lv[j];
     p.levels.row0[p.levels.nlev + 1] = p.levels.row0[p.levels.nlev] + p.lv[j].nrows;
     p.levels.grp0[p.levels.nlev + 1] = p.levels.grp0[p.levels.nlev] + p.lv[j].ngroups;
     p.levels.cgrp0[p.levels.nlev + 1] = p.levels.cgrp0[p.levels.nlev] + p.lv[j].ncgroups;
+    p.levels.wgrp0[p.levels.nlev + 1] = p.levels.wgrp0[p.levels.nlev] + p.lv[j].nwgroups;
     ++p.levels.nlev;
   }
   for (int j = 0; j <= h->L; ++j) {
@@ -496,17 +505,22 @@ void do_assemble(afmm_handle* h) {
     fill_box_map(v.node_off, v.nbox, v.node_box, s);
     h->launches += 2;
     // row groups of at most 8 skeleton rows of one box (on-the-fly M2L
-    // tiles), and balanced chunks of at most kChunkRows skeleton rows
-    // (M2L / M2M tiles) or node rows (L2L tiles): a box of n rows is cut into
-    // ceil(n / kChunkRows) chunks of equal size rounded up to 8 rows
-    for (int span : {8, kChunkRows, -kChunkRows}) {
+    // tiles), balanced chunks of at most kChunkRows skeleton rows (M2L / M2M
+    // tiles) or node rows (L2L tiles): a box of n rows is cut into
+    // ceil(n / kChunkRows) chunks of equal size rounded up to 8 rows; and
+    // balanced chunks of at most 32 skeleton rows (a warp's lanes, the
+    // one-column M2L)
+    for (int kind = 0; kind < 4; ++kind) {
+      const int span = kind == 0 ? 8 : (kind == 3 ? 32 : kChunkRows);
+      const bool nodes = kind == 2;
       std::vector<int32_t> gb, gr;
       for (long b = 0; b < v.nbox; ++b) {
-        const int rows = span > 0 ? v.h_rank[b] : v.h_node_off[b + 1] - v.h_node_off[b];
-        const int first = span > 0 ? v.h_skel_off[b] : v.h_node_off[b];
-        const int nch = (rows + std::abs(span) - 1) / std::abs(span);
-        const int step = nch > 0 ? ((rows + nch - 1) / nch + 7) / 8 * 8 : 0;
-        for (int i = 0; i < rows; i += (span == 8 ? 8 : step)) {
+        const int rows = nodes ? v.h_node_off[b + 1] - v.h_node_off[b] : v.h_rank[b];
+        const int first = nodes ? v.h_node_off[b] : v.h_skel_off[b];
+        const int nch = (rows + span - 1) / span;
+        int step = nch > 0 ? (rows + nch - 1) / nch : 0;
+        if (kind == 1 || kind == 2) step = (step + 7) / 8 * 8;
+        for (int i = 0; i < rows; i += (kind == 0 ? 8 : step)) {
           gb.push_back((int32_t)b);
           gr.push_back(first + i);
         }
@@ -518,18 +532,22 @@ void do_assemble(afmm_handle* h) {
         AFMM_CUDA(cudaMemcpyAsync(dr, gr.data(), sizeof(int32_t) * gr.size(), cudaMemcpyHostToDevice, s));
         AFMM_CUDA(cudaStreamSynchronize(s));
       }
-      if (span == 8) {
+      if (kind == 0) {
         v.ngroups = (long)gb.size();
         v.grp_box = db;
         v.grp_row = dr;
-      } else if (span == kChunkRows) {
+      } else if (kind == 1) {
         v.ncgroups = (long)gb.size();
         v.cgrp_box = db;
         v.cgrp_row = dr;
-      } else {
+      } else if (kind == 2) {
         v.nncgroups = (long)gb.size();
         v.ncgrp_box = db;
         v.ncgrp_row = dr;
+      } else {
+        v.nwgroups = (long)gb.size();
+        v.wgrp_box = db;
+        v.wgrp_row = dr;
       }
     }
   }
@@ -550,6 +568,31 @@ void do_assemble(afmm_handle* h) {
   }
   AFMM_CUDA(cudaStreamSynchronize(s));
   h->setup_phase[2].second += now_s() - t_ph;
+  // 32-bit fixed-point copy of the blocks for the mixed-precision paths, when
+  // it fits beside the rest (half the bytes of the FP64 blocks)
+  if (h->m2l_stored && h->m2l_q_mode) {
+    size_t free_b = 0, total_b = 0;
+    AFMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const double need = 4.0 * (double)m2l_total;
+    const double reserve = 8.0 * (double)l2p_total + (double)h->N * (16 * 8 * 4 + 64) +
+                           (double)rows_total * 16 * 8 * 2 + 2e9;
+    if (need <= (double)free_b - reserve) {
+      t_ph = now_s();
+      for (int j = 2; j <= L; ++j) {
+        LevelDev& v = h->lv[j];
+        v.m2l_q = h->arena.alloc<uint32_t>(v.h_m2l_off[v.nbox] + 64);  // + 256 B for whole-piece L2 prefetches
+        v.m2l_dec = h->arena.alloc<double2>((size_t)v.nbox * 40);
+      }
+      build_plan(h);
+      for (int j = 2; j <= L; ++j) {
+        m2l_compress(h->plan.lv[j], s);
+        ++h->launches;
+      }
+      AFMM_CUDA(cudaStreamSynchronize(s));
+      h->m2l_q_stored = true;
+      h->setup_phase[2].second += now_s() - t_ph;
+    }
+  }
   t_ph = now_s();
   for (int j = 2; j <= L; ++j) {
     l2p_transpose(h->plan.lv[j], h->lv[j].l2p, h->lv[j].l2p_rm, s);
@@ -832,6 +875,22 @@ afmm_status afmm_set_m2l_storage(afmm_handle* h, int mode) {
     return AFMM_BAD_ARG;
   }
   h->m2l_mode = mode;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on) {
+  if (!h) return AFMM_BAD_ARG;
+  if (h->assembled) {
+    h->err = "afmm_set_m2l_fixed_point after afmm_assemble";
+    return AFMM_BAD_ARG;
+  }
+  h->m2l_q_mode = on ? 1 : 0;
+  return AFMM_OK;
+}
+
+afmm_status afmm_get_m2l_fixed_point(afmm_handle* h, int* stored) {
+  if (!h || !stored) return AFMM_BAD_ARG;
+  *stored = h->m2l_q_stored ? 1 : 0;
   return AFMM_OK;
 }
 

@@ -128,6 +128,81 @@ void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s) {
   dispatch_kernel<M2lAssembleRun>(kp.id, v, kp, s);
 }
 
+// 32-bit fixed-point copy of the FP64 blocks: per block a power-of-two scale
+// 2^k with max|M| * 2^-k in [2^30, 2^31), entries rounded to the nearest
+// multiple of 2^k (absolute error <= 2^-31 max|M|) and stored offset by 2^31
+// as unsigned.  A block whose largest entry is 0 or below 2^-960 decodes to
+// zeros; a block holding a non-finite entry decodes to NaN (as the FP64
+// blocks would propagate it).  One CTA per box.
+__global__ void __launch_bounds__(256) k_m2l_compress(LevelView v) {
+  const long b = blockIdx.x;
+  const int r = v.rank[b];
+  __shared__ double red[8];
+  __shared__ double2 s_dec;
+  const double* M = v.m2l + v.m2l_off[b];
+  uint32_t* Q = v.m2l_q + v.m2l_off[b];
+  long off = 0;
+  for (int s = 0; s < 40; ++s) {
+    const int c = v.il[b * 40 + s];
+    const int rc = (c >= 0 && r > 0) ? v.rank[c] : 0;
+    const long n = (long)r * rc;
+    if (n == 0) {
+      if (threadIdx.x == 0) v.m2l_dec[b * 40 + s] = make_double2(0.0, 0.0);
+      continue;
+    }
+    double mx = 0.0;
+    bool bad = false;
+    for (long e = threadIdx.x; e < n; e += blockDim.x) {
+      const double x = M[off + e];
+      bad |= !isfinite(x);
+      mx = fmax(mx, fabs(x));
+    }
+    if (bad) mx = __longlong_as_double(0x7ff0000000000000ll);  // +inf
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+      int ex = 0;
+      frexp(m, &ex);  // m in [2^(ex-1), 2^ex)
+      const int k = ex - 31;
+      if (!isfinite(m)) {
+        const double nan = __longlong_as_double(0x7ff8000000000000ll);
+        s_dec = make_double2(nan, nan);
+      } else if (m == 0.0 || k < -960) {
+        s_dec = make_double2(0.0, 0.0);
+      } else {
+        const double sc = scalbn(1.0, k);
+        s_dec = make_double2(sc, -(4503601774854144.0 * sc));  // 2^52 + 2^31
+      }
+      v.m2l_dec[b * 40 + s] = s_dec;
+    }
+    __syncthreads();
+    const double2 dec = s_dec;
+    const bool zero = !(dec.x != 0.0) || !isfinite(dec.x);
+    int ex = 0;
+    if (!zero) frexp(dec.x, &ex);
+    const int k = ex - 1;  // dec.x = 2^k
+    for (long e = threadIdx.x; e < n; e += blockDim.x) {
+      uint32_t u = 0x80000000u;
+      if (!zero) {
+        long long t = llrint(scalbn(M[off + e], -k)) + 0x80000000ll;
+        t = t < 0 ? 0 : (t > 0xffffffffll ? 0xffffffffll : t);
+        u = (uint32_t)t;
+      }
+      Q[off + e] = u;
+    }
+    off += n;
+    __syncthreads();
+  }
+}
+
+void m2l_compress(const LevelView& v, cudaStream_t s) {
+  k_m2l_compress<<<(int)v.nbox, 256, 0, s>>>(v);
+  AFMM_LAUNCH_CHECK();
+}
+
 // ---------------------------------------------------------------- sweeps
 // qs[i] = q[perm[i]]  (src/AFMM2D.cpp:49-51)
 __global__ void k_gather(const double* __restrict__ q, const int64_t* __restrict__ perm, int n, double* qs) {
@@ -168,21 +243,86 @@ void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_
   AFMM_LAUNCH_CHECK();
 }
 
-// Level of flat row g of a LevelSet (row0 is its prefix of row counts).
-__device__ __forceinline__ int level_of_row(const LevelSet& ls, long g) {
+// Level of flat warp chunk g of a LevelSet (wgrp0: prefix of chunk counts).
+__device__ __forceinline__ int level_of_wchunk(const LevelSet& ls, long g) {
   int j = 0;
-  while (j + 1 < ls.nlev && g >= ls.row0[j + 1]) ++j;
+  while (j + 1 < ls.nlev && g >= ls.wgrp0[j + 1]) ++j;
   return j;
 }
 
-// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch, one thread
-// per skeleton row (upper levels first); the column-major blocks let a warp's
-// consecutive rows read contiguously.
-__global__ void k_m2l_apply(LevelSet ls) {
-  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ls.row0[ls.nlev]) return;
-  const int j = level_of_row(ls, g);
-  m2l_row(ls.lv[j], g - ls.row0[j]);
+// M2L (src/AFMM2DTree.cpp:1156-1178) for every level in one launch, one warp
+// per chunk of up to 32 skeleton rows of one box, lane = row.  Each row's
+// arithmetic is m2l_row's (slots in the reference's order, four partial sums
+// per block), so the result has the same bits as the thread-per-row form; the
+// warp's loads of one block column are contiguous, every lane of a warp
+// takes the same slots, and the box's block region is streamed into L2 ahead
+// of the loads.  Q32: the 32-bit fixed-point blocks (decode_q32) instead of
+// the FP64 ones (the single-RHS mixed path).
+template <bool Q32>
+__global__ void __launch_bounds__(128) k_m2l_apply_w(LevelSet ls) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ls.wgrp0[ls.nlev]) return;  // whole warps only
+  const int j = level_of_wchunk(ls, gw);
+  const LevelView& v = ls.lv[j];
+  const long g = gw - ls.wgrp0[j];
+  const int b = v.wgrp_box[g];
+  const int r0 = v.wgrp_row[g];
+  const int box_end = v.skel_off[b] + v.rank[b];
+  const int next = g + 1 < v.nwgroups ? min(box_end, v.wgrp_row[g + 1]) : box_end;
+  const int r = v.rank[b];
+  const int i = r0 - v.skel_off[b] + lane;
+  const bool act = lane < next - r0;
+  // slot table: lane l holds slot l (and slot 32 + l for l < 8)
+  const int sa = v.il[(long)b * 40 + lane];
+  const int sb = lane < 8 ? v.il[(long)b * 40 + 32 + lane] : -1;
+  const int ra = sa >= 0 ? v.rank[sa] : 0, rb = sb >= 0 ? v.rank[sb] : 0;
+  const int oa = sa >= 0 ? v.skel_off[sa] : 0, ob = sb >= 0 ? v.skel_off[sb] : 0;
+  const long base = v.m2l_off[b];
+  const long stop = v.m2l_off[b + 1];
+  long pos = base;  // first entry of the current slot's block
+  L2Stream pf(Q32 ? (const void*)(v.m2l_q + base) : (const void*)(v.m2l + base),
+              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop));
+  double acc = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
+    if (rc == 0) continue;  // empty slot or rank-0 box: no block stored
+    const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
+    const double* qc = v.qhat + sc;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int cc = 0;
+    if (Q32) {
+      const double2 dec = v.m2l_dec[(long)b * 40 + s];
+      pf.advance(v.m2l_q + pos, lane);
+      const uint32_t* M = v.m2l_q + pos + i;
+#define AFMM_ENT(c) (act ? decode_q32(M[(long)(c) * r], dec) : 0.0)
+#pragma unroll 2
+      for (; cc + 3 < rc; cc += 4) {
+        a0 += AFMM_ENT(cc) * qc[cc];
+        a1 += AFMM_ENT(cc + 1) * qc[cc + 1];
+        a2 += AFMM_ENT(cc + 2) * qc[cc + 2];
+        a3 += AFMM_ENT(cc + 3) * qc[cc + 3];
+      }
+      for (; cc < rc; ++cc) a0 += AFMM_ENT(cc) * qc[cc];
+#undef AFMM_ENT
+    } else {
+      pf.advance(v.m2l + pos, lane);
+      const double* M = v.m2l + pos + i;
+#define AFMM_ENT(c) (act ? M[(long)(c) * r] : 0.0)
+#pragma unroll 2
+      for (; cc + 3 < rc; cc += 4) {
+        a0 += AFMM_ENT(cc) * qc[cc];
+        a1 += AFMM_ENT(cc + 1) * qc[cc + 1];
+        a2 += AFMM_ENT(cc + 2) * qc[cc + 2];
+        a3 += AFMM_ENT(cc + 3) * qc[cc + 3];
+      }
+      for (; cc < rc; ++cc) a0 += AFMM_ENT(cc) * qc[cc];
+#undef AFMM_ENT
+    }
+    acc += (a0 + a1) + (a2 + a3);
+    pos += (long)r * rc;
+  }
+  if (act) v.yhat[r0 + lane] = acc;
 }
 
 // L2L (src/AFMM2DTree.cpp:1180-1197): one thread per node row of the level.
@@ -237,7 +377,16 @@ void m2l_apply(const MatvecPlan& p, cudaStream_t s) {
     m2l_apply_otf(p, s);
     return;
   }
-  k_m2l_apply<<<(int)((rows + 127) / 128), 128, 0, s>>>(p.levels);
+  const long warps = p.levels.wgrp0[p.levels.nlev];
+  k_m2l_apply_w<false><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(p.levels);
+  AFMM_LAUNCH_CHECK();
+}
+
+void m2l_apply_q32(const MatvecPlan& p, cudaStream_t s) {
+  const long warps = p.levels.wgrp0[p.levels.nlev];
+  if (warps == 0) return;
+  if (p.levels.lv[0].m2l_q == nullptr) throw Error{AFMM_BAD_ARG, "no fixed-point M2L blocks stored"};
+  k_m2l_apply_w<true><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(p.levels);
   AFMM_LAUNCH_CHECK();
 }
 

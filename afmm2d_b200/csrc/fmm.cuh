@@ -48,6 +48,11 @@ struct LevelView {
   const int32_t* ncgrp_box = nullptr;  // node-row chunk (<= kChunkRows node rows of one box) -> box
   const int32_t* ncgrp_row = nullptr;  // node-row chunk -> first node row
   long nncgroups = 0;
+  const int32_t* wgrp_box = nullptr;  // row chunk (<= 32 skeleton rows of one box) -> box
+  const int32_t* wgrp_row = nullptr;  // row chunk -> first skeleton row
+  long nwgroups = 0;
+  uint32_t* m2l_q = nullptr;          // 32-bit fixed-point blocks (null when not stored)
+  double2* m2l_dec = nullptr;         // per (box, slot) decode constants
   long nrows = 0;                     // skeleton rows (sum of ranks)
   long nnodes = 0;                    // node rows (sum of node counts)
 };
@@ -60,7 +65,43 @@ struct LevelSet {
   long row0[kMaxLevels + 1] = {0};
   long grp0[kMaxLevels + 1] = {0};   // prefix of row-group counts
   long cgrp0[kMaxLevels + 1] = {0};  // prefix of row-chunk counts
+  long wgrp0[kMaxLevels + 1] = {0};  // prefix of warp row-chunk counts
 };
+
+// L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned
+// start, size a multiple of 16).  Issued by one lane.
+__device__ __forceinline__ void prefetch_l2_bulk(uintptr_t p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Streams a box's contiguous M2L region into L2 ahead of the warp that
+// consumes it in order: `advance(pos)` keeps the prefetched front kAhead bytes
+// beyond `pos`, in kStep pieces (the last piece may extend < 16 bytes past the
+// region; the block allocations are padded for that).
+struct L2Stream {
+  static constexpr uintptr_t kAhead = 12 * 1024, kStep = 4096;
+  uintptr_t front, end;
+  __device__ __forceinline__ L2Stream(const void* begin, const void* stop)
+      : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop) {}
+  __device__ __forceinline__ void advance(const void* pos, int lane) {
+    uintptr_t upto = (uintptr_t)pos + kAhead;
+    if (upto > end) upto = end;
+    while (front < upto) {  // warp-uniform
+      if (lane == 0) {
+        const uintptr_t left = (end - front + 15) & ~(uintptr_t)15;
+        prefetch_l2_bulk(front, (uint32_t)(left < kStep ? left : kStep));
+      }
+      front += kStep;
+    }
+  }
+};
+
+// Value of a 32-bit fixed-point M2L entry: the double with high word
+// 0x43300000 and low word u is 2^52 + u exactly, so one FMA with the block's
+// decode constants (2^k, -(2^52 + 2^31) 2^k) gives (u - 2^31) 2^k exactly.
+__device__ __forceinline__ double decode_q32(uint32_t u, double2 dec) {
+  return fma(__hiloint2double(0x43300000, (int)u), dec.x, dec.y);
+}
 
 // Leaf-level data for the near field.
 struct NearView {
@@ -293,11 +334,15 @@ void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s);
 // iperm[perm[i]] = i
 void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
+// 32-bit fixed-point copy of the stored FP64 blocks (m2l_q, m2l_dec).
+void m2l_compress(const LevelView& v, cudaStream_t s);
 void l2p_transpose(const LevelView& v, const double* cm, double* rm, cudaStream_t s);
 void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s, StageTimer* tm, int64_t* launches);
 // M2L of every level in FP64: the stored blocks (one thread per skeleton row),
 // or m2l_apply_otf when no blocks are stored.
 void m2l_apply(const MatvecPlan& p, cudaStream_t s);
+// M2L of every level from the 32-bit fixed-point blocks (FP64 arithmetic).
+void m2l_apply_q32(const MatvecPlan& p, cudaStream_t s);
 // M2L of every level with the entries evaluated on the fly in FP64 (mixed.cu).
 void m2l_apply_otf(const MatvecPlan& p, cudaStream_t s);
 // The FP64 sweeps shared by both precisions (leaf charges qs in FP64).

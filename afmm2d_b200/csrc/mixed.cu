@@ -3,12 +3,14 @@
 //
 // Same sweeps as the FP64 path (src/AFMM2DTree.cpp:1129-1213), changed in two
 // places:
-//  * M2L is evaluated on the fly from the skeleton coordinates instead of
-//    streaming stored blocks: the blocks are plain kernel entries between
-//    skeleton points (src/AFMM2DTree.cpp:1080), so the 8-byte-per-entry read
-//    becomes one FP64 kernel evaluation per entry.  It stays in FP64 because
-//    the outgoing charges are combinations with large, mixed-sign weights
-//    (ACA interpolation matrices) and FP32 entries lose ~10x to cancellation.
+//  * M2L reads the 32-bit fixed-point copy of the blocks (half the bytes of
+//    FP64; entries within 2^-31 of their block's largest) or evaluates the
+//    entries on the fly from the skeleton coordinates (the blocks are plain
+//    kernel entries between skeleton points, src/AFMM2DTree.cpp:1080),
+//    whichever the first matvec measures faster.  The arithmetic stays FP64
+//    because the outgoing charges are combinations with large, mixed-sign
+//    weights (ACA interpolation matrices) and FP32 entries lose ~10x to
+//    cancellation.
 //  * The near field is evaluated in FP32 from coordinates relative to a
 //    per-leaf anchor point (anchor differences formed in FP64 before
 //    rounding, so dx keeps ~2^-24 relative precision however clustered the
@@ -121,6 +123,7 @@ template <class K>
 struct M2lOtfRun {
   static void run(const LevelSet& ls, const KernelParams& kp, cudaStream_t s) {
     const long rows = ls.row0[ls.nlev];
+    if (rows == 0) return;  // every box of ACA rank 0: no far field
     k_m2l_otf<K><<<(int)((rows + 127) / 128), 128, 0, s>>>(ls, kp);
     AFMM_LAUNCH_CHECK();
   }
@@ -289,7 +292,13 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     if (tm) tm->mark(s, "m2m");
     sweep_m2m(p, ms.qs, s, launches);
     if (tm) tm->mark(s, "m2l");
-    const bool stored = p.levels.nlev > 0 && p.levels.lv[0].m2l != nullptr;
+    // stored form: the 32-bit fixed-point blocks when kept, else the FP64 ones
+    const bool q32 = p.levels.nlev > 0 && p.levels.lv[0].m2l_q != nullptr;
+    const bool stored = q32 || (p.levels.nlev > 0 && p.levels.lv[0].m2l != nullptr);
+    auto m2l_stored_form = [&] {
+      if (q32) m2l_apply_q32(p, s);
+      else m2l_apply(p, s);
+    };
     if (ms.m2l_form < 0 && stored) {
       // one-time choice: both forms write the same yhat (to FP64 rounding);
       // time each once on this problem and keep the faster
@@ -298,7 +307,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
       AFMM_CUDA(cudaEventRecord(e[0], s));
       dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);
       AFMM_CUDA(cudaEventRecord(e[1], s));
-      m2l_apply(p, s);
+      m2l_stored_form();
       AFMM_CUDA(cudaEventRecord(e[2], s));
       AFMM_CUDA(cudaEventSynchronize(e[2]));
       AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[0], e[0], e[1]));
@@ -311,7 +320,7 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
         ++*launches;
       }
     } else if (ms.m2l_form == 1 && stored) {
-      m2l_apply(p, s);
+      m2l_stored_form();
       ++*launches;
     } else {
       dispatch_kernel<M2lOtfRun>(p.kp.id, p.levels, p.kp, s);

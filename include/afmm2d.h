@@ -71,7 +71,8 @@ typedef enum {
 
 typedef enum {
   AFMM_PREC_FP64 = 0,        /* plain FP64 apply (stored operators), column by column */
-  AFMM_PREC_MIXED = 1,       /* FP32 apply with FP64 where it matters */
+  AFMM_PREC_MIXED = 1,       /* FP32 near field (FP64 for close pairs), far field in FP64
+                                arithmetic on 32-bit fixed-point M2L blocks */
   AFMM_PREC_FP64_BATCHED = 2 /* FP64 throughout, 8 or 16 columns per pass on the FP64 tensor
                                 cores; agrees with AFMM_PREC_FP64 to FP64 rounding (the
                                 summation order differs) */
@@ -110,6 +111,17 @@ afmm_status afmm_assemble(afmm_handle* h);
 afmm_status afmm_set_m2l_storage(afmm_handle* h, int mode);
 /* 1 when the assembled handle stores its M2L blocks. */
 afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored);
+/* Whether assembly also keeps a 32-bit fixed-point copy of the stored M2L
+ * blocks for AFMM_PREC_MIXED (on by default, when it fits in device memory),
+ * before afmm_assemble.  No reference counterpart (the reference keeps FP64
+ * blocks only, src/AFMM2DTree.cpp:1070-1097).  Each block carries a
+ * power-of-two scale; its entries are stored as 32-bit integers of that
+ * scale, within 2^-31 of the block's largest entry, and applied in FP64
+ * arithmetic: half the bytes of the FP64 blocks.  AFMM_PREC_FP64 and
+ * AFMM_PREC_FP64_BATCHED always apply the FP64 blocks. */
+afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on);
+/* 1 when the assembled handle keeps the fixed-point copy. */
+afmm_status afmm_get_m2l_fixed_point(afmm_handle* h, int* stored);
 
 /* y = K q for nrhs right-hand sides.  q and y are N x nrhs, column j at
  * offset j*ld (ld >= N), in the caller's ORIGINAL point order.
