@@ -70,7 +70,18 @@ struct afmm_handle {
       {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}, {"tables_alloc", 0.0},
       {"m2l_cudamalloc", 0.0}, {"level_prep", 0.0}, {"aca_alloc_other", 0.0}};
   bool have_last = false;
+  // host-pointer matvecs: copy streams and pass width (0: automatic)
+  cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+  cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
+  cudaEvent_t ev_sync = nullptr;
+  int host_pass_cols = 0;
   std::string err;
+  ~afmm_handle() {
+    for (cudaEvent_t e : {ev_in[0], ev_in[1], ev_done[0], ev_done[1], ev_out[0], ev_out[1], ev_sync})
+      if (e) cudaEventDestroy(e);
+    if (s_h2d) cudaStreamDestroy(s_h2d);
+    if (s_d2h) cudaStreamDestroy(s_d2h);
+  }
 };
 
 namespace {
@@ -323,6 +334,11 @@ void do_create(afmm_handle* h, const double* loc, int layout) {
   check_device();
   AFMM_CUDA(cudaGetDevice(&h->device));
   AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&h->ev_in[0], &h->ev_in[1], &h->ev_done[0], &h->ev_done[1], &h->ev_out[0], &h->ev_out[1],
+                         &h->ev_sync})
+    AFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
   cudaStream_t s = h->stream;
   double* d_xy = h->arena.alloc<double>(2 * (size_t)N);
   AFMM_CUDA(cudaMemcpyAsync(d_xy, xy.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
@@ -684,6 +700,57 @@ afmm_status afmm_assemble(afmm_handle* h) {
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+// Host-pointer matvec: passes of at most W columns, each copied in on the
+// h2d stream, computed on the handle's stream and copied out on the d2h
+// stream, with two staging buffers so that the copies of one pass overlap the
+// computation of its neighbours.  compute(qd, yd, nc) runs nc columns from
+// device staging (leading dimension N) on the handle's stream.
+template <class F>
+void host_pipeline(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int W, F&& compute) {
+  const int N = h->N;
+  const size_t need = 2 * (size_t)W;
+  if (h->mixed.host_cap < need) {
+    if (h->mixed.d_qin) h->arena.release(h->mixed.d_qin);
+    if (h->mixed.d_yout) h->arena.release(h->mixed.d_yout);
+    mixed_reserve_io(h->mixed, N, (int)need, h->arena);
+  }
+  cudaStream_t s = h->stream, si = h->s_h2d, so = h->s_d2h;
+  const size_t bytes = sizeof(double) * (size_t)N;
+  // the copy streams start after the work already queued on the handle's stream
+  AFMM_CUDA(cudaEventRecord(h->ev_sync, s));
+  AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_sync, 0));
+  AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_sync, 0));
+  int k = 0;
+  for (int c0 = 0; c0 < nrhs; c0 += W, ++k) {
+    const int nc = std::min(W, nrhs - c0), buf = k & 1;
+    double* qb = h->mixed.d_qin + (size_t)buf * W * N;
+    double* yb = h->mixed.d_yout + (size_t)buf * W * N;
+    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_done[buf], 0));  // pass k-2 has read qb
+    for (int c = 0; c < nc; ++c)
+      AFMM_CUDA(cudaMemcpyAsync(qb + (size_t)c * N, q + (size_t)(c0 + c) * ld, bytes, cudaMemcpyHostToDevice, si));
+    AFMM_CUDA(cudaEventRecord(h->ev_in[buf], si));
+    AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_in[buf], 0));
+    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_out[buf], 0));  // pass k-2's results have left yb
+    compute(qb, yb, nc);
+    AFMM_CUDA(cudaEventRecord(h->ev_done[buf], s));
+    AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_done[buf], 0));
+    for (int c = 0; c < nc; ++c)
+      AFMM_CUDA(cudaMemcpyAsync(y + (size_t)(c0 + c) * ld, yb + (size_t)c * N, bytes, cudaMemcpyDeviceToHost, so));
+    AFMM_CUDA(cudaEventRecord(h->ev_out[buf], so));
+  }
+  // the handle's stream ends after the last copy out
+  AFMM_CUDA(cudaEventRecord(h->ev_sync, so));
+  AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_sync, 0));
+}
+
+}  // namespace
+
+extern "C" {
+
 afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int precision,
                         int mem_device) {
   if (!h) return AFMM_BAD_ARG;
@@ -692,50 +759,39 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
     if (!q || !y || nrhs < 1 || ld < h->N) throw Error{AFMM_BAD_ARG, "bad q/y/nrhs/ld"};
     if (precision != AFMM_PREC_FP64 && precision != AFMM_PREC_MIXED && precision != AFMM_PREC_FP64_BATCHED)
       throw Error{AFMM_BAD_ARG, "bad precision"};
-    // one column in FP64 batched mode is the plain FP64 apply
-    if (precision == AFMM_PREC_FP64_BATCHED && nrhs == 1) precision = AFMM_PREC_FP64;
     cudaStream_t s = h->stream;
-    const size_t bytes = sizeof(double) * (size_t)h->N;
     if (h->profiling) h->timer.reset();
     StageTimer* tm = h->profiling ? &h->timer : nullptr;
-    if (precision == AFMM_PREC_MIXED || precision == AFMM_PREC_FP64_BATCHED) {
-      const int fp64 = precision == AFMM_PREC_FP64_BATCHED;
+    if (precision != AFMM_PREC_FP64) {
       mixed_reserve(h->mixed, h->N, 1, h->arena);
       if (nrhs > 1) batch_reserve(h->plan, h->batch, h->arena, s);
-      auto run = [&](const double* qq, int64_t ldq, double* yy, int64_t ldy) {
-        if (nrhs > 1) matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nrhs, fp64, s, tm, &h->launches);
-        else matvec_mixed(h->plan, h->mixed, qq, ldq, yy, ldy, nrhs, s, tm, &h->launches);
-      };
-      if (!mem_device) {
-        if (h->mixed.host_cap < (size_t)nrhs) mixed_reserve_io(h->mixed, h->N, nrhs, h->arena);
-        if (tm) tm->mark(s, "h2d");
-        for (int c = 0; c < nrhs; ++c)
-          AFMM_CUDA(cudaMemcpyAsync(h->mixed.d_qin + (size_t)c * h->N, q + (size_t)c * ld, bytes, cudaMemcpyHostToDevice, s));
-        run(h->mixed.d_qin, h->N, h->mixed.d_yout, h->N);
-        if (tm) tm->mark(s, "d2h");
-        for (int c = 0; c < nrhs; ++c)
-          AFMM_CUDA(cudaMemcpyAsync(y + (size_t)c * ld, h->mixed.d_yout + (size_t)c * h->N, bytes, cudaMemcpyDeviceToHost, s));
-      } else {
-        run(q, ld, y, ld);
-      }
-      if (tm) tm->mark(s, "end");
-    } else {
-      for (int c = 0; c < nrhs; ++c) {
-        const double* qc = q + (size_t)c * ld;
-        double* yc = y + (size_t)c * ld;
-        if (!mem_device) {
-          if (tm) tm->mark(s, "h2d");
-          AFMM_CUDA(cudaMemcpyAsync(h->d_q, qc, bytes, cudaMemcpyHostToDevice, s));
-          matvec_fp64(h->plan, h->d_q, h->d_y, s, tm, &h->launches);
-          if (tm) tm->mark(s, "d2h");
-          AFMM_CUDA(cudaMemcpyAsync(yc, h->d_y, bytes, cudaMemcpyDeviceToHost, s));
-          if (tm) tm->mark(s, "end");
-        } else {
-          matvec_fp64(h->plan, qc, yc, s, tm, &h->launches);
-        }
-      }
-      h->have_last = true;
     }
+    // nc columns (leading dimensions ldq, ldy) on the handle's stream; one
+    // column in FP64 batched mode is the plain FP64 apply
+    auto compute = [&](const double* qq, int64_t ldq, double* yy, int64_t ldy, int nc) {
+      if (precision == AFMM_PREC_FP64 || (precision == AFMM_PREC_FP64_BATCHED && nc == 1)) {
+        for (int c = 0; c < nc; ++c)
+          matvec_fp64(h->plan, qq + (size_t)c * ldq, yy + (size_t)c * ldy, s, tm, &h->launches);
+        h->have_last = true;
+      } else if (nc > 1) {
+        matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nc, precision == AFMM_PREC_FP64_BATCHED, s, tm,
+                       &h->launches);
+      } else {
+        matvec_mixed(h->plan, h->mixed, qq, ldq, yy, ldy, 1, s, tm, &h->launches);
+      }
+    };
+    if (mem_device) {
+      compute(q, ld, y, ld, nrhs);
+    } else {
+      // pass width: one column for the column-by-column FP64 apply; for the
+      // batched modes at most 8 columns, so that 16 columns make two passes
+      // whose copies overlap each other's computation
+      int W = 1;
+      if (precision != AFMM_PREC_FP64) W = h->host_pass_cols > 0 ? h->host_pass_cols : std::min(nrhs, 8);
+      host_pipeline(h, q, y, nrhs, ld, W,
+                    [&](const double* qd, double* yd, int nc) { compute(qd, h->N, yd, h->N, nc); });
+    }
+    if (tm) tm->mark(s, "end");
     AFMM_CUDA(cudaStreamSynchronize(s));
     if (tm) tm->collect(h->stage_ms);
   });
