@@ -766,14 +766,16 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
       mixed_reserve(h->mixed, h->N, 1, h->arena);
       if (nrhs > 1) batch_reserve(h->plan, h->batch, h->arena, s);
     }
-    // nc columns (leading dimensions ldq, ldy) on the handle's stream; one
-    // column in FP64 batched mode is the plain FP64 apply
+    // nc columns (leading dimensions ldq, ldy) on the handle's stream.  A
+    // one-column call in FP64 batched mode is the plain FP64 apply, and in
+    // mixed mode the single-RHS path; every pass of a multi-column call takes
+    // the batched passes, so that host and device calls give the same bits
     auto compute = [&](const double* qq, int64_t ldq, double* yy, int64_t ldy, int nc) {
-      if (precision == AFMM_PREC_FP64 || (precision == AFMM_PREC_FP64_BATCHED && nc == 1)) {
+      if (precision == AFMM_PREC_FP64 || (precision == AFMM_PREC_FP64_BATCHED && nrhs == 1)) {
         for (int c = 0; c < nc; ++c)
           matvec_fp64(h->plan, qq + (size_t)c * ldq, yy + (size_t)c * ldy, s, tm, &h->launches);
         h->have_last = true;
-      } else if (nc > 1) {
+      } else if (nrhs > 1) {
         matvec_batched(h->plan, h->mixed, h->batch, qq, ldq, yy, ldy, nc, precision == AFMM_PREC_FP64_BATCHED, s, tm,
                        &h->launches);
       } else {

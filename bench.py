@@ -189,7 +189,11 @@ def run_ours(args):
     pts, q, p = workloads.make(args.workload, N=args.N)
     N = len(pts)
     Q = np.random.Generator(np.random.PCG64(p["seed"] + 1)).standard_normal((N, R))
-    Q[:, 0] = q
+    if q.ndim == 2:  # workloads with several charge vectors (gauss1m: 64)
+        k = min(R, q.shape[1])
+        Q[:, :k] = q[:, :k]
+    else:
+        Q[:, 0] = q
     # warm process: CUDA context and the library's kernels loaded by a small
     # problem of the same kernel first; the cold figure of a fresh process is
     # reported beside it
@@ -302,7 +306,19 @@ def run_ours(args):
     sb = stages["batched"]
     dom = max((k for k in sb if k not in ("end", "h2d", "d2h")), key=lambda k: sb[k])
     rows = counts["sum_rank"]
-    if dom == "m2l":
+    fixed = a.m2l_fixed_point()
+    nbox = sum(4 ** j for j in range(2, counts["nlevels"] + 1))
+    if dom == "m2l" and fixed:
+        byts = counts["m2l_entries"] * 4 + nbox * 40 * 16 + 2 * rows * R * 8
+        roof = {"bound": "hbm",
+                "kernel": "k_m2l_stored_mma<Q32> (32-bit fixed-point M2L blocks, FP64 tensor-core tiles)",
+                "unit": "GB/s", "achieved": byts / (sb[dom] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
+                "algorithmic_bytes": byts,
+                "byte_definition": "4 B per stored M2L entry (read once) + 16 B decode constants per (box, slot) + "
+                                   "nrhs*8 B per skeleton row in and out",
+                "ms": sb[dom]}
+        roof["traffic"] = scaled_traffic("k_m2l_stored_mma_q32", byts)
+    elif dom == "m2l":
         byts = counts["m2l_entries"] * 8 + 2 * rows * R * 8
         roof = {"bound": "hbm", "kernel": "k_m2l_stored_mma (stored FP64 M2L blocks, FP64 tensor-core tiles)",
                 "unit": "GB/s", "achieved": byts / (sb[dom] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
@@ -324,7 +340,7 @@ def run_ours(args):
     # the FP64 path's stored M2L is HBM-bound
     s64 = stages["fp64"]
     m2l_bytes = counts["m2l_entries"] * 8
-    roof64 = {"bound": "hbm", "kernel": "k_m2l_apply (stored FP64 M2L, one RHS)", "unit": "GB/s",
+    roof64 = {"bound": "hbm", "kernel": "k_m2l_apply_w (stored FP64 M2L, one RHS, warp per row chunk)", "unit": "GB/s",
               "achieved": m2l_bytes / (s64["m2l"] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
               "algorithmic_bytes": m2l_bytes, "ms": s64["m2l"]}
     roof64["frac"] = roof64["achieved"] / hbm
@@ -332,7 +348,8 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": t_dev["batched"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "N": N, "kernel": p["kernel"], "M": p["M"], "TOL_POW": p["tol"],
-                       "nrhs": R, "precision": "mixed, batched", "l2": "flushed (256 MB write) before every timed step",
+                       "nrhs": R, "precision": "mixed, batched", "m2l_blocks": "fixed32" if fixed else "fp64",
+                       "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"replicas x{world}"},
             "paths": {name: {"ms_per_step": t_dev[name], "nrhs": paths[name][1],
                              "points_rhs_per_s": world * N * paths[name][1] / (t_dev[name] * 1e-3),
@@ -355,6 +372,32 @@ def run_ours(args):
             line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             line["cpu_baseline"]["setup_s"] = cb["setup_s"]
             line["fp64_gpu_vs_cpu_reference_matvec"] = (N / (t_dev["fp64"] * 1e-3)) / cb["value"]
+            n_s = min(args.cpu_sample, N)
+            if n_s < N:
+                # the FP64 GPU path on the reference's own sample (equal N)
+                s_pts, s_q, s_p = workloads.make(args.workload, N=n_s)
+                s_q = s_q[:, 0] if s_q.ndim == 2 else s_q
+                sa = A.AFMM(n_s, s_p["M"], s_p["tol"], s_pts, kernel=s_p["kernel"])
+                sa.assemble()
+                dq_s = torch.from_numpy(np.ascontiguousarray(s_q)).to(dev)
+                dy_s = torch.empty_like(dq_s)
+                st_s = torch.cuda.ExternalStream(sa.stream())
+                for _ in range(3):
+                    sa.matvec_device(dq_s.data_ptr(), dy_s.data_ptr(), 1, n_s, "fp64")
+                ms_s = []
+                for _ in range(10):
+                    with torch.cuda.stream(st_s):
+                        flush.zero_()
+                    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e0.record(st_s)
+                    sa.matvec_device(dq_s.data_ptr(), dy_s.data_ptr(), 1, n_s, "fp64")
+                    e1.record(st_s)
+                    e1.synchronize()
+                    ms_s.append(e0.elapsed_time(e1))
+                t_s = float(np.mean(ms_s))
+                line["fp64_gpu_same_n"] = {"N": n_s, "ms_per_step": t_s, "points_per_s": n_s / (t_s * 1e-3),
+                                           "vs_cpu_reference": (n_s / (t_s * 1e-3)) / cb["value"]}
+                sa.close()
             if full:
                 yr = cb["y"]
                 line["rel_err_fp64_vs_reference"] = float(np.linalg.norm(y64[:, 0] - yr) / np.linalg.norm(yr))
