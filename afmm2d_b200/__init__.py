@@ -33,11 +33,14 @@ _vp, _i, _i64, _u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_ui
 _SIGS = {
     "afmm_create": [_i, _i, _i, _vp, _i, _i, _vp, _i, _vp],
     "afmm_assemble": [_vp],
+    "afmm_save": [_vp, ctypes.c_char_p],
+    "afmm_load": [ctypes.c_char_p, _vp],
     "afmm_matvec": [_vp, _vp, _vp, _i, _i64, _i, _i],
     "afmm_eval_error": [_vp, _i, _u64, _vp],
     "afmm_get_permutation": [_vp, _vp],
     "afmm_get_sorted_locations": [_vp, _vp],
     "afmm_get_nlevels": [_vp, _vp],
+    "afmm_get_params": [_vp, _vp, _vp],
     "afmm_get_leaves": [_vp, _vp, _vp],
     "afmm_get_lists": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_ranks": [_vp, _i, _vp],
@@ -149,8 +152,11 @@ class AFMM:
     permutation and the interaction lists on the GPU (src/AFMM2D.cpp:3-39).
     """
 
-    def __init__(self, N, MinParticlesInLeaf, TOL_POW, loc, kernel="log", kparam=None):
+    def __init__(self, N, MinParticlesInLeaf, TOL_POW, loc, kernel="log", kparam=None, _handle=None):
         L = lib()
+        if _handle is not None:  # AFMM.load
+            self._adopt(_handle)
+            return
         kid = KERNELS[kernel] if isinstance(kernel, str) else int(kernel)
         loc = np.ascontiguousarray(np.asarray(loc, dtype=np.float64).reshape(N, 2))
         kp = np.array([kparam if kparam is not None else 0.01], dtype=np.float64)
@@ -167,6 +173,26 @@ class AFMM:
         _check(L.afmm_get_nlevels(h, ctypes.byref(n)), h)
         self.nLevels = n.value
         self.assembled = False
+
+    def _adopt(self, h):
+        self._h = h
+        v = np.zeros(5, np.int32)
+        _check(lib().afmm_get_params(h, _ptr(v), None), h)
+        self.N, self.MinParticlesInLeaf, self.TOL_POW, self.nLevels, self.kernel_id = (int(x) for x in v)
+        self.assembled = True
+
+    def save(self, path):
+        """Writes the assembled setup (permutation, ranks, skeletons, L2P) to
+        a versioned binary file that AFMM.load reads back."""
+        _check(lib().afmm_save(self._h, os.fsencode(path)), self._h)
+
+    @classmethod
+    def load(cls, path):
+        """An assembled AFMM from a file written by save(), without the KD
+        sort and the ACA; its matvecs have the same bits as the saved one's."""
+        h = ctypes.c_void_p()
+        _check(lib().afmm_load(os.fsencode(path), ctypes.byref(h)))
+        return cls(0, 0, 0, None, _handle=h)
 
     # ------------------------------------------------------- reference API
     def assemble(self):

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <new>
 #include <string>
@@ -314,6 +315,19 @@ void build_plan(afmm_handle* h) {
   nv.nbr = h->lv[h->L].nbr;
 }
 
+void create_layout(afmm_handle* h);
+
+// Streams and events of a handle (afmm_create, afmm_load).
+void create_streams(afmm_handle* h) {
+  AFMM_CUDA(cudaGetDevice(&h->device));
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
+  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&h->ev_in[0], &h->ev_in[1], &h->ev_done[0], &h->ev_done[1], &h->ev_out[0], &h->ev_out[1],
+                         &h->ev_sync})
+    AFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+}
+
 void do_create(afmm_handle* h, const double* loc, int layout) {
   const int N = h->N, L = h->L;
   std::vector<double> xy(2 * (size_t)N);
@@ -332,23 +346,26 @@ void do_create(afmm_handle* h, const double* loc, int layout) {
     if (nmax > 1024) throw Error{AFMM_BAD_ARG, "leaf size " + std::to_string(nmax) + " exceeds 1024; use a smaller M"};
   }
   check_device();
-  AFMM_CUDA(cudaGetDevice(&h->device));
-  AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
-  AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
-  for (cudaEvent_t* e : {&h->ev_in[0], &h->ev_in[1], &h->ev_done[0], &h->ev_done[1], &h->ev_out[0], &h->ev_out[1],
-                         &h->ev_sync})
-    AFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  create_streams(h);
   cudaStream_t s = h->stream;
   double* d_xy = h->arena.alloc<double>(2 * (size_t)N);
   AFMM_CUDA(cudaMemcpyAsync(d_xy, xy.data(), sizeof(double) * 2 * N, cudaMemcpyHostToDevice, s));
   h->d_perm = h->arena.alloc<int64_t>(N);
   h->d_pts = h->arena.alloc<double2>(N);
   kd_sort_device(d_xy, N, L, h->d_perm, (double*)h->d_pts, s, &h->launches);
+  h->arena.release(d_xy);
+  create_layout(h);
+}
+
+// Everything of afmm_create after the KD sort (d_perm and d_pts set): the
+// inverse permutation, the leaf layout, the lists of every level and the
+// matvec buffers.
+void create_layout(afmm_handle* h) {
+  const int N = h->N, L = h->L;
+  cudaStream_t s = h->stream;
   h->d_iperm = h->arena.alloc<int32_t>(N);
   invert_permutation(h->d_perm, N, h->d_iperm, s);
   ++h->launches;
-  h->arena.release(d_xy);
   // Leaf layout: DFS leaf d owns a contiguous sorted range; its quadtree box
   // number follows src/KDTree.cpp:211-223 (children 4p+0, 4p+3, 4p+1, 4p+2).
   auto sizes = kd_segment_sizes(N, L);
@@ -412,6 +429,8 @@ void do_create(afmm_handle* h, const double* loc, int layout) {
   AFMM_CUDA(cudaStreamSynchronize(s));
 }
 
+void finish_assemble(afmm_handle* h);
+
 void do_assemble(afmm_handle* h) {
   cudaStream_t s = h->stream;
   const int L = h->L;
@@ -473,6 +492,16 @@ void do_assemble(afmm_handle* h) {
     v.rmax = out.rmax;
     v.total_rank = out.h_skel_off[v.nbox];
   }
+  finish_assemble(h);
+}
+
+// Everything of afmm_assemble after the skeletons (rank, skel_off/ids, cpiv,
+// skel_xy, l2p and their host copies of every level 2..L): M2L block sizes
+// and storage, row tables, M2L blocks (FP64 and fixed point), the row-major
+// L2P copy, the mixed-precision set-up and the structure counts.
+void finish_assemble(afmm_handle* h) {
+  cudaStream_t s = h->stream;
+  const int L = h->L;
   // M2L blocks, levels 2..L: sizes first, then the storage decision
   const double t_tab = now_s();
   int64_t m2l_total = 0, l2p_total = 0, rows_total = 0;
@@ -645,6 +674,264 @@ void do_assemble(afmm_handle* h) {
   h->assembled = true;
 }
 
+// ------------------------------------------------------- setup files
+// Versioned binary image of an assembled handle (afmm_save / afmm_load):
+// everything ACA decided -- the KD permutation and sorted points, and per
+// level the ranks, skeletons (incoming check points), pivot columns and L2P
+// operators -- so that a later process skips the KD sort and the ACA.  The
+// lists, row tables and M2L blocks are rebuilt from these by the same code
+// as afmm_assemble, so a loaded handle's matvecs have the bits of the
+// original's.  Layout (little-endian, native widths):
+//   char[8] "AFMM2DB\n"; u32 version; u32 0x01020304 (byte order check)
+//   i32 N, M, TOL_POW, L, kernel id, M2L storage mode, fixed-point flag, 0
+//   f64 a, kernel parameter
+//   f64 sorted points [2N]; i64 permutation [N]
+//   per level j = L..2: i64 boxes, i64 skeleton rows, i64 L2P entries;
+//     i32 ranks [boxes]; i32 skeleton ids [rows]; i32 pivot columns [rows];
+//     f64 L2P [entries] (per box n_b x r_b, column-major)
+//   u64 FNV-1a digest (64-bit words, then the tail bytes) of all bytes before
+constexpr char kSetupMagic[8] = {'A', 'F', 'M', 'M', '2', 'D', 'B', '\n'};
+constexpr uint32_t kSetupVersion = 1;
+
+struct Fnv64 {
+  uint64_t h = 1469598103934665603ull;
+  void add(const void* p, size_t n) {
+    const unsigned char* b = (const unsigned char*)p;
+    size_t w = n / 8;
+    for (size_t i = 0; i < w; ++i) {
+      uint64_t x;
+      std::memcpy(&x, b + 8 * i, 8);
+      h = (h ^ x) * 1099511628211ull;
+    }
+    for (size_t i = 8 * w; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+  }
+};
+
+struct SetupWriter {
+  FILE* f = nullptr;
+  Fnv64 dig;
+  explicit SetupWriter(const char* path) : f(std::fopen(path, "wb")) {
+    if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot open ") + path + " for writing"};
+  }
+  ~SetupWriter() {
+    if (f) std::fclose(f);
+  }
+  void put(const void* p, size_t n) {
+    dig.add(p, n);
+    if (n && std::fwrite(p, 1, n, f) != n) throw Error{AFMM_BAD_ARG, "write failed"};
+  }
+  template <class T>
+  void put_vec(const std::vector<T>& v) {
+    put(v.data(), sizeof(T) * v.size());
+  }
+  void finish() {
+    const uint64_t d = dig.h;
+    if (std::fwrite(&d, 8, 1, f) != 1 || std::fclose(f) != 0) {
+      f = nullptr;
+      throw Error{AFMM_BAD_ARG, "write failed"};
+    }
+    f = nullptr;
+  }
+};
+
+struct SetupReader {
+  FILE* f = nullptr;
+  Fnv64 dig;
+  explicit SetupReader(const char* path) : f(std::fopen(path, "rb")) {
+    if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot open ") + path};
+  }
+  ~SetupReader() {
+    if (f) std::fclose(f);
+  }
+  void get(void* p, size_t n) {
+    if (n && std::fread(p, 1, n, f) != n) throw Error{AFMM_BAD_ARG, "setup file is truncated"};
+    dig.add(p, n);
+  }
+  template <class T>
+  T val() {
+    T x;
+    get(&x, sizeof(T));
+    return x;
+  }
+  template <class T>
+  void get_vec(std::vector<T>& v, int64_t n) {
+    if (n < 0 || n > (int64_t)1 << 40) throw Error{AFMM_BAD_ARG, "setup file has a bad size field"};
+    v.resize((size_t)n);
+    get(v.data(), sizeof(T) * (size_t)n);
+  }
+  void finish() {
+    uint64_t d = 0;
+    if (std::fread(&d, 8, 1, f) != 1) throw Error{AFMM_BAD_ARG, "setup file is truncated"};
+    if (d != dig.h) throw Error{AFMM_BAD_ARG, "setup file digest mismatch (corrupted file)"};
+    if (std::fgetc(f) != EOF) throw Error{AFMM_BAD_ARG, "setup file has trailing bytes"};
+  }
+};
+
+struct SetupLevel {
+  std::vector<int32_t> rank, skel_ids, cpiv_ids;
+  std::vector<double> l2p;
+};
+
+struct SetupImage {
+  int N = 0, M = 0, tol_pow = 0, L = 0, kernel_id = 0, m2l_mode = 0, q_mode = 0;
+  double a = 0, param = 0;
+  std::vector<double> pts;
+  std::vector<int64_t> perm;
+  std::vector<SetupLevel> lv;  // index j = level
+};
+
+void do_save(afmm_handle* h, const char* path) {
+  if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_save before afmm_assemble"};
+  const int N = h->N, L = h->L;
+  AFMM_CUDA(cudaStreamSynchronize(h->stream));
+  std::vector<double> pts(2 * (size_t)N);
+  std::vector<int64_t> perm(N);
+  AFMM_CUDA(cudaMemcpy(pts.data(), h->d_pts, sizeof(double) * pts.size(), cudaMemcpyDeviceToHost));
+  AFMM_CUDA(cudaMemcpy(perm.data(), h->d_perm, sizeof(int64_t) * N, cudaMemcpyDeviceToHost));
+  SetupWriter w(path);
+  w.put(kSetupMagic, 8);
+  const uint32_t ver[2] = {kSetupVersion, 0x01020304u};
+  w.put(ver, sizeof(ver));
+  const int32_t hdr[8] = {N, h->M, h->tol_pow, L, h->kernel_id, h->m2l_mode, h->m2l_q_mode, 0};
+  w.put(hdr, sizeof(hdr));
+  const double par[2] = {h->kp.a, h->kp.param};
+  w.put(par, sizeof(par));
+  w.put_vec(pts);
+  w.put_vec(perm);
+  for (int j = L; j >= 2; --j) {
+    const LevelDev& v = h->lv[j];
+    const int64_t tr = v.total_rank, ne = v.h_l2p_off[v.nbox];
+    const int64_t sz[3] = {v.nbox, tr, ne};
+    w.put(sz, sizeof(sz));
+    w.put_vec(v.h_rank);
+    std::vector<int32_t> ids(tr);
+    std::vector<double> l2p(ne);
+    if (tr) AFMM_CUDA(cudaMemcpy(ids.data(), v.skel_ids, sizeof(int32_t) * tr, cudaMemcpyDeviceToHost));
+    w.put_vec(ids);
+    if (tr) AFMM_CUDA(cudaMemcpy(ids.data(), v.cpiv_ids, sizeof(int32_t) * tr, cudaMemcpyDeviceToHost));
+    w.put_vec(ids);
+    if (ne) AFMM_CUDA(cudaMemcpy(l2p.data(), v.l2p, sizeof(double) * ne, cudaMemcpyDeviceToHost));
+    w.put_vec(l2p);
+  }
+  w.finish();
+}
+
+// Reads and checks a setup file on the host (no device work).
+SetupImage read_setup(const char* path) {
+  SetupReader r(path);
+  char magic[8];
+  r.get(magic, 8);
+  if (std::memcmp(magic, kSetupMagic, 8) != 0) throw Error{AFMM_BAD_ARG, "not an AFMM2D setup file"};
+  const uint32_t ver = r.val<uint32_t>(), bom = r.val<uint32_t>();
+  if (bom != 0x01020304u) throw Error{AFMM_BAD_ARG, "setup file written with another byte order"};
+  if (ver != kSetupVersion) throw Error{AFMM_BAD_ARG, "setup file version " + std::to_string(ver) + " not supported"};
+  SetupImage im;
+  int32_t hdr[8];
+  r.get(hdr, sizeof(hdr));
+  im.N = hdr[0];
+  im.M = hdr[1];
+  im.tol_pow = hdr[2];
+  im.L = hdr[3];
+  im.kernel_id = hdr[4];
+  im.m2l_mode = hdr[5];
+  im.q_mode = hdr[6];
+  double par[2];
+  r.get(par, sizeof(par));
+  im.a = par[0];
+  im.param = par[1];
+  if (im.N < 1 || im.M < 1 || im.L < 2 || im.L >= kMaxLevels || im.L != n_levels(im.N, im.M) || im.kernel_id < 0 ||
+      im.kernel_id > AFMM_KERNEL_GAUSSIAN || im.m2l_mode < 0 || im.m2l_mode > 2)
+    throw Error{AFMM_BAD_ARG, "setup file header is inconsistent"};
+  const int N = im.N, L = im.L;
+  r.get_vec(im.pts, 2 * (int64_t)N);
+  r.get_vec(im.perm, N);
+  std::vector<char> seen(N, 0);
+  for (int64_t p : im.perm) {
+    if (p < 0 || p >= N || seen[p]) throw Error{AFMM_BAD_ARG, "setup file permutation is not a permutation"};
+    seen[p] = 1;
+  }
+  for (double x : im.pts)
+    if (!std::isfinite(x)) throw Error{AFMM_BAD_ARG, "setup file holds a non-finite point"};
+  im.lv.resize(L + 1);
+  for (int j = L; j >= 2; --j) {
+    SetupLevel& lv = im.lv[j];
+    int64_t sz[3];
+    r.get(sz, sizeof(sz));
+    if (sz[0] != ((int64_t)1 << (2 * j))) throw Error{AFMM_BAD_ARG, "setup file level size mismatch"};
+    r.get_vec(lv.rank, sz[0]);
+    int64_t tr = 0;
+    for (int32_t x : lv.rank) {
+      if (x < 0) throw Error{AFMM_BAD_ARG, "setup file holds a negative rank"};
+      tr += x;
+    }
+    if (tr != sz[1]) throw Error{AFMM_BAD_ARG, "setup file rank sum mismatch"};
+    r.get_vec(lv.skel_ids, sz[1]);
+    r.get_vec(lv.cpiv_ids, sz[1]);
+    for (int32_t x : lv.skel_ids)
+      if (x < 0 || x >= N) throw Error{AFMM_BAD_ARG, "setup file skeleton id out of range"};
+    for (int32_t x : lv.cpiv_ids)
+      if (x < 0 || x >= N) throw Error{AFMM_BAD_ARG, "setup file pivot id out of range"};
+    r.get_vec(lv.l2p, sz[2]);
+  }
+  r.finish();
+  return im;
+}
+
+// The ACA results of every level from a setup image (in place of the level
+// loop of do_assemble); the L2P sizes are checked against the node counts.
+void load_levels(afmm_handle* h, SetupImage& im) {
+  cudaStream_t s = h->stream;
+  const int L = h->L;
+  for (int j = L; j >= 2; --j) {
+    LevelDev& v = h->lv[j];
+    SetupLevel& f = im.lv[j];
+    if (j < L) {
+      LevelDev& c = h->lv[j + 1];
+      v.h_node_off.assign(v.nbox + 1, 0);
+      for (long b = 0; b <= v.nbox; ++b) v.h_node_off[b] = c.h_skel_off[4 * b];
+      v.node_off = h->arena.alloc<int32_t>(v.nbox + 1);
+      AFMM_CUDA(cudaMemcpyAsync(v.node_off, v.h_node_off.data(), sizeof(int32_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+      v.node_ids = c.skel_ids;
+    }
+    v.h_rank = f.rank;
+    v.h_skel_off.assign(v.nbox + 1, 0);
+    v.h_l2p_off.assign(v.nbox + 1, 0);
+    int n1max = 0, rmax = 0;
+    for (long b = 0; b < v.nbox; ++b) {
+      const int n = v.h_node_off[b + 1] - v.h_node_off[b];
+      if (v.h_rank[b] > n) throw Error{AFMM_BAD_ARG, "setup file rank exceeds its box's node count"};
+      v.h_skel_off[b + 1] = v.h_skel_off[b] + v.h_rank[b];
+      v.h_l2p_off[b + 1] = v.h_l2p_off[b] + (int64_t)n * v.h_rank[b];
+      n1max = std::max(n1max, n);
+      rmax = std::max(rmax, v.h_rank[b]);
+    }
+    if (v.h_l2p_off[v.nbox] != (int64_t)f.l2p.size()) throw Error{AFMM_BAD_ARG, "setup file L2P size mismatch"};
+    v.n1max = n1max;
+    v.rmax = rmax;
+    v.total_rank = v.h_skel_off[v.nbox];
+    const long tr = v.total_rank;
+    v.rank = h->arena.alloc<int32_t>(v.nbox);
+    v.skel_off = h->arena.alloc<int32_t>(v.nbox + 1);
+    v.l2p_off = h->arena.alloc<int64_t>(v.nbox + 1);
+    v.skel_ids = h->arena.alloc<int32_t>(tr);
+    v.cpiv_ids = h->arena.alloc<int32_t>(tr);
+    v.skel_xy = h->arena.alloc<double2>(tr);
+    v.l2p = h->arena.alloc<double>(f.l2p.size());
+    AFMM_CUDA(cudaMemcpyAsync(v.rank, v.h_rank.data(), sizeof(int32_t) * v.nbox, cudaMemcpyHostToDevice, s));
+    AFMM_CUDA(cudaMemcpyAsync(v.skel_off, v.h_skel_off.data(), sizeof(int32_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+    AFMM_CUDA(cudaMemcpyAsync(v.l2p_off, v.h_l2p_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+    if (tr) {
+      AFMM_CUDA(cudaMemcpyAsync(v.skel_ids, f.skel_ids.data(), sizeof(int32_t) * tr, cudaMemcpyHostToDevice, s));
+      AFMM_CUDA(cudaMemcpyAsync(v.cpiv_ids, f.cpiv_ids.data(), sizeof(int32_t) * tr, cudaMemcpyHostToDevice, s));
+    }
+    if (!f.l2p.empty())
+      AFMM_CUDA(cudaMemcpyAsync(v.l2p, f.l2p.data(), sizeof(double) * f.l2p.size(), cudaMemcpyHostToDevice, s));
+    gather_points(h->d_pts, v.skel_ids, tr, v.skel_xy, s);
+    ++h->launches;
+    AFMM_CUDA(cudaStreamSynchronize(s));  // the host vectors of f may be freed after this
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -681,6 +968,51 @@ afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const dou
     double t0 = now_s();
     do_create(h, loc, loc_layout);
     h->t_create = now_s() - t0;
+  });
+  if (st != AFMM_OK) {
+    delete h;
+    return st;
+  }
+  *out = h;
+  return AFMM_OK;
+}
+
+afmm_status afmm_save(afmm_handle* h, const char* path) {
+  if (!h || !path) return AFMM_BAD_ARG;
+  return guard(h, [&] { do_save(h, path); });
+}
+
+afmm_status afmm_load(const char* path, afmm_handle** out) {
+  if (!out || !path) {
+    g_err = "path and out must not be NULL";
+    return AFMM_BAD_ARG;
+  }
+  *out = nullptr;
+  afmm_handle* h = nullptr;
+  afmm_status st = guard(nullptr, [&] {
+    const double t0 = now_s();
+    SetupImage im = read_setup(path);
+    check_device();
+    h = new afmm_handle();
+    h->N = im.N;
+    h->M = im.M;
+    h->tol_pow = im.tol_pow;
+    h->L = im.L;
+    h->kernel_id = im.kernel_id;
+    h->m2l_mode = im.m2l_mode;
+    h->m2l_q_mode = im.q_mode;
+    h->kp = make_kernel_params(im.kernel_id, im.a, im.param);
+    create_streams(h);
+    h->d_pts = h->arena.alloc<double2>(im.N);
+    h->d_perm = h->arena.alloc<int64_t>(im.N);
+    AFMM_CUDA(cudaMemcpyAsync(h->d_pts, im.pts.data(), sizeof(double) * im.pts.size(), cudaMemcpyHostToDevice, h->stream));
+    AFMM_CUDA(cudaMemcpyAsync(h->d_perm, im.perm.data(), sizeof(int64_t) * im.N, cudaMemcpyHostToDevice, h->stream));
+    create_layout(h);
+    const double t1 = now_s();
+    h->t_create = t1 - t0;
+    load_levels(h, im);
+    finish_assemble(h);
+    h->t_assemble = now_s() - t1;
   });
   if (st != AFMM_OK) {
     delete h;
@@ -850,6 +1182,17 @@ afmm_status afmm_get_permutation(afmm_handle* h, int64_t* perm) {
 afmm_status afmm_get_sorted_locations(afmm_handle* h, double* xy) {
   if (!h || !xy) return AFMM_BAD_ARG;
   return guard(h, [&] { AFMM_CUDA(cudaMemcpy(xy, h->d_pts, sizeof(double) * 2 * h->N, cudaMemcpyDeviceToHost)); });
+}
+
+afmm_status afmm_get_params(afmm_handle* h, int* i5, double* kparam) {
+  if (!h || !i5) return AFMM_BAD_ARG;
+  i5[0] = h->N;
+  i5[1] = h->M;
+  i5[2] = h->tol_pow;
+  i5[3] = h->L;
+  i5[4] = h->kernel_id;
+  if (kparam) *kparam = h->kp.param;
+  return AFMM_OK;
 }
 
 afmm_status afmm_get_nlevels(afmm_handle* h, int* nlevels) {

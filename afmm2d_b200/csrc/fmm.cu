@@ -82,6 +82,18 @@ __global__ void k_invert_perm(const int64_t* __restrict__ perm, int n, int32_t* 
   if (i < n) iperm[perm[i]] = i;
 }
 
+__global__ void k_gather_points(const double2* __restrict__ pts, const int32_t* __restrict__ ids, long n,
+                                double2* out) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) out[t] = pts[ids[t]];
+}
+
+void gather_points(const double2* pts, const int32_t* ids, long n, double2* out, cudaStream_t s) {
+  if (n == 0) return;
+  k_gather_points<<<(int)((n + 255) / 256), 256, 0, s>>>(pts, ids, n, out);
+  AFMM_LAUNCH_CHECK();
+}
+
 void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t s) {
   k_invert_perm<<<(n + 255) / 256, 256, 0, s>>>(perm, n, iperm);
   AFMM_LAUNCH_CHECK();

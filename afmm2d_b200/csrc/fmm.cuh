@@ -333,6 +333,8 @@ void build_lists(int j, long nbox, int32_t* nbr, int32_t* il, cudaStream_t s);
 void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s);
 // iperm[perm[i]] = i
 void invert_permutation(const int64_t* perm, int n, int32_t* iperm, cudaStream_t s);
+// out[t] = pts[ids[t]]
+void gather_points(const double2* pts, const int32_t* ids, long n, double2* out, cudaStream_t s);
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s);
 // 32-bit fixed-point copy of the stored FP64 blocks (m2l_q, m2l_dec).
 void m2l_compress(const LevelView& v, cudaStream_t s);

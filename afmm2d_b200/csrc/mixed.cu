@@ -6,8 +6,9 @@
 //  * M2L reads the 32-bit fixed-point copy of the blocks (half the bytes of
 //    FP64; entries within 2^-31 of their block's largest) or evaluates the
 //    entries on the fly from the skeleton coordinates (the blocks are plain
-//    kernel entries between skeleton points, src/AFMM2DTree.cpp:1080),
-//    whichever the first matvec measures faster.  The arithmetic stays FP64
+//    kernel entries between skeleton points, src/AFMM2DTree.cpp:1080); the
+//    fixed-point copy when kept, otherwise whichever of the FP64 blocks and
+//    the on-the-fly form the first matvec measures faster.  The arithmetic stays FP64
 //    because the outgoing charges are combinations with large, mixed-sign
 //    weights (ACA interpolation matrices) and FP32 entries lose ~10x to
 //    cancellation.
@@ -299,9 +300,13 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
       if (q32) m2l_apply_q32(p, s);
       else m2l_apply(p, s);
     };
+    // the fixed-point blocks (half the bytes of FP64) are always taken when
+    // kept, so every handle of a problem gives the same bits
+    if (q32) ms.m2l_form = 1;
     if (ms.m2l_form < 0 && stored) {
-      // one-time choice: both forms write the same yhat (to FP64 rounding);
-      // time each once on this problem and keep the faster
+      // one-time choice between the FP64 blocks and the entries on the fly:
+      // both write the same yhat (to FP64 rounding); time each once on this
+      // problem and keep the faster
       cudaEvent_t e[3];
       for (auto& x : e) AFMM_CUDA(cudaEventCreate(&x));
       AFMM_CUDA(cudaEventRecord(e[0], s));

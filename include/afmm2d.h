@@ -102,6 +102,20 @@ afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const dou
 /* ACA skeletonisation of every box (levels L..2), L2P, and M2L blocks. */
 afmm_status afmm_assemble(afmm_handle* h);
 
+/* Setup files.  No reference counterpart: the reference keeps the setup only
+ * in memory, per box (FMM2DBox members, include/AFMM2DBox.hpp:25-35, filled
+ * by src/AFMM2DTree.cpp:1009-1097), so every process repeats the ACA.
+ * afmm_save writes an assembled handle's KD permutation, sorted points and,
+ * per level, ranks, skeletons, pivot columns and L2P operators to a
+ * versioned binary file with a digest; afmm_load rebuilds an assembled
+ * handle from it on the current device (lists, row tables and M2L blocks are
+ * recomputed from the file's contents), skipping the KD sort and the ACA.
+ * The loaded handle's matvecs have the same bits as the saved handle's.  A
+ * file that is truncated, corrupted, of another version or inconsistent is
+ * rejected with AFMM_BAD_ARG before any device work. */
+afmm_status afmm_save(afmm_handle* h, const char* path);
+afmm_status afmm_load(const char* path, afmm_handle** out);
+
 /* M2L storage policy (afmm_m2l_storage), before afmm_assemble.  No reference
  * counterpart: the reference always stores the blocks in std::maps
  * (src/AFMM2DTree.cpp:1070-1097), which at 16M points and TOL 12 needs
@@ -140,6 +154,10 @@ afmm_status afmm_get_permutation(afmm_handle* h, int64_t* perm);
 /* Sorted locations, interleaved x,y (sorted_Locations). */
 afmm_status afmm_get_sorted_locations(afmm_handle* h, double* xy);
 afmm_status afmm_get_nlevels(afmm_handle* h, int* nlevels);
+/* The construction parameters: i5 = [N, MinParticlesInLeaf, TOL_POW,
+ * nLevels, kernel id]; kparam (may be NULL) = the kernel parameter
+ * (AFMM::N, MinParticlesInLeaf, TOL_POW, nLevels, include/AFMM2D.hpp:16-19). */
+afmm_status afmm_get_params(afmm_handle* h, int* i5, double* kparam);
 /* Leaf counts in KD (DFS) order and the DFS -> quadtree box-number map, 4^L each. */
 afmm_status afmm_get_leaves(afmm_handle* h, int32_t* counts, int32_t* box_numbers);
 /* Lists of one level (4^level boxes): nbr[8], inner[16], outer[24] per box, -1 = none. */
