@@ -18,8 +18,8 @@ import os
 
 import numpy as np
 
-__all__ = ["AFMM", "AFMMError", "AFMMSet", "KERNELS", "PRECISIONS", "device_alloc_count", "kernel_eval", "lib",
-           "nlevels"]
+__all__ = ["AFMM", "AFMMError", "AFMMSet", "KERNELS", "PRECISIONS", "device_alloc_count", "kernel_eval", "kernel_name",
+           "lib", "load_kernel_plugin", "nlevels"]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libafmm2d.so")
@@ -62,6 +62,8 @@ _SIGS = {
     "afmm_measure_fma_peaks": [_vp, _vp],
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_get_device_alloc_count": [_vp],
+    "afmm_register_kernel": [_i, _vp, ctypes.c_size_t, _i],
+    "afmm_kernel_name": [_i, _vp],
     "afmm_destroy": [_vp],
     "afmm_set_create": [_vp, _i, _vp],
     "afmm_set_matvec": [_vp, _vp, _vp, _i],
@@ -128,6 +130,26 @@ def measure_fma_peaks():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(lib().afmm_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+_plugins = []
+
+
+def load_kernel_plugin(path):
+    """Loads a user kernel library (built from a translation unit using
+    AFMM_REGISTER_KERNEL, see include/afmm2d_kernel.cuh); its kernel ids are
+    then accepted by AFMM(kernel=id).  Returns the ctypes library handle."""
+    lib()
+    h = ctypes.CDLL(os.path.abspath(path))
+    _plugins.append(h)
+    return h
+
+
+def kernel_name(kernel_id):
+    """Name of a built-in or registered kernel id."""
+    p = ctypes.c_char_p()
+    _check(lib().afmm_kernel_name(int(kernel_id), ctypes.byref(p)))
+    return p.value.decode()
 
 
 def device_alloc_count():

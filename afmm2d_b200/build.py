@@ -11,7 +11,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "libafmm2d.so")
-SOURCES = ["kd_sort.cu", "aca.cu", "fmm.cu", "mixed.cu", "batched.cu", "set.cu", "capi.cu"]
+SOURCES = ["kd_sort.cu", "aca.cu", "fmm.cu", "mixed.cu", "batched.cu", "set.cu", "capi.cu",
+           "kernels_one_over_r_scaled.cu", "kernels_log.cu", "kernels_one_over_r.cu", "kernels_gaussian.cu"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -60,6 +61,20 @@ def build(force=False, verbose=False, extra=()):
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True, cwd=CSRC)
     return OUT
+
+
+def build_kernel_plugin(source, out, verbose=False):
+    """Compiles a user kernel translation unit (one that includes
+    include/afmm2d_kernel.cuh and uses AFMM_REGISTER_KERNEL) into a shared
+    library linked against libafmm2d.so; loading it registers the kernel."""
+    include = os.path.abspath(os.path.join(HERE, "..", "include"))
+    rel = os.path.relpath(HERE, os.path.dirname(os.path.abspath(out)))
+    cmd = [nvcc(), *NVCC_FLAGS, "-I", include, os.path.abspath(source), "-o", os.path.abspath(out),
+           "-L", HERE, "-lafmm2d", "-Xlinker", "-rpath,$ORIGIN/" + rel]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True, cwd=os.path.dirname(os.path.abspath(source)))
+    return out
 
 
 if __name__ == "__main__":

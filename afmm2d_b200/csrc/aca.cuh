@@ -8,6 +8,64 @@
 
 namespace afmm {
 
+// Launch parameters of the ACA kernel (aca_k.cuh) and of the L2P solve,
+// shared by the level planner (aca.cu) and the kernel instantiations.
+constexpr int ACA_T = 256;
+constexpr int ACA_WARPS = ACA_T / 32;
+enum { AR_ROWS = 0, AR_COLS, AR_V, AR_U, AR_XDOT, AR_SMALL, AR_OK, AR_XARG, AR_N };
+
+struct AcaArgs {
+  int nbox;
+  const double2* pts;
+  const int32_t* node_off;
+  const int32_t* node_ids;
+  const int32_t* il;
+  double tol;
+  KernelParams kp;
+  int rcap;       // max rank stored per box
+  int n1max;
+  int chunk;      // columns per CTA
+  int vcap;       // ranks of V held in shared memory
+  int ucap;       // ranks of U held in shared memory
+  double* vspill; // [cluster][C][rcap - vcap][chunk]
+  double* uspill; // [cluster][C][rcap - ucap][n1max]
+  // Placement of the per-CTA arrays: byte offset into shared memory when the
+  // flag is set, else into this CTA's slot of `gscr` (gslot bytes per CTA).
+  unsigned char* gscr;
+  size_t gslot;
+  size_t off[8];
+  int in_smem[8];
+  int32_t* rank_out;
+  int32_t* rowpiv;  // nbox * rcap, local row index
+  int32_t* colpiv;  // nbox * rcap, sorted point id
+};
+
+// ------------------------------------------------------------------ L2P
+// One CTA per box: D = K(R, C) (r x r), A = D^T factorised with partial
+// pivoting; each thread solves A x = (K(row_i, C))^T for one row i of L2P.
+constexpr int L2P_T = 128;
+
+struct L2pArgs {
+  int nbox;
+  const double2* pts;
+  const int32_t* node_off;
+  const int32_t* node_ids;
+  const int32_t* rank;
+  const int32_t* rowpiv;
+  const int32_t* colpiv;
+  int rcap;
+  KernelParams kp;
+  const int32_t* skel_off;
+  const int64_t* l2p_off;
+  int32_t* skel_ids;
+  int32_t* cpiv_ids;
+  double2* skel_xy;
+  double* l2p;
+  int xs;            // rows of L2P solved at once (one per thread)
+  int rmax;          // largest rank of the level
+  double* gscratch;  // gridDim.x * rmax^2 when the factor lives in global memory
+};
+
 struct AcaLevelIn {
   long nbox;
   const double2* pts;       // sorted points

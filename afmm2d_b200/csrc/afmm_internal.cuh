@@ -64,7 +64,7 @@ __device__ __forceinline__ double r2_exact(double xi, double yi, double xj, doub
 // One over r, scaled (examples/testAFMM2D.cpp:9-20): R < a ? R/a : a/R.
 struct KOneOverRScaled {
   static constexpr int id = AFMM_KERNEL_ONE_OVER_R_SCALED;
-  __device__ __forceinline__ static double at_zero() { return 0.0; }
+  __device__ __forceinline__ static double at_zero(const KernelParams&) { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     double R = __dsqrt_rn(R2);
     return (R < p.a) ? __ddiv_rn(R, p.a) : __ddiv_rn(p.a, R);
@@ -84,7 +84,7 @@ struct KOneOverRScaled {
 // log(r) with the diagonal convention (examples/tutorial.cpp:22-35).
 struct KLog {
   static constexpr int id = AFMM_KERNEL_LOG;
-  __device__ __forceinline__ static double at_zero() { return 0.0; }
+  __device__ __forceinline__ static double at_zero(const KernelParams&) { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     if (R2 < 1e-10) return 0.0;
     const double l = log_cr(R2);
@@ -118,7 +118,7 @@ struct KLog {
 // 1/r with 0 at r = 0.
 struct KOneOverR {
   static constexpr int id = AFMM_KERNEL_ONE_OVER_R;
-  __device__ __forceinline__ static double at_zero() { return 0.0; }
+  __device__ __forceinline__ static double at_zero(const KernelParams&) { return 0.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams&) {
     if (R2 == 0.0) return 0.0;
     return __ddiv_rn(1.0, __dsqrt_rn(R2));
@@ -146,7 +146,7 @@ struct KOneOverR {
 // Gaussian exp(-R2/param) (1 on the diagonal).
 struct KGaussian {
   static constexpr int id = AFMM_KERNEL_GAUSSIAN;
-  __device__ __forceinline__ static double at_zero() { return 1.0; }
+  __device__ __forceinline__ static double at_zero(const KernelParams&) { return 1.0; }
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     return exp_cr(-__ddiv_rn(R2, p.param));
   }
@@ -158,18 +158,6 @@ struct KGaussian {
     return __expf(-__fdividef(R2, param));
   }
 };
-
-// Calls F::template run<K>(args...) for the kernel id.
-template <template <class> class F, class... Args>
-void dispatch_kernel(int id, Args&&... args) {
-  switch (id) {
-    case AFMM_KERNEL_ONE_OVER_R_SCALED: F<KOneOverRScaled>::run(args...); break;
-    case AFMM_KERNEL_LOG: F<KLog>::run(args...); break;
-    case AFMM_KERNEL_ONE_OVER_R: F<KOneOverR>::run(args...); break;
-    case AFMM_KERNEL_GAUSSIAN: F<KGaussian>::run(args...); break;
-    default: throw Error{AFMM_BAD_ARG, "unknown kernel id"};
-  }
-}
 
 // ------------------------------------------------------------- allocation
 // Every device allocation of the library goes through DevArena::alloc, which

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -13,10 +14,39 @@
 #include "afmm_internal.cuh"
 #include "fmm.cuh"
 #include "kd_sort.cuh"
+#include "kernel_table.cuh"
 #include "mixed.cuh"
 #include "set.cuh"
 
 using namespace afmm;
+
+// ------------------------------------------------------- kernel registry
+namespace {
+std::mutex g_kernel_mu;
+const KernelTable* g_user_kernels[AFMM_KERNEL_USER_COUNT] = {};
+}  // namespace
+
+bool afmm::kernel_known(int id) {
+  if (id >= 0 && id <= AFMM_KERNEL_GAUSSIAN) return true;
+  if (id < AFMM_KERNEL_USER_FIRST || id >= AFMM_KERNEL_USER_FIRST + AFMM_KERNEL_USER_COUNT) return false;
+  std::lock_guard<std::mutex> lock(g_kernel_mu);
+  return g_user_kernels[id - AFMM_KERNEL_USER_FIRST] != nullptr;
+}
+
+const KernelTable& afmm::kernel_table(int id) {
+  switch (id) {
+    case AFMM_KERNEL_ONE_OVER_R_SCALED: return builtin_table_one_over_r_scaled();
+    case AFMM_KERNEL_LOG: return builtin_table_log();
+    case AFMM_KERNEL_ONE_OVER_R: return builtin_table_one_over_r();
+    case AFMM_KERNEL_GAUSSIAN: return builtin_table_gaussian();
+    default: break;
+  }
+  if (id >= AFMM_KERNEL_USER_FIRST && id < AFMM_KERNEL_USER_FIRST + AFMM_KERNEL_USER_COUNT) {
+    std::lock_guard<std::mutex> lock(g_kernel_mu);
+    if (const KernelTable* t = g_user_kernels[id - AFMM_KERNEL_USER_FIRST]) return *t;
+  }
+  throw Error{AFMM_BAD_ARG, "unknown kernel id " + std::to_string(id)};
+}
 
 std::atomic<int64_t>& afmm::device_alloc_counter() {
   static std::atomic<int64_t> n{0};
@@ -138,45 +168,6 @@ uint64_t splitmix(uint64_t& s) {
   return z ^ (z >> 31);
 }
 
-// Direct FP64 potentials at selected sorted points, Neumaier-compensated.
-template <class K>
-__global__ void k_dense_rows(const double2* __restrict__ pts, const double* __restrict__ qs, int N,
-                             const int32_t* __restrict__ rows, KernelParams kp, double* out) {
-  const int t = blockIdx.x;
-  const double2 xi = pts[rows[t]];
-  double s = 0.0, c = 0.0;
-  for (int j = threadIdx.x; j < N; j += blockDim.x) {
-    double v = K::eval(r2_exact(xi.x, xi.y, pts[j].x, pts[j].y), kp) * qs[j];
-    double tt = s + v;
-    c += (fabs(s) >= fabs(v)) ? ((s - tt) + v) : ((v - tt) + s);
-    s = tt;
-  }
-  __shared__ double ss[256], sc[256];
-  ss[threadIdx.x] = s;
-  sc[threadIdx.x] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double S = 0.0, Cc = 0.0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      double v = ss[i];
-      double tt = S + v;
-      Cc += (fabs(S) >= fabs(v)) ? ((S - tt) + v) : ((v - tt) + S);
-      S = tt;
-      Cc += sc[i];
-    }
-    out[t] = S + Cc;
-  }
-}
-
-template <class K>
-struct DenseRun {
-  static void run(const double2* pts, const double* qs, int N, const int32_t* rows, int nrows, KernelParams kp,
-                  double* out, cudaStream_t s) {
-    k_dense_rows<K><<<nrows, 256, 0, s>>>(pts, qs, N, rows, kp, out);
-    AFMM_LAUNCH_CHECK();
-  }
-};
-
 // FMA throughput: 8 independent chains per thread, `iters` rounds.
 template <class T>
 __global__ void k_fma_peak(T seed, int iters, T* out) {
@@ -217,31 +208,6 @@ double fma_peak_tflops() {
   AFMM_LAUNCH_CHECK();
   return 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3) / 1e12;
 }
-
-template <class K>
-__global__ void k_kernel_pairs(const double2* __restrict__ a, const double2* __restrict__ b, long n, KernelParams kp,
-                               int mode, double* out) {
-  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  double2 p = a[t], q = b[t];
-  if (mode == 0) {
-    out[t] = K::eval_exact(r2_exact(p.x, p.y, q.x, q.y), kp);
-  } else if (mode == 1) {
-    double dx = p.x - q.x, dy = p.y - q.y;
-    out[t] = K::eval(dx * dx + dy * dy, kp);
-  } else {
-    float dx = (float)(p.x - q.x), dy = (float)(p.y - q.y);
-    out[t] = (double)K::eval32(fmaf(dx, dx, dy * dy), (float)kp.a, (float)kp.param);
-  }
-}
-
-template <class K>
-struct PairsRun {
-  static void run(const double2* a, const double2* b, long n, KernelParams kp, int mode, double* out) {
-    k_kernel_pairs<K><<<(int)((n + 255) / 256), 256>>>(a, b, n, kp, mode, out);
-    AFMM_LAUNCH_CHECK();
-  }
-};
 
 void build_plan(afmm_handle* h) {
   MatvecPlan& p = h->plan;
@@ -839,9 +805,11 @@ SetupImage read_setup(const char* path) {
   r.get(par, sizeof(par));
   im.a = par[0];
   im.param = par[1];
-  if (im.N < 1 || im.M < 1 || im.L < 2 || im.L >= kMaxLevels || im.L != n_levels(im.N, im.M) || im.kernel_id < 0 ||
-      im.kernel_id > AFMM_KERNEL_GAUSSIAN || im.m2l_mode < 0 || im.m2l_mode > 2)
+  if (im.N < 1 || im.M < 1 || im.L < 2 || im.L >= kMaxLevels || im.L != n_levels(im.N, im.M) || im.m2l_mode < 0 ||
+      im.m2l_mode > 2)
     throw Error{AFMM_BAD_ARG, "setup file header is inconsistent"};
+  if (!kernel_known(im.kernel_id))
+    throw Error{AFMM_BAD_ARG, "setup file uses kernel id " + std::to_string(im.kernel_id) + ", which is not registered"};
   const int N = im.N, L = im.L;
   r.get_vec(im.pts, 2 * (int64_t)N);
   r.get_vec(im.perm, N);
@@ -948,7 +916,7 @@ afmm_status afmm_create(int N, int min_particles_in_leaf, int tol_pow, const dou
     if (N < 1 || min_particles_in_leaf < 1) throw Error{AFMM_BAD_ARG, "N and MinParticlesInLeaf must be >= 1"};
     if (!loc) throw Error{AFMM_BAD_ARG, "loc is NULL"};
     if (loc_layout != AFMM_LOC_COLMAJOR && loc_layout != AFMM_LOC_INTERLEAVED) throw Error{AFMM_BAD_ARG, "bad loc_layout"};
-    if (kernel_id < 0 || kernel_id > AFMM_KERNEL_GAUSSIAN) throw Error{AFMM_BAD_ARG, "unknown kernel_id"};
+    if (!kernel_known(kernel_id)) throw Error{AFMM_BAD_ARG, "unknown kernel_id " + std::to_string(kernel_id)};
     int L = n_levels(N, min_particles_in_leaf);
     if (L < 2)
       throw Error{AFMM_BAD_ARG, "N/MinParticlesInLeaf gives nLevels = " + std::to_string(L) + " < 2"};
@@ -1158,7 +1126,7 @@ afmm_status afmm_eval_error(afmm_handle* h, int nsample, uint64_t seed, double* 
     double* d_out = tmp.alloc<double>(rows.size());
     cudaStream_t s = h->stream;
     AFMM_CUDA(cudaMemcpyAsync(d_rows, rows.data(), sizeof(int32_t) * rows.size(), cudaMemcpyHostToDevice, s));
-    dispatch_kernel<DenseRun>(h->kp.id, h->d_pts, h->d_qs, h->N, d_rows, (int)rows.size(), h->kp, d_out, s);
+    kernel_table(h->kp.id).dense_rows(h->d_pts, h->d_qs, h->N, d_rows, (int)rows.size(), h->kp, d_out, s);
     ++h->launches;
     std::vector<double> dense(rows.size()), ys(h->N);
     AFMM_CUDA(cudaMemcpyAsync(dense.data(), d_out, sizeof(double) * rows.size(), cudaMemcpyDeviceToHost, s));
@@ -1354,8 +1322,7 @@ afmm_status afmm_get_stream(afmm_handle* h, void** stream) {
 
 afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, const double* xy1, const double* xy2,
                              double* out, int mode) {
-  if (!xy1 || !xy2 || !out || n < 0 || mode < 0 || mode > 2 || kernel_id < 0 || kernel_id > AFMM_KERNEL_GAUSSIAN)
-    return AFMM_BAD_ARG;
+  if (!xy1 || !xy2 || !out || n < 0 || mode < 0 || mode > 2 || !kernel_known(kernel_id)) return AFMM_BAD_ARG;
   if (n == 0) return AFMM_OK;
   return guard(nullptr, [&] {
     check_device();
@@ -1365,7 +1332,7 @@ afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, c
     double* dout = tmp.alloc<double>(n);
     AFMM_CUDA(cudaMemcpy(da, xy1, sizeof(double2) * n, cudaMemcpyHostToDevice));
     AFMM_CUDA(cudaMemcpy(db, xy2, sizeof(double2) * n, cudaMemcpyHostToDevice));
-    dispatch_kernel<PairsRun>(kernel_id, da, db, (long)n, make_kernel_params(kernel_id, a, param), mode, dout);
+    kernel_table(kernel_id).kernel_pairs(da, db, (long)n, make_kernel_params(kernel_id, a, param), mode, dout);
     AFMM_CUDA(cudaMemcpy(out, dout, sizeof(double) * n, cudaMemcpyDeviceToHost));
   });
 }
@@ -1391,6 +1358,32 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
     check_device();
     kd_sort_noalloc(xy, N, L, perm, xy_sorted, (cudaStream_t)stream);
   });
+}
+
+afmm_status afmm_register_kernel(int kernel_id, const void* table, size_t table_bytes, int abi_version) {
+  if (kernel_id < AFMM_KERNEL_USER_FIRST || kernel_id >= AFMM_KERNEL_USER_FIRST + AFMM_KERNEL_USER_COUNT) {
+    g_err = "user kernel ids are " + std::to_string(AFMM_KERNEL_USER_FIRST) + " .. " +
+            std::to_string(AFMM_KERNEL_USER_FIRST + AFMM_KERNEL_USER_COUNT - 1);
+    return AFMM_BAD_ARG;
+  }
+  if (!table || table_bytes != sizeof(KernelTable) || abi_version != kKernelTableAbi ||
+      ((const KernelTable*)table)->abi != kKernelTableAbi) {
+    g_err = "kernel table built against other library headers (size or ABI version differs)";
+    return AFMM_BAD_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_kernel_mu);
+  const KernelTable*& slot = g_user_kernels[kernel_id - AFMM_KERNEL_USER_FIRST];
+  if (slot && slot != table) {
+    g_err = "kernel id " + std::to_string(kernel_id) + " is already registered";
+    return AFMM_BAD_ARG;
+  }
+  slot = (const KernelTable*)table;
+  return AFMM_OK;
+}
+
+afmm_status afmm_kernel_name(int kernel_id, const char** name) {
+  if (!name) return AFMM_BAD_ARG;
+  return guard(nullptr, [&] { *name = kernel_table(kernel_id).name; });
 }
 
 afmm_status afmm_get_device_alloc_count(int64_t* n) {

@@ -4,6 +4,7 @@
 
 #include "afmm_internal.cuh"
 #include "fmm.cuh"
+#include "kernel_table.cuh"
 
 namespace afmm {
 
@@ -105,39 +106,9 @@ void fill_box_map(const int32_t* off, long nbox, int32_t* map, cudaStream_t s) {
 }
 
 // ------------------------------------------------------------ M2L blocks
-// M2L[b][c] = K(R_b, R_c) for every valid inner/outer slot of b, in slot
-// order (src/AFMM2DTree.cpp:1070-1097), stored column-major r_b x r_c.
-template <class K>
-__global__ void k_m2l_assemble(LevelView v, KernelParams kp) {
-  const long b = blockIdx.x;
-  const int r = v.rank[b];
-  if (r == 0) return;
-  double* out = v.m2l + v.m2l_off[b];
-  const double2* xb = v.skel_xy + v.skel_off[b];
-  long off = 0;
-  for (int s = 0; s < 40; ++s) {
-    int c = v.il[b * 40 + s];
-    if (c < 0) continue;
-    const int rc = v.rank[c];
-    const double2* xc = v.skel_xy + v.skel_off[c];
-    for (int e = threadIdx.x; e < r * rc; e += blockDim.x) {
-      int cc = e / r, i = e - cc * r;
-      out[off + e] = K::eval_exact(r2_exact(xb[i].x, xb[i].y, xc[cc].x, xc[cc].y), kp);
-    }
-    off += (long)r * rc;
-  }
-}
-
-template <class K>
-struct M2lAssembleRun {
-  static void run(const LevelView& v, const KernelParams& kp, cudaStream_t s) {
-    k_m2l_assemble<K><<<(int)v.nbox, 128, 0, s>>>(v, kp);
-    AFMM_LAUNCH_CHECK();
-  }
-};
-
+// (k_m2l_assemble, fmm_k.cuh)
 void m2l_assemble(const LevelView& v, const KernelParams& kp, cudaStream_t s) {
-  dispatch_kernel<M2lAssembleRun>(kp.id, v, kp, s);
+  kernel_table(kp.id).m2l_assemble(v, kp, s);
 }
 
 // 32-bit fixed-point copy of the FP64 blocks: per block a power-of-two scale
@@ -343,25 +314,6 @@ __global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __re
   if (g < v.nnodes) l2l_row(v, child_yhat, ys, leaf, g);
 }
 
-// Near field (src/AFMM2DTree.cpp:1199-1213): one CTA per leaf.
-template <class K>
-__global__ void k_p2p64(NearView nv, KernelParams kp, const double* __restrict__ qs, double* __restrict__ ys, int NT,
-                        int G) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  p2p64_leaf<K>(nv, kp, qs, ys, NT, G, blockIdx.x, smem);
-}
-
-template <class K>
-struct P2p64Run {
-  static void run(const NearView& nv, const KernelParams& kp, const double* qs, double* ys, cudaStream_t s) {
-    P2pShape sh = p2p_shape(nv.nmax);
-    size_t smem = (size_t)9 * nv.nmax * (sizeof(double2) + sizeof(double)) + sizeof(double) * sh.threads;
-    allow_smem(k_p2p64<K>, smem);
-    k_p2p64<K><<<(int)nv.nleaf, sh.threads, smem, s>>>(nv, kp, qs, ys, sh.nt, sh.g);
-    AFMM_LAUNCH_CHECK();
-  }
-};
-
 void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches) {
   for (int j = p.L; j >= 2; --j) {
     const LevelView& v = p.lv[j];
@@ -417,7 +369,7 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   if (tm) tm->mark(s, "l2l");
   sweep_l2l(p, p.ys, s, launches);
   if (tm) tm->mark(s, "p2p");
-  dispatch_kernel<P2p64Run>(p.kp.id, p.near, p.kp, p.qs, p.ys, s);
+  kernel_table(p.kp.id).p2p64(p.near, p.kp, p.qs, p.ys, s);
   ++*launches;
   if (tm) tm->mark(s, "scatter");
   k_scatter<<<gb, 256, 0, s>>>(p.ys, p.perm, N, y);

@@ -4,22 +4,12 @@
 // every problem's result is bit-identical to its own FP64 matvec.
 #include <algorithm>
 
+#include "kernel_table.cuh"
 #include "set.cuh"
 
 namespace afmm {
 
 namespace {
-
-// Segment of flat item g: the largest s with first[s] <= g.
-__device__ __forceinline__ int seg_of(const SetSegs& sg, long g) {
-  int lo = 0, hi = sg.n - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (sg.first[mid] <= g) lo = mid;
-    else hi = mid - 1;
-  }
-  return lo;
-}
 
 // qs_p[i] = q[off[p] + perm_p[i]]  (src/AFMM2D.cpp:49-51 per problem)
 __global__ void k_set_gather(SetDev d, SetSegs sg, const double* __restrict__ q) {
@@ -72,37 +62,6 @@ __global__ void k_set_l2l(SetDev d, SetSegs sg) {
   double* child = leaf ? nullptr : d.lv[(long)p * kMaxLevels + j + 1].yhat;
   l2l_row(v, child, d.ys[p], leaf ? 1 : 0, g - sg.first[s]);
 }
-
-// Near field: one CTA per leaf of every problem, each problem with its own
-// (NT, G) shape so the group sums add in the same order as its own launch.
-template <class K>
-__global__ void k_set_p2p64(SetDev d, SetSegs sg) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const long g = blockIdx.x;
-  const int s = seg_of(sg, g);
-  const int p = sg.prob[s];
-  const int2 sh = d.p2p[p];
-  p2p64_leaf<K>(d.nv[p], d.kp[p], d.qs[p], d.ys[p], sh.x, sh.y, g - sg.first[s], smem);
-}
-
-template <class K>
-struct SetP2pRun {
-  static void prepare(size_t smem) { allow_smem(k_set_p2p64<K>, smem); }
-  static void run(const SetPlan& sp, cudaStream_t s) {
-    k_set_p2p64<K><<<(int)sp.p2p.total, sp.p2p_threads, sp.p2p_smem, s>>>(sp.dev, sp.p2p);
-    AFMM_LAUNCH_CHECK();
-  }
-};
-
-template <class K>
-struct SetP2pPrepare {
-  static void run(size_t smem) { SetP2pRun<K>::prepare(smem); }
-};
-
-template <class K>
-struct SetP2pLaunch {
-  static void run(const SetPlan& sp, cudaStream_t s) { SetP2pRun<K>::run(sp, s); }
-};
 
 struct SegBuilder {
   std::vector<int64_t> first{0};
@@ -177,7 +136,7 @@ void record(SetPlan& sp, cudaStream_t s) {
     ++n;
   }
   mark("p2p");
-  dispatch_kernel<SetP2pLaunch>(sp.kernel_id, sp, s);
+  kernel_table(sp.kernel_id).set_p2p_run(sp, s);
   ++n;
   mark("scatter");
   k_set_scatter<<<nb(sp.gather.total, 256), 256, 0, s>>>(sp.dev, sp.gather, sp.y);
@@ -257,7 +216,7 @@ void set_build(SetPlan& sp, const std::vector<SetProblem>& probs, DevArena& aren
   sp.y = arena.alloc<double>(off[np]);
   AFMM_CUDA(cudaStreamSynchronize(s));
   // kernel attributes are set before capture; then the graph is recorded once
-  dispatch_kernel<SetP2pPrepare>(sp.kernel_id, sp.p2p_smem);
+  kernel_table(sp.kernel_id).set_p2p_prepare(sp.p2p_smem);
   AFMM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
   try {
     record(sp, s);

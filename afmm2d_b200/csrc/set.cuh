@@ -31,6 +31,17 @@ struct SetSegs {
   long total = 0;
 };
 
+// Segment of flat item g: the largest s with first[s] <= g.
+__device__ __forceinline__ int seg_of(const SetSegs& sg, long g) {
+  int lo = 0, hi = sg.n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sg.first[mid] <= g) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Host description of one problem of the set.
 struct SetProblem {
   const MatvecPlan* plan;

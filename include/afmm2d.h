@@ -61,7 +61,11 @@ typedef enum {
   AFMM_NO_DEVICE = 7      /* no CUDA device of compute capability 10.x */
 } afmm_status;
 
-/* Built-in kernels (userkernel::getMatrixEntry variants). */
+/* Kernels (userkernel::getMatrixEntry, include/kernel.hpp:58).  Ids 0..3 are
+ * built in; ids AFMM_KERNEL_USER_FIRST .. + AFMM_KERNEL_USER_COUNT - 1 are
+ * user kernels registered with afmm_register_kernel. */
+#define AFMM_KERNEL_USER_FIRST 16
+#define AFMM_KERNEL_USER_COUNT 64
 typedef enum {
   AFMM_KERNEL_ONE_OVER_R_SCALED = 0, /* R<a ? R/a : a/R  (examples/testAFMM2D.cpp:9-20) */
   AFMM_KERNEL_LOG = 1,               /* log r with diagonal convention (examples/tutorial.cpp:22-35) */
@@ -234,6 +238,21 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
  * process so far, over all handles and sets.  No reference counterpart: a
  * diagnostic that lets a caller check that a call allocated nothing. */
 afmm_status afmm_get_device_alloc_count(int64_t* n);
+
+/* Registers a user kernel: the reference's plug-in point, a user-defined
+ * userkernel::getMatrixEntry (include/kernel.hpp:23,58; defined out of line
+ * in examples/testAFMM2D.cpp:9-20), becomes a kernel functor compiled in the
+ * user's own CUDA translation unit.  That unit includes afmm2d_kernel.cuh and
+ * writes AFMM_REGISTER_KERNEL(id, Functor), which instantiates every stage
+ * that evaluates the kernel (ACA, L2P, M2L blocks, near fields, on-the-fly
+ * M2L, sets, diagnostics) for the functor and calls this function with the
+ * table of their launchers when the unit's library is loaded.  kernel_id in
+ * AFMM_KERNEL_USER_FIRST ..; table_bytes and abi_version must match this
+ * library's headers.  Afterwards the id is accepted by afmm_create,
+ * afmm_kernel_eval and afmm_load like a built-in id. */
+afmm_status afmm_register_kernel(int kernel_id, const void* table, size_t table_bytes, int abi_version);
+/* Name of a built-in or registered kernel (AFMM_BAD_ARG for unknown ids). */
+afmm_status afmm_kernel_name(int kernel_id, const char** name);
 
 afmm_status afmm_destroy(afmm_handle* h);
 

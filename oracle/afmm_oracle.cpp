@@ -49,6 +49,9 @@ struct Kern {
       case 2:  // 1/r, 0 at r = 0
         if (R2 == 0.0) return 0.0;
         return 1.0 / std::sqrt(R2);
+      case 16:  // inverse multiquadric 1/sqrt(R2 + param): the user kernel of the
+                // plug-in test (tests/plugin/imq_kernel.cu), registered out of tree
+        return 1.0 / std::sqrt(R2 + param);
       default:  // Gaussian exp(-R2/param)
         return crm::exp_cr(-R2 / param);
     }

@@ -13,7 +13,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_SO = os.path.join(ROOT, "oracle", "libafmm_oracle.so")
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libafmm2d_ref.so")
-KERNEL_IDS = {"one_over_r_scaled": 0, "log": 1, "one_over_r": 2, "gaussian": 3}
+KERNEL_IDS = {"one_over_r_scaled": 0, "log": 1, "one_over_r": 2, "gaussian": 3, "imq": 16}
 
 vp, I, D, L = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_long
 
