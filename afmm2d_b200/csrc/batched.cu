@@ -243,7 +243,7 @@ __device__ __forceinline__ void store_tiles(const double (&c)[NT][RC / 8][2], do
 // L2 ahead of the loads.
 template <int RC, int NT, bool Q32>
 __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const double* __restrict__ qh,
-                                                 double* __restrict__ yb, int b, int r0, int lane) {
+                                                 double* __restrict__ yb, int b, int r0, int lane, uint32_t ahead) {
   const int r = v.rank[b];
   const int i0 = r0 - v.skel_off[b];
   const int nrow = min(8 * NT, r - i0);
@@ -259,7 +259,7 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
   long pos = v.m2l_off[b];  // first entry of the current slot's block
   const long stop = v.m2l_off[b + 1];
   L2Stream pf(Q32 ? (const void*)(v.m2l_q + pos) : (const void*)(v.m2l + pos),
-              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop));
+              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop), ahead);
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   for (int s = 0; s < 40; ++s) {
@@ -378,7 +378,7 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
   const long g = gw - ls.cgrp0[j];
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
-#define AFMM_M2L(NT) m2l_stored_chunk<RC, NT, Q32>(v, qhat_lv[j], yhat_lv[j], b, r0, lane)
+#define AFMM_M2L(NT) m2l_stored_chunk<RC, NT, Q32>(v, qhat_lv[ls.src[j]], yhat_lv[ls.src[j]], b, r0, lane, ls.pf_ahead)
   AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2L)
 #undef AFMM_M2L
 }
@@ -390,25 +390,32 @@ struct Pass {
   // M2L of every level: the stored blocks (fixed point in mixed precision,
   // FP64 otherwise; kernel-independent), or the entries on the fly (the
   // kernel's table)
-  static void m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, cudaStream_t s) {
+  // (the levels of the tuning mask, in mixed precision, on the fly as well)
+  static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, cudaStream_t s) {
     constexpr int RM = RC >= 8 ? RC : 8;
-    const LevelSet& ls = p.levels;
-    if (ls.row0[ls.nlev] == 0) return;  // every box of ACA rank 0: no far field
-    if (RC >= 8 && !fp64 && ls.lv[0].m2l_q != nullptr) {
-      // mixed precision: the 32-bit fixed-point blocks (half the bytes)
-      const long warps = ls.cgrp0[ls.nlev];
-      k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
-      AFMM_LAUNCH_CHECK();
-    } else if (RC >= 8 && ls.lv[0].m2l != nullptr) {
+    if (p.levels.row0[p.levels.nlev] == 0) return 0;  // every box of ACA rank 0: no far field
+    const bool q32 = RC >= 8 && !fp64 && p.levels.lv[0].m2l_q != nullptr;
+    const bool stored = RC >= 8 && (q32 || p.levels.lv[0].m2l != nullptr);
+    const uint32_t otf = !stored ? 0xffffffffu : (fp64 ? 0u : p.tune.otf_batched);
+    LevelSet st = level_subset(p.levels, otf, false);
+    const LevelSet fly = level_subset(p.levels, otf, true);
+    st.pf_ahead = p.tune.pf_batched;
+    int n = 0;
+    if (st.nlev > 0 && st.cgrp0[st.nlev] > 0) {
       // stored blocks: one HBM read of the blocks serves all RC columns
-      const long warps = ls.cgrp0[ls.nlev];
-      k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, qh, yh);
+      // (mixed precision: the 32-bit fixed-point copy, half the bytes)
+      const long warps = st.cgrp0[st.nlev];
+      if (q32) k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+      else k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       AFMM_LAUNCH_CHECK();
-    } else if (RC >= 8) {
-      kernel_table(p.kp.id).m2l_otf_mma[RC == 16](ls, p.kp, qh, yh, s);
-    } else {
-      kernel_table(p.kp.id).m2l_otf_b4(ls, p.kp, qh, yh, s);
+      ++n;
     }
+    if (fly.nlev > 0 && fly.row0[fly.nlev] > 0) {
+      if (RC >= 8) kernel_table(p.kp.id).m2l_otf_mma[RC == 16](fly, p.kp, qh, yh, s);
+      else kernel_table(p.kp.id).m2l_otf_b4(fly, p.kp, qh, yh, s);
+      ++n;
+    }
+    return n;
   }
 
   static void run(const MatvecPlan& p, BatchState& bs, const NearView& nv, const double* q, int64_t ldq, double* y,
@@ -432,8 +439,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "m2l");
-    m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
-    ++*launches;
+    *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];

@@ -20,7 +20,7 @@ __global__ void k_m2l_b(LevelSet ls, KernelParams kp, const double* const* __res
   int j = 0;
   while (j + 1 < ls.nlev && g >= ls.row0[j + 1]) ++j;
   const LevelView& v = ls.lv[j];
-  const double* qh = qhat_lv[j];
+  const double* qh = qhat_lv[ls.src[j]];
   const long row = g - ls.row0[j];
   const int b = v.skel_box[row];
   const double2 xi = v.skel_xy[row];
@@ -43,7 +43,7 @@ __global__ void k_m2l_b(LevelSet ls, KernelParams kp, const double* const* __res
       for (int k = 0; k < RC; ++k) acc[k] = fma(kv, q[k], acc[k]);
     }
   }
-  store_vec<RC>(yhat_lv[j] + row * RC, acc);
+  store_vec<RC>(yhat_lv[ls.src[j]] + row * RC, acc);
 }
 
 template <class K>
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
   int j = 0;
   while (j + 1 < ls.nlev && gw >= ls.grp0[j + 1]) ++j;
   const LevelView& v = ls.lv[j];
-  const double* qh = qhat_lv[j];
+  const double* qh = qhat_lv[ls.src[j]];
   const long g = gw - ls.grp0[j];
   const int b = v.grp_box[g];
   const int r0 = v.grp_row[g];
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(128) k_m2l_mma(LevelSet ls, KernelParams kp, c
     }
   }
   if (vrow) {
-    double* out = yhat_lv[j] + (long)(r0 + trow) * RC;
+    double* out = yhat_lv[ls.src[j]] + (long)(r0 + trow) * RC;
 #pragma unroll
     for (int t = 0; t < RC / 8; ++t) {
       out[t * 8 + 2 * tsrc] = c[t][0];

@@ -265,7 +265,7 @@ __global__ void __launch_bounds__(128) k_m2l_apply_w(LevelSet ls) {
   const long stop = v.m2l_off[b + 1];
   long pos = base;  // first entry of the current slot's block
   L2Stream pf(Q32 ? (const void*)(v.m2l_q + base) : (const void*)(v.m2l + base),
-              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop));
+              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop), ls.pf_ahead);
   double acc = 0.0;
   for (int s = 0; s < 40; ++s) {
     const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
@@ -338,19 +338,25 @@ void m2l_apply(const MatvecPlan& p, cudaStream_t s) {
   const long rows = p.levels.row0[p.levels.nlev];
   if (rows == 0) return;
   if (p.levels.lv[0].m2l == nullptr) {  // blocks not stored: entries on the fly
-    m2l_apply_otf(p, s);
+    m2l_apply_otf(p, p.levels, s);
     return;
   }
-  const long warps = p.levels.wgrp0[p.levels.nlev];
-  k_m2l_apply_w<false><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(p.levels);
+  LevelSet ls = p.levels;
+  ls.pf_ahead = p.tune.pf_fp64;
+  const long warps = ls.wgrp0[ls.nlev];
+  k_m2l_apply_w<false><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(ls);
   AFMM_LAUNCH_CHECK();
 }
 
-void m2l_apply_q32(const MatvecPlan& p, cudaStream_t s) {
-  const long warps = p.levels.wgrp0[p.levels.nlev];
+void m2l_apply_stored(const MatvecPlan& p, const LevelSet& levels, bool q32, cudaStream_t s) {
+  LevelSet ls = levels;
+  ls.pf_ahead = p.tune.pf_fp64;
+  const long warps = ls.wgrp0[ls.nlev];
   if (warps == 0) return;
-  if (p.levels.lv[0].m2l_q == nullptr) throw Error{AFMM_BAD_ARG, "no fixed-point M2L blocks stored"};
-  k_m2l_apply_w<true><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(p.levels);
+  if (q32 && ls.lv[0].m2l_q == nullptr) throw Error{AFMM_BAD_ARG, "no fixed-point M2L blocks stored"};
+  if (!q32 && ls.lv[0].m2l == nullptr) throw Error{AFMM_BAD_ARG, "no M2L blocks stored"};
+  if (q32) k_m2l_apply_w<true><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(ls);
+  else k_m2l_apply_w<false><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(ls);
   AFMM_LAUNCH_CHECK();
 }
 

@@ -66,6 +66,37 @@ struct LevelSet {
   long grp0[kMaxLevels + 1] = {0};   // prefix of row-group counts
   long cgrp0[kMaxLevels + 1] = {0};  // prefix of row-chunk counts
   long wgrp0[kMaxLevels + 1] = {0};  // prefix of warp row-chunk counts
+  int src[kMaxLevels] = {0};         // index of entry j among levels 2..L (per-level device tables)
+  uint32_t pf_ahead = 12 * 1024;     // L2 prefetch window of the stored-block M2L kernels (bytes)
+};
+
+// The levels of `ls` whose bit in `mask` (bit t = entry t) equals `keep`,
+// with their prefixes rebuilt and their original indices kept in src.
+inline LevelSet level_subset(const LevelSet& ls, uint32_t mask, bool keep) {
+  LevelSet o;
+  o.pf_ahead = ls.pf_ahead;
+  for (int t = 0; t < ls.nlev; ++t) {
+    if ((((mask >> t) & 1u) != 0) != keep) continue;
+    const int n = o.nlev;
+    o.lv[n] = ls.lv[t];
+    o.src[n] = ls.src[t];
+    o.row0[n + 1] = o.row0[n] + (ls.row0[t + 1] - ls.row0[t]);
+    o.grp0[n + 1] = o.grp0[n] + (ls.grp0[t + 1] - ls.grp0[t]);
+    o.cgrp0[n + 1] = o.cgrp0[n] + (ls.cgrp0[t + 1] - ls.cgrp0[t]);
+    o.wgrp0[n + 1] = o.wgrp0[n] + (ls.wgrp0[t + 1] - ls.wgrp0[t]);
+    ++o.nlev;
+  }
+  return o;
+}
+
+// Tunable launch parameters of a handle (afmm_autotune / afmm_set_tuning);
+// none of them changes the FP64 path's arithmetic.
+struct Tuning {
+  uint32_t pf_fp64 = 12 * 1024;     // L2 prefetch window of the one-column FP64 / mixed M2L (bytes)
+  uint32_t pf_batched = 12 * 1024;  // L2 prefetch window of the batched stored-block M2L (bytes)
+  uint32_t otf_mixed = 0;           // bit t: level t + 2 evaluated on the fly in the one-column mixed path
+  uint32_t otf_batched = 0;         // bit t: level t + 2 evaluated on the fly in batched mixed passes
+  int host_pass_cols = 0;           // columns per pass of host-pointer batched calls (0: automatic)
 };
 
 // L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned
@@ -75,16 +106,17 @@ __device__ __forceinline__ void prefetch_l2_bulk(uintptr_t p, uint32_t bytes) {
 }
 
 // Streams a box's contiguous M2L region into L2 ahead of the warp that
-// consumes it in order: `advance(pos)` keeps the prefetched front kAhead bytes
-// beyond `pos`, in kStep pieces (the last piece may extend < 16 bytes past the
-// region; the block allocations are padded for that).
+// consumes it in order: `advance(pos)` keeps the prefetched front `ahead`
+// bytes beyond `pos` (0: no prefetch), in kStep pieces (the last piece may
+// extend < 16 bytes past the region; the block allocations are padded for
+// that).
 struct L2Stream {
-  static constexpr uintptr_t kAhead = 12 * 1024, kStep = 4096;
-  uintptr_t front, end;
-  __device__ __forceinline__ L2Stream(const void* begin, const void* stop)
-      : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop) {}
+  static constexpr uintptr_t kStep = 4096;
+  uintptr_t front, end, ahead;
+  __device__ __forceinline__ L2Stream(const void* begin, const void* stop, uintptr_t window)
+      : front((uintptr_t)begin & ~(uintptr_t)15), end((uintptr_t)stop), ahead(window) {}
   __device__ __forceinline__ void advance(const void* pos, int lane) {
-    uintptr_t upto = (uintptr_t)pos + kAhead;
+    uintptr_t upto = (uintptr_t)pos + ahead;
     if (upto > end) upto = end;
     while (front < upto) {  // warp-uniform
       if (lane == 0) {
@@ -163,6 +195,7 @@ struct MatvecPlan {
   int n1max[kMaxLevels] = {0};  // largest node count per level
   LevelSet levels;       // levels 2..L for the M2L launch
   NearView near;
+  Tuning tune;
 };
 
 // Near-field launch shape: NT threads per target group (targets rounded up to
@@ -343,10 +376,11 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
 // M2L of every level in FP64: the stored blocks (one thread per skeleton row),
 // or m2l_apply_otf when no blocks are stored.
 void m2l_apply(const MatvecPlan& p, cudaStream_t s);
-// M2L of every level from the 32-bit fixed-point blocks (FP64 arithmetic).
-void m2l_apply_q32(const MatvecPlan& p, cudaStream_t s);
-// M2L of every level with the entries evaluated on the fly in FP64 (mixed.cu).
-void m2l_apply_otf(const MatvecPlan& p, cudaStream_t s);
+// M2L of the given levels from the stored blocks, 32-bit fixed point (q32)
+// or FP64, FP64 arithmetic, one warp per row chunk.
+void m2l_apply_stored(const MatvecPlan& p, const LevelSet& levels, bool q32, cudaStream_t s);
+// M2L of the given levels with the entries evaluated on the fly in FP64 (mixed.cu).
+void m2l_apply_otf(const MatvecPlan& p, const LevelSet& levels, cudaStream_t s);
 // The FP64 sweeps shared by both precisions (leaf charges qs in FP64).
 void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches);
 void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches);

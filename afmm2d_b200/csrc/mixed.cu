@@ -75,9 +75,9 @@ inline int nb(long n, int t) { return (int)((n + t - 1) / t); }
 
 }  // namespace
 
-void m2l_apply_otf(const MatvecPlan& p, cudaStream_t s) {
-  if (p.levels.row0[p.levels.nlev] == 0) return;
-  kernel_table(p.kp.id).m2l_otf(p.levels, p.kp, s);
+void m2l_apply_otf(const MatvecPlan& p, const LevelSet& levels, cudaStream_t s) {
+  if (levels.row0[levels.nlev] == 0) return;
+  kernel_table(p.kp.id).m2l_otf(levels, p.kp, s);
 }
 
 
@@ -124,42 +124,19 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     if (tm) tm->mark(s, "m2m");
     sweep_m2m(p, ms.qs, s, launches);
     if (tm) tm->mark(s, "m2l");
-    // stored form: the 32-bit fixed-point blocks when kept, else the FP64 ones
+    // stored form: the 32-bit fixed-point blocks when kept, else the FP64
+    // ones; the levels of the tuning mask (or all, without stored blocks)
+    // evaluate the entries on the fly
     const bool q32 = p.levels.nlev > 0 && p.levels.lv[0].m2l_q != nullptr;
     const bool stored = q32 || (p.levels.nlev > 0 && p.levels.lv[0].m2l != nullptr);
-    auto m2l_stored_form = [&] {
-      if (q32) m2l_apply_q32(p, s);
-      else m2l_apply(p, s);
-    };
-    // the fixed-point blocks (half the bytes of FP64) are always taken when
-    // kept, so every handle of a problem gives the same bits
-    if (q32) ms.m2l_form = 1;
-    if (ms.m2l_form < 0 && stored) {
-      // one-time choice between the FP64 blocks and the entries on the fly:
-      // both write the same yhat (to FP64 rounding); time each once on this
-      // problem and keep the faster
-      cudaEvent_t e[3];
-      for (auto& x : e) AFMM_CUDA(cudaEventCreate(&x));
-      AFMM_CUDA(cudaEventRecord(e[0], s));
-      kernel_table(p.kp.id).m2l_otf(p.levels, p.kp, s);
-      AFMM_CUDA(cudaEventRecord(e[1], s));
-      m2l_stored_form();
-      AFMM_CUDA(cudaEventRecord(e[2], s));
-      AFMM_CUDA(cudaEventSynchronize(e[2]));
-      AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[0], e[0], e[1]));
-      AFMM_CUDA(cudaEventElapsedTime(&ms.m2l_ms[1], e[1], e[2]));
-      for (auto& x : e) cudaEventDestroy(x);
-      ms.m2l_form = ms.m2l_ms[1] < ms.m2l_ms[0] ? 1 : 0;
-      *launches += 2;
-      if (ms.m2l_form == 0) {  // the result must come from the chosen form
-        kernel_table(p.kp.id).m2l_otf(p.levels, p.kp, s);
-        ++*launches;
-      }
-    } else if (ms.m2l_form == 1 && stored) {
-      m2l_stored_form();
+    const uint32_t otf = stored ? p.tune.otf_mixed : 0xffffffffu;
+    const LevelSet st = level_subset(p.levels, otf, false), fly = level_subset(p.levels, otf, true);
+    if (st.nlev > 0) {
+      m2l_apply_stored(p, st, q32, s);
       ++*launches;
-    } else {
-      kernel_table(p.kp.id).m2l_otf(p.levels, p.kp, s);
+    }
+    if (fly.nlev > 0) {
+      m2l_apply_otf(p, fly, s);
       ++*launches;
     }
     if (tm) tm->mark(s, "l2l");

@@ -21,10 +21,6 @@ struct MixedState {
   double2* leaf_anchor = nullptr;
   float* leaf_span = nullptr;
   float2* rel = nullptr;    // sorted point minus its leaf anchor (FP32)
-  // M2L form: -1 not chosen yet, 0 entries on the fly (FP64), 1 stored FP64
-  // blocks; the first matvec times both once and keeps the faster
-  int m2l_form = -1;
-  float m2l_ms[2] = {0.f, 0.f};
 };
 
 // Buffers of the batched path (kBatchMax right-hand sides per pass).
