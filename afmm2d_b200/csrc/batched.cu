@@ -473,6 +473,12 @@ struct Pass {
 
 }  // namespace
 
+int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {
+  if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+}
+
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s) {
   if (bs.ready) return;
   const int RC = kBatchMax;

@@ -101,11 +101,10 @@ struct afmm_handle {
       {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}, {"tables_alloc", 0.0},
       {"m2l_cudamalloc", 0.0}, {"level_prep", 0.0}, {"aca_alloc_other", 0.0}};
   bool have_last = false;
-  // host-pointer matvecs: copy streams and pass width (0: automatic)
+  // host-pointer matvecs: copy streams
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
   cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
   cudaEvent_t ev_sync = nullptr;
-  int host_pass_cols = 0;
   std::string err;
   ~afmm_handle() {
     for (cudaEvent_t e : {ev_in[0], ev_in[1], ev_done[0], ev_done[1], ev_out[0], ev_out[1], ev_sync})
@@ -901,6 +900,267 @@ void load_levels(afmm_handle* h, SetupImage& im) {
   }
 }
 
+// Host-pointer matvec: passes of at most W columns, each copied in on the
+// h2d stream, computed on the handle's stream and copied out on the d2h
+// stream, with two staging buffers so that the copies of one pass overlap the
+// computation of its neighbours.  compute(qd, yd, nc) runs nc columns from
+// device staging (leading dimension N) on the handle's stream.
+template <class F>
+void host_pipeline(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int W, F&& compute) {
+  const int N = h->N;
+  const size_t need = 2 * (size_t)W;
+  if (h->mixed.host_cap < need) {
+    if (h->mixed.d_qin) h->arena.release(h->mixed.d_qin);
+    if (h->mixed.d_yout) h->arena.release(h->mixed.d_yout);
+    mixed_reserve_io(h->mixed, N, (int)need, h->arena);
+  }
+  cudaStream_t s = h->stream, si = h->s_h2d, so = h->s_d2h;
+  const size_t bytes = sizeof(double) * (size_t)N;
+  // the copy streams start after the work already queued on the handle's stream
+  AFMM_CUDA(cudaEventRecord(h->ev_sync, s));
+  AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_sync, 0));
+  AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_sync, 0));
+  int k = 0;
+  for (int c0 = 0; c0 < nrhs; c0 += W, ++k) {
+    const int nc = std::min(W, nrhs - c0), buf = k & 1;
+    double* qb = h->mixed.d_qin + (size_t)buf * W * N;
+    double* yb = h->mixed.d_yout + (size_t)buf * W * N;
+    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_done[buf], 0));  // pass k-2 has read qb
+    for (int c = 0; c < nc; ++c)
+      AFMM_CUDA(cudaMemcpyAsync(qb + (size_t)c * N, q + (size_t)(c0 + c) * ld, bytes, cudaMemcpyHostToDevice, si));
+    AFMM_CUDA(cudaEventRecord(h->ev_in[buf], si));
+    AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_in[buf], 0));
+    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_out[buf], 0));  // pass k-2's results have left yb
+    compute(qb, yb, nc);
+    AFMM_CUDA(cudaEventRecord(h->ev_done[buf], s));
+    AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_done[buf], 0));
+    for (int c = 0; c < nc; ++c)
+      AFMM_CUDA(cudaMemcpyAsync(y + (size_t)(c0 + c) * ld, yb + (size_t)c * N, bytes, cudaMemcpyDeviceToHost, so));
+    AFMM_CUDA(cudaEventRecord(h->ev_out[buf], so));
+  }
+  // the handle's stream ends after the last copy out
+  AFMM_CUDA(cudaEventRecord(h->ev_sync, so));
+  AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_sync, 0));
+}
+
+
+// ------------------------------------------------------------ autotuner
+// Times the tunable launch parameters (Tuning) on the handle's own problem
+// with CUDA events on its stream and keeps the fastest: the L2 prefetch
+// windows of the stored-block M2L kernels, per level the stored or on-the-fly
+// M2L form of the one-column and batched mixed paths, and the pass width of
+// host-pointer batched calls.  None changes the FP64 path's results; the
+// mixed forms agree within the mixed tolerance.  A cache file keyed by the
+// device and the problem's structure makes repeated tuning free.
+
+// Median of `reps` timed runs of f (after one warm-up), ms.
+template <class F>
+float time_ms(cudaStream_t s, int reps, F&& f) {
+  cudaEvent_t e0, e1;
+  AFMM_CUDA(cudaEventCreate(&e0));
+  AFMM_CUDA(cudaEventCreate(&e1));
+  f();
+  std::vector<float> t;
+  for (int r = 0; r < reps; ++r) {
+    AFMM_CUDA(cudaEventRecord(e0, s));
+    f();
+    AFMM_CUDA(cudaEventRecord(e1, s));
+    AFMM_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    AFMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    t.push_back(ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::sort(t.begin(), t.end());
+  return t[t.size() / 2];
+}
+
+std::string tuning_key(afmm_handle* h) {
+  cudaDeviceProp pr;
+  AFMM_CUDA(cudaGetDeviceProperties(&pr, h->device));
+  std::string name = pr.name;
+  for (char& c : name)
+    if (c == ' ' || c == '|') c = '_';
+  return "dev=" + name + "|N=" + std::to_string(h->N) + "|M=" + std::to_string(h->M) + "|L=" + std::to_string(h->L) +
+         "|kernel=" + std::to_string(h->kernel_id) + "|tol=" + std::to_string(h->tol_pow) +
+         "|stored=" + std::to_string((h->m2l_stored ? 1 : 0) + (h->m2l_q_stored ? 2 : 0)) +
+         "|ranks=" + std::to_string(h->counts[2]) + "|entries=" + std::to_string(h->counts[4]);
+}
+
+void tuning_to(const Tuning& t, int64_t* v) {
+  v[0] = t.pf_fp64;
+  v[1] = t.pf_batched;
+  v[2] = t.otf_mixed;
+  v[3] = t.otf_batched;
+  v[4] = t.host_pass_cols;
+}
+
+Tuning tuning_from(const int64_t* v) {
+  if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[3] < 0 || v[4] < 0 ||
+      v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16))
+    throw Error{AFMM_BAD_ARG, "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16)"};
+  Tuning t;
+  t.pf_fp64 = (uint32_t)v[0];
+  t.pf_batched = (uint32_t)v[1];
+  t.otf_mixed = (uint32_t)v[2];
+  t.otf_batched = (uint32_t)v[3];
+  t.host_pass_cols = (int)v[4];
+  return t;
+}
+
+bool cache_lookup(const char* path, const std::string& key, Tuning& t) {
+  if (!path) return false;
+  FILE* f = std::fopen(path, "r");
+  if (!f) return false;
+  char line[4096];
+  bool hit = false;
+  while (std::fgets(line, sizeof(line), f)) {
+    std::string l(line);
+    const size_t sp = l.find(' ');
+    if (sp == std::string::npos || l.compare(0, sp, key) != 0 || sp != key.size()) continue;
+    long long v[5];
+    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4]) == 5) {
+      int64_t w[5] = {v[0], v[1], v[2], v[3], v[4]};
+      try {
+        t = tuning_from(w);
+        hit = true;  // the last matching line wins
+      } catch (const Error&) {
+      }
+    }
+  }
+  std::fclose(f);
+  return hit;
+}
+
+void cache_store(const char* path, const std::string& key, const Tuning& t) {
+  if (!path) return;
+  FILE* f = std::fopen(path, "a");
+  if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot write the tuning cache ") + path};
+  int64_t v[5];
+  tuning_to(t, v);
+  std::fprintf(f, "%s %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1], (long long)v[2],
+               (long long)v[3], (long long)v[4]);
+  std::fclose(f);
+}
+
+void do_autotune(afmm_handle* h, int what) {
+  cudaStream_t s = h->stream;
+  MatvecPlan& p = h->plan;
+  const int N = h->N;
+  const int nlev = p.levels.nlev;
+  const bool q32 = h->m2l_q_stored, fp64b = h->m2l_stored;
+  // outgoing charges of every level for the M2L timings: one FP64 matvec and
+  // one 16-column mixed pass of seeded random charges
+  DevArena tmp;
+  const int R = kBatchMax;
+  double* dq = tmp.alloc<double>((size_t)N * R);
+  double* dy = tmp.alloc<double>((size_t)N * R);
+  {
+    std::vector<double> hq((size_t)N * R);
+    uint64_t st = 0xA5A5F00Dull;
+    for (double& x : hq) x = (double)(splitmix(st) >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+    AFMM_CUDA(cudaMemcpyAsync(dq, hq.data(), sizeof(double) * hq.size(), cudaMemcpyHostToDevice, s));
+    AFMM_CUDA(cudaStreamSynchronize(s));
+  }
+  mixed_reserve(h->mixed, N, 1, h->arena);
+  batch_reserve(p, h->batch, h->arena, s);
+  int64_t launches = 0;
+  matvec_fp64(p, dq, dy, s, nullptr, &launches);
+  matvec_batched(p, h->mixed, h->batch, dq, N, dy, N, R, 0, s, nullptr, &launches);
+  const int reps = 5;
+  const uint32_t windows[] = {0, 4096, 8192, 12288, 16384, 24576, 32768};
+  if ((what & 1) && nlev > 0 && (fp64b || q32)) {
+    // prefetch window of the one-column stored M2L (FP64 blocks when stored:
+    // the FP64 path's kernel; else the fixed-point copy)
+    float best = 1e30f;
+    uint32_t arg = p.tune.pf_fp64;
+    for (uint32_t w : windows) {
+      p.tune.pf_fp64 = w;
+      const float ms = time_ms(s, reps, [&] { m2l_apply_stored(p, p.levels, !fp64b, s); });
+      if (ms < best) {
+        best = ms;
+        arg = w;
+      }
+    }
+    p.tune.pf_fp64 = arg;
+    // prefetch window of the batched stored-block M2L (mixed: fixed point)
+    best = 1e30f;
+    arg = p.tune.pf_batched;
+    const uint32_t keep = p.tune.otf_batched;
+    p.tune.otf_batched = 0;
+    for (uint32_t w : windows) {
+      p.tune.pf_batched = w;
+      const float ms = time_ms(s, reps, [&] { m2l_batched(p, h->batch, R, 0, s); });
+      if (ms < best) {
+        best = ms;
+        arg = w;
+      }
+    }
+    p.tune.pf_batched = arg;
+    p.tune.otf_batched = keep;
+  }
+  if ((what & 2) && nlev > 0 && (fp64b || q32)) {
+    // per level: stored blocks or entries on the fly, one column and batched
+    uint32_t om = 0, ob = 0;
+    for (int t = 0; t < nlev; ++t) {
+      const LevelSet one = level_subset(p.levels, 1u << t, true);
+      if (one.row0[one.nlev] == 0) continue;
+      const float st_ms = time_ms(s, reps, [&] { m2l_apply_stored(p, one, q32, s); });
+      const float of_ms = time_ms(s, reps, [&] { m2l_apply_otf(p, one, s); });
+      if (of_ms < 0.97f * st_ms) om |= 1u << t;
+      MatvecPlan pc = p;
+      pc.levels = one;
+      pc.tune.otf_batched = 0;
+      const float sb = time_ms(s, reps, [&] { m2l_batched(pc, h->batch, R, 0, s); });
+      pc.tune.otf_batched = 0xffffffffu;
+      const float fb = time_ms(s, reps, [&] { m2l_batched(pc, h->batch, R, 0, s); });
+      if (fb < 0.97f * sb) ob |= 1u << t;
+    }
+    p.tune.otf_mixed = om;
+    p.tune.otf_batched = ob;
+  }
+  if (what & 4) {
+    // pass width of host-pointer batched calls: 16 columns as one pass or as
+    // two overlapped passes of 8 (pinned staging for the timing only)
+    double* hq = nullptr;
+    double* hy = nullptr;
+    AFMM_CUDA(cudaMallocHost(&hq, sizeof(double) * (size_t)N * R));
+    device_alloc_counter().fetch_add(1, std::memory_order_relaxed);
+    cudaError_t e = cudaMallocHost(&hy, sizeof(double) * (size_t)N * R);
+    if (e != cudaSuccess) {
+      cudaFreeHost(hq);
+      AFMM_CUDA(e);
+    }
+    try {
+      AFMM_CUDA(cudaMemcpy(hq, dq, sizeof(double) * (size_t)N * R, cudaMemcpyDeviceToHost));
+      float best = 1e30f;
+      int arg = 0;
+      for (int W : {8, 16}) {
+        p.tune.host_pass_cols = W;
+        const float ms = time_ms(s, 3, [&] {
+          host_pipeline(h, hq, hy, R, N, W, [&](const double* qd, double* yd, int nc) {
+            matvec_batched(p, h->mixed, h->batch, qd, N, yd, N, nc, 0, s, nullptr, &launches);
+          });
+        });
+        if (ms < best) {
+          best = ms;
+          arg = W;
+        }
+      }
+      p.tune.host_pass_cols = arg;
+    } catch (...) {
+      cudaFreeHost(hq);
+      cudaFreeHost(hy);
+      throw;
+    }
+    cudaFreeHost(hq);
+    cudaFreeHost(hy);
+  }
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  h->launches += launches;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1001,57 +1261,6 @@ afmm_status afmm_assemble(afmm_handle* h) {
   });
 }
 
-}  // extern "C"
-
-namespace {
-
-// Host-pointer matvec: passes of at most W columns, each copied in on the
-// h2d stream, computed on the handle's stream and copied out on the d2h
-// stream, with two staging buffers so that the copies of one pass overlap the
-// computation of its neighbours.  compute(qd, yd, nc) runs nc columns from
-// device staging (leading dimension N) on the handle's stream.
-template <class F>
-void host_pipeline(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int W, F&& compute) {
-  const int N = h->N;
-  const size_t need = 2 * (size_t)W;
-  if (h->mixed.host_cap < need) {
-    if (h->mixed.d_qin) h->arena.release(h->mixed.d_qin);
-    if (h->mixed.d_yout) h->arena.release(h->mixed.d_yout);
-    mixed_reserve_io(h->mixed, N, (int)need, h->arena);
-  }
-  cudaStream_t s = h->stream, si = h->s_h2d, so = h->s_d2h;
-  const size_t bytes = sizeof(double) * (size_t)N;
-  // the copy streams start after the work already queued on the handle's stream
-  AFMM_CUDA(cudaEventRecord(h->ev_sync, s));
-  AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_sync, 0));
-  AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_sync, 0));
-  int k = 0;
-  for (int c0 = 0; c0 < nrhs; c0 += W, ++k) {
-    const int nc = std::min(W, nrhs - c0), buf = k & 1;
-    double* qb = h->mixed.d_qin + (size_t)buf * W * N;
-    double* yb = h->mixed.d_yout + (size_t)buf * W * N;
-    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(si, h->ev_done[buf], 0));  // pass k-2 has read qb
-    for (int c = 0; c < nc; ++c)
-      AFMM_CUDA(cudaMemcpyAsync(qb + (size_t)c * N, q + (size_t)(c0 + c) * ld, bytes, cudaMemcpyHostToDevice, si));
-    AFMM_CUDA(cudaEventRecord(h->ev_in[buf], si));
-    AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_in[buf], 0));
-    if (k >= 2) AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_out[buf], 0));  // pass k-2's results have left yb
-    compute(qb, yb, nc);
-    AFMM_CUDA(cudaEventRecord(h->ev_done[buf], s));
-    AFMM_CUDA(cudaStreamWaitEvent(so, h->ev_done[buf], 0));
-    for (int c = 0; c < nc; ++c)
-      AFMM_CUDA(cudaMemcpyAsync(y + (size_t)(c0 + c) * ld, yb + (size_t)c * N, bytes, cudaMemcpyDeviceToHost, so));
-    AFMM_CUDA(cudaEventRecord(h->ev_out[buf], so));
-  }
-  // the handle's stream ends after the last copy out
-  AFMM_CUDA(cudaEventRecord(h->ev_sync, so));
-  AFMM_CUDA(cudaStreamWaitEvent(s, h->ev_sync, 0));
-}
-
-}  // namespace
-
-extern "C" {
-
 afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, int64_t ld, int precision,
                         int mem_device) {
   if (!h) return AFMM_BAD_ARG;
@@ -1090,7 +1299,8 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
       // batched modes at most 8 columns, so that 16 columns make two passes
       // whose copies overlap each other's computation
       int W = 1;
-      if (precision != AFMM_PREC_FP64) W = h->host_pass_cols > 0 ? h->host_pass_cols : std::min(nrhs, 8);
+      if (precision != AFMM_PREC_FP64)
+        W = h->plan.tune.host_pass_cols > 0 ? std::min(nrhs, h->plan.tune.host_pass_cols) : std::min(nrhs, 8);
       host_pipeline(h, q, y, nrhs, ld, W,
                     [&](const double* qd, double* yd, int nc) { compute(qd, h->N, yd, h->N, nc); });
     }
@@ -1385,6 +1595,35 @@ afmm_status afmm_register_kernel(int kernel_id, const void* table, size_t table_
 afmm_status afmm_kernel_name(int kernel_id, const char** name) {
   if (!name) return AFMM_BAD_ARG;
   return guard(nullptr, [&] { *name = kernel_table(kernel_id).name; });
+}
+
+afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int* from_cache) {
+  if (!h) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_autotune before afmm_assemble"};
+    if (what < 0 || what > 7) throw Error{AFMM_BAD_ARG, "what: bit 0 windows, bit 1 M2L forms, bit 2 host passes"};
+    const std::string key = tuning_key(h);
+    Tuning t;
+    if (cache_lookup(cache_path, key, t)) {
+      h->plan.tune = t;
+      if (from_cache) *from_cache = 1;
+      return;
+    }
+    if (from_cache) *from_cache = 0;
+    do_autotune(h, what == 0 ? 7 : what);
+    cache_store(cache_path, key, h->plan.tune);
+  });
+}
+
+afmm_status afmm_get_tuning(afmm_handle* h, int64_t* v5) {
+  if (!h || !v5) return AFMM_BAD_ARG;
+  tuning_to(h->plan.tune, v5);
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_tuning(afmm_handle* h, const int64_t* v5) {
+  if (!h || !v5) return AFMM_BAD_ARG;
+  return guard(h, [&] { h->plan.tune = tuning_from(v5); });
 }
 
 afmm_status afmm_get_device_alloc_count(int64_t* n) {

@@ -37,6 +37,9 @@ struct BatchState {
   double** d_yhat_lv = nullptr;
 };
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s);
+// The M2L stage alone of a batched pass of rc columns (on the batch buffers'
+// current outgoing charges); returns the launches made.
+int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s);
 // y = K q for nrhs > 1 columns in passes of 4, 8 or 16 right-hand sides.
 // fp64 = 1: FP64 throughout (FP64 near field on the tensor cores), passes of 8
 // or 16 columns.

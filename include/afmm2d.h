@@ -234,6 +234,27 @@ afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const double* xy, int64_t* perm,
                                         double* xy_sorted, void* stream);
 
+/* Autotuner.  No reference counterpart (the reference has no launch
+ * parameters; its M2L loop is uniform over levels, src/AFMM2DTree.cpp:1156-1178).
+ * afmm_autotune times, on the handle's own problem with CUDA events, the
+ * launch parameters `what` selects (bit 0: L2 prefetch windows of the
+ * stored-block M2L kernels; bit 1: per level, stored blocks or entries on
+ * the fly in the mixed paths; bit 2: pass width of host-pointer batched
+ * calls; 0 = all) and keeps the fastest in the handle.  With a cache_path
+ * (may be NULL), a line keyed by the device name and the problem's structure
+ * (N, M, levels, kernel, TOL_POW, storage, sum of ranks, M2L entries) is
+ * reused when present (*from_cache = 1) and appended otherwise.  The FP64
+ * path's results do not depend on the tuning; the mixed paths' stay within
+ * their tolerance.  The handle must be assembled.
+ * afmm_get_tuning / afmm_set_tuning read or set the values
+ * v5 = [prefetch window of the one-column M2L (bytes), prefetch window of the
+ * batched M2L (bytes), on-the-fly level mask of the one-column mixed path
+ * (bit t = level t + 2), the same for batched mixed passes, host pass width
+ * (0 = automatic)]. */
+afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int* from_cache);
+afmm_status afmm_get_tuning(afmm_handle* h, int64_t* v5);
+afmm_status afmm_set_tuning(afmm_handle* h, const int64_t* v5);
+
 /* Number of device allocations (cudaMalloc) this library has made in the
  * process so far, over all handles and sets.  No reference counterpart: a
  * diagnostic that lets a caller check that a call allocated nothing. */
