@@ -154,7 +154,7 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   out.skel_ids = arena.alloc<int32_t>(tr);
   out.cpiv_ids = arena.alloc<int32_t>(tr);
   out.skel_xy = arena.alloc<double2>(tr);
-  out.l2p = arena.alloc<double>(out.h_l2p_off[in.nbox]);
+  out.l2p = arena.alloc<double>(out.h_l2p_off[in.nbox] + 4);  // + 32 B for whole-piece L2 prefetches
   AFMM_CUDA(cudaMemcpyAsync(out.skel_off, out.h_skel_off.data(), sizeof(int32_t) * (in.nbox + 1), cudaMemcpyHostToDevice, s));
   AFMM_CUDA(cudaMemcpyAsync(out.l2p_off, out.h_l2p_off.data(), sizeof(int64_t) * (in.nbox + 1), cudaMemcpyHostToDevice, s));
   if (rmax > 0) {

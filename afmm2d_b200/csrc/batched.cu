@@ -294,6 +294,10 @@ __device__ __forceinline__ void m2m_chunk(const LevelView& v, const double* __re
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
   const double* src = src_all + (long)(leaf ? v.leaf_start[b] : v.node_off[b]) * RC;
+  // the box's L2P block and source rows are read once, in order: bring
+  // them into L2 up front
+  prefetch_l2_region(v.l2p_rm + v.l2p_off[b], v.l2p_rm + v.l2p_off[b + 1], lane);
+  prefetch_l2_region(src, src + (long)n * RC, lane);
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   mma_rows<RC, NT>(c, v.l2p_rm + v.l2p_off[b] + i0 + trow, r, n, src, rowok, trow, tsrc);
@@ -315,6 +319,7 @@ __device__ __forceinline__ void l2l_chunk(const LevelView& v, const double* __re
   bool rowok[NT];
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  prefetch_l2_region(v.l2p + v.l2p_off[b] + (long)i0, v.l2p + v.l2p_off[b + 1], lane);
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   mma_rows<RC, NT>(c, v.l2p + v.l2p_off[b] + i0 + trow, n, r, yhat + (long)v.skel_off[b] * RC, rowok, trow, tsrc);

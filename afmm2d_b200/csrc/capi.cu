@@ -564,7 +564,7 @@ void finish_assemble(afmm_handle* h) {
   }
   for (int j = 2; j <= L; ++j) {
     LevelDev& v = h->lv[j];
-    v.l2p_rm = h->arena.alloc<double>(v.h_l2p_off[v.nbox]);
+    v.l2p_rm = h->arena.alloc<double>(v.h_l2p_off[v.nbox] + 4);  // + 32 B for whole-piece L2 prefetches
   }
   build_plan(h);
   AFMM_CUDA(cudaStreamSynchronize(s));
@@ -884,7 +884,7 @@ void load_levels(afmm_handle* h, SetupImage& im) {
     v.skel_ids = h->arena.alloc<int32_t>(tr);
     v.cpiv_ids = h->arena.alloc<int32_t>(tr);
     v.skel_xy = h->arena.alloc<double2>(tr);
-    v.l2p = h->arena.alloc<double>(f.l2p.size());
+    v.l2p = h->arena.alloc<double>(f.l2p.size() + 4);  // + 32 B for whole-piece L2 prefetches
     AFMM_CUDA(cudaMemcpyAsync(v.rank, v.h_rank.data(), sizeof(int32_t) * v.nbox, cudaMemcpyHostToDevice, s));
     AFMM_CUDA(cudaMemcpyAsync(v.skel_off, v.h_skel_off.data(), sizeof(int32_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
     AFMM_CUDA(cudaMemcpyAsync(v.l2p_off, v.h_l2p_off.data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));

@@ -128,6 +128,18 @@ struct L2Stream {
   }
 };
 
+// Prefetches [begin, end) into L2 in 4 KB pieces spread over the warp's
+// lanes (start rounded down to 16 bytes, end up to 16 bytes: the arrays are
+// allocated with that much padding).
+__device__ __forceinline__ void prefetch_l2_region(const void* begin, const void* end, int lane) {
+  const uintptr_t a = (uintptr_t)begin & ~(uintptr_t)15;
+  const uintptr_t e = ((uintptr_t)end + 15) & ~(uintptr_t)15;
+  for (uintptr_t p = a + (uintptr_t)lane * 4096; p < e; p += 32 * 4096) {
+    const uintptr_t left = e - p;
+    prefetch_l2_bulk(p, (uint32_t)(left < 4096 ? left : 4096));
+  }
+}
+
 // Value of a 32-bit fixed-point M2L entry: the double with high word
 // 0x43300000 and low word u is 2^52 + u exactly, so one FMA with the block's
 // decode constants (2^k, -(2^52 + 2^31) 2^k) gives (u - 2^31) 2^k exactly.
