@@ -63,8 +63,8 @@ _SIGS = {
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_get_device_alloc_count": [_vp],
     "afmm_autotune": [_vp, _i, ctypes.c_char_p, _vp],
-    "afmm_get_tuning": [_vp, _vp],
-    "afmm_set_tuning": [_vp, _vp],
+    "afmm_get_tuning": [_vp, _vp, _i],
+    "afmm_set_tuning": [_vp, _vp, _i],
     "afmm_register_kernel": [_i, _vp, ctypes.c_size_t, _i],
     "afmm_kernel_name": [_i, _vp],
     "afmm_destroy": [_vp],
@@ -331,12 +331,12 @@ class AFMM:
                    self._h)
         return out
 
-    TUNING_KEYS = ("pf_fp64", "pf_batched", "otf_mixed", "otf_batched", "host_pass_cols")
+    TUNING_KEYS = ("pf_fp64", "pf_batched", "otf_mixed", "otf_batched", "host_pass_cols", "m2l_t16")
 
     def autotune(self, what=0, cache=None):
         """Times the launch parameters on this problem and keeps the fastest
         (what: bit 0 prefetch windows, bit 1 per-level M2L forms, bit 2 host
-        pass width; 0 = all).  With `cache` (a file path) a stored result for
+        pass width, bit 3 M2L tile shape; 0 = all).  With `cache` (a file path) a stored result for
         the same device and problem structure is reused.  Returns
         (tuning dict, from_cache)."""
         hit = ctypes.c_int()
@@ -345,13 +345,13 @@ class AFMM:
         return self.tuning(), bool(hit.value)
 
     def tuning(self):
-        v = np.zeros(5, np.int64)
-        _check(lib().afmm_get_tuning(self._h, _ptr(v)), self._h)
+        v = np.zeros(len(self.TUNING_KEYS), np.int64)
+        _check(lib().afmm_get_tuning(self._h, _ptr(v), len(v)), self._h)
         return dict(zip(self.TUNING_KEYS, v.tolist()))
 
     def set_tuning(self, **kw):
         v = np.array([kw.get(k, x) for k, x in self.tuning().items()], np.int64)
-        _check(lib().afmm_set_tuning(self._h, _ptr(v)), self._h)
+        _check(lib().afmm_set_tuning(self._h, _ptr(v), len(v)), self._h)
 
     def set_profiling(self, on=True):
         _check(lib().afmm_set_profiling(self._h, 1 if on else 0), self._h)

@@ -279,6 +279,87 @@ __device__ __forceinline__ void m2l_stored_chunk(const LevelView& v, const doubl
   store_tiles<RC, NT, false>(c, yb + (long)r0 * RC, rowok, trow, tsrc);
 }
 
+// m2l_stored_chunk for 16 columns in transposed form on m16n8k4 tiles:
+// yhat^T (16 columns x rows) += qhat_c^T (16 x r_c) M^T (r_c x rows), so the
+// 16 right-hand sides fill the tile's M dimension without padding and the
+// chunk's rows (NT tiles of 8) are the N dimension; half the MMA
+// instructions of the 8x8x4 form for the same products.  Same block reads,
+// same per-box L2 streaming.
+template <int NT, bool Q32>
+__device__ __forceinline__ void m2l_stored_chunk_t16(const LevelView& v, const double* __restrict__ qh,
+                                                     double* __restrict__ yb, int b, int r0, int lane,
+                                                     uint32_t ahead) {
+  constexpr int RC = 16;
+  const int r = v.rank[b];
+  const int i0 = r0 - v.skel_off[b];
+  const int nrow = min(8 * NT, r - i0);
+  const int g = lane >> 2, t = lane & 3;
+  const int sa = v.il[(long)b * 40 + lane];
+  const int sb = lane < 8 ? v.il[(long)b * 40 + 32 + lane] : -1;
+  const int ra = sa >= 0 ? v.rank[sa] : 0, rb = sb >= 0 ? v.rank[sb] : 0;
+  const int oa = sa >= 0 ? v.skel_off[sa] : 0, ob = sb >= 0 ? v.skel_off[sb] : 0;
+  bool rowok[NT];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + g < nrow;
+  long pos = v.m2l_off[b];
+  const long stop = v.m2l_off[b + 1];
+  L2Stream pf(Q32 ? (const void*)(v.m2l_q + pos) : (const void*)(v.m2l + pos),
+              Q32 ? (const void*)(v.m2l_q + stop) : (const void*)(v.m2l + stop), ahead);
+  double c[NT][4];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) c[u][0] = c[u][1] = c[u][2] = c[u][3] = 0.0;
+  for (int s = 0; s < 40; ++s) {
+    const int rc = __shfl_sync(0xffffffffu, s < 32 ? ra : rb, s & 31);
+    if (rc == 0) continue;
+    const int sc = __shfl_sync(0xffffffffu, s < 32 ? oa : ob, s & 31);
+    const double* qb = qh + (long)sc * RC + g;
+    double2 dec = make_double2(0.0, 0.0);
+    if (Q32) {
+      dec = v.m2l_dec[(long)b * 40 + s];
+      pf.advance(v.m2l_q + pos, lane);
+    } else {
+      pf.advance(v.m2l + pos, lane);
+    }
+    const double* M = v.m2l + pos + i0 + g;
+    const uint32_t* MQ = v.m2l_q + pos + i0 + g;
+#pragma unroll 4
+    for (int k0 = 0; k0 < rc; k0 += 4) {
+      const int k = k0 + t;
+      const bool vk = k < rc;
+      const double a0 = vk ? qb[(long)k * RC] : 0.0;
+      const double a1 = vk ? qb[(long)k * RC + 8] : 0.0;
+      double bm[NT];
+      if (Q32) {
+        uint32_t uq[NT];
+#pragma unroll
+        for (int u = 0; u < NT; ++u) uq[u] = (vk && rowok[u]) ? MQ[(long)k * r + u * 8] : 0x80000000u;
+#pragma unroll
+        for (int u = 0; u < NT; ++u) bm[u] = decode_q32(uq[u], dec);
+      } else {
+#pragma unroll
+        for (int u = 0; u < NT; ++u) bm[u] = (vk && rowok[u]) ? M[(long)k * r + u * 8] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < NT; ++u) mma_f64_16x8x4(c[u], a0, a1, bm[u]);
+    }
+    pos += (long)r * rc;
+  }
+  // D^T[col][row]: lane holds columns g, g + 8 of rows 2t, 2t + 1 of each tile
+#pragma unroll
+  for (int u = 0; u < NT; ++u) {
+    const int row = u * 8 + 2 * t;
+    double* o = yb + (long)(r0 + row) * RC + g;
+    if (row < nrow) {
+      o[0] = c[u][0];
+      o[8] = c[u][2];
+    }
+    if (row + 1 < nrow) {
+      o[RC] = c[u][1];
+      o[RC + 8] = c[u][3];
+    }
+  }
+}
+
 // M2M on FP64 tensor-core tiles: qhat rows of box b = L2P_b^T src_b, one warp
 // per chunk of up to kChunkRows skeleton rows (the row-major L2P copy is the
 // column-major A with lda = rank).
@@ -388,6 +469,23 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const doubl
 #undef AFMM_M2L
 }
 
+template <bool Q32>
+__global__ void __launch_bounds__(128) k_m2l_stored_mma_t16(LevelSet ls, const double* const* __restrict__ qhat_lv,
+                                                            double* const* __restrict__ yhat_lv) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ls.cgrp0[ls.nlev]) return;  // whole warps only
+  int j = 0;
+  while (j + 1 < ls.nlev && gw >= ls.cgrp0[j + 1]) ++j;
+  const LevelView& v = ls.lv[j];
+  const long g = gw - ls.cgrp0[j];
+  const int b = v.cgrp_box[g];
+  const int r0 = v.cgrp_row[g];
+#define AFMM_M2L(NT) m2l_stored_chunk_t16<NT, Q32>(v, qhat_lv[ls.src[j]], yhat_lv[ls.src[j]], b, r0, lane, ls.pf_ahead)
+  AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2L)
+#undef AFMM_M2L
+}
+
 inline int nbk(long n, int t) { return (int)((n + t - 1) / t); }
 
 template <int RC>
@@ -410,8 +508,14 @@ struct Pass {
       // stored blocks: one HBM read of the blocks serves all RC columns
       // (mixed precision: the 32-bit fixed-point copy, half the bytes)
       const long warps = st.cgrp0[st.nlev];
-      if (q32) k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
-      else k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+      if (RC == 16 && p.tune.m2l_t16) {
+        if (q32) k_m2l_stored_mma_t16<true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+        else k_m2l_stored_mma_t16<false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+      } else if (q32) {
+        k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+      } else {
+        k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+      }
       AFMM_LAUNCH_CHECK();
       ++n;
     }

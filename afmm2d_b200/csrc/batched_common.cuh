@@ -47,6 +47,15 @@ __device__ __forceinline__ void mma_f64_8x8x4(double& c0, double& c1, double a, 
                : "d"(a), "d"(b));
 }
 
+// FP64 MMA m16n8k4 (sm_90 and later; D = A B + C, A 16x4, B 4x8): lane
+// l = 4g + t holds A[g][t], A[g+8][t]; B[t][g]; D[g][2t], D[g][2t+1],
+// D[g+8][2t], D[g+8][2t+1].
+__device__ __forceinline__ void mma_f64_16x8x4(double (&c)[4], double a0, double a1, double b) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a0), "d"(a1), "d"(b));
+}
+
 }  // namespace batched_common
 
 using namespace batched_common;

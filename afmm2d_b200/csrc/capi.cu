@@ -988,24 +988,29 @@ std::string tuning_key(afmm_handle* h) {
          "|ranks=" + std::to_string(h->counts[2]) + "|entries=" + std::to_string(h->counts[4]);
 }
 
+constexpr int kTuningValues = 6;
+
 void tuning_to(const Tuning& t, int64_t* v) {
   v[0] = t.pf_fp64;
   v[1] = t.pf_batched;
   v[2] = t.otf_mixed;
   v[3] = t.otf_batched;
   v[4] = t.host_pass_cols;
+  v[5] = t.m2l_t16;
 }
 
 Tuning tuning_from(const int64_t* v) {
-  if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[3] < 0 || v[4] < 0 ||
-      v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16))
-    throw Error{AFMM_BAD_ARG, "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16)"};
+  if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[2] > 0xffffffffll || v[3] < 0 ||
+      v[3] > 0xffffffffll || v[4] < 0 || v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16) || v[5] < 0 || v[5] > 1)
+    throw Error{AFMM_BAD_ARG,
+                "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16; shape 0 or 1)"};
   Tuning t;
   t.pf_fp64 = (uint32_t)v[0];
   t.pf_batched = (uint32_t)v[1];
   t.otf_mixed = (uint32_t)v[2];
   t.otf_batched = (uint32_t)v[3];
   t.host_pass_cols = (int)v[4];
+  t.m2l_t16 = (int)v[5];
   return t;
 }
 
@@ -1019,9 +1024,10 @@ bool cache_lookup(const char* path, const std::string& key, Tuning& t) {
     std::string l(line);
     const size_t sp = l.find(' ');
     if (sp == std::string::npos || l.compare(0, sp, key) != 0 || sp != key.size()) continue;
-    long long v[5];
-    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4]) == 5) {
-      int64_t w[5] = {v[0], v[1], v[2], v[3], v[4]};
+    long long v[kTuningValues];
+    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) ==
+        kTuningValues) {
+      int64_t w[kTuningValues] = {v[0], v[1], v[2], v[3], v[4], v[5]};
       try {
         t = tuning_from(w);
         hit = true;  // the last matching line wins
@@ -1037,10 +1043,10 @@ void cache_store(const char* path, const std::string& key, const Tuning& t) {
   if (!path) return;
   FILE* f = std::fopen(path, "a");
   if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot write the tuning cache ") + path};
-  int64_t v[5];
+  int64_t v[kTuningValues];
   tuning_to(t, v);
-  std::fprintf(f, "%s %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1], (long long)v[2],
-               (long long)v[3], (long long)v[4]);
+  std::fprintf(f, "%s %lld %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1], (long long)v[2],
+               (long long)v[3], (long long)v[4], (long long)v[5]);
   std::fclose(f);
 }
 
@@ -1119,6 +1125,20 @@ void do_autotune(afmm_handle* h, int what) {
     }
     p.tune.otf_mixed = om;
     p.tune.otf_batched = ob;
+  }
+  if ((what & 8) && nlev > 0 && (fp64b || q32)) {
+    // tile shape of the 16-column stored M2L (the levels kept stored)
+    float best = 1e30f;
+    int arg = p.tune.m2l_t16;
+    for (int t16 : {0, 1}) {
+      p.tune.m2l_t16 = t16;
+      const float ms = time_ms(s, reps, [&] { m2l_batched(p, h->batch, R, 0, s); });
+      if (ms < best) {
+        best = ms;
+        arg = t16;
+      }
+    }
+    p.tune.m2l_t16 = arg;
   }
   if (what & 4) {
     // pass width of host-pointer batched calls: 16 columns as one pass or as
@@ -1601,7 +1621,8 @@ afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int*
   if (!h) return AFMM_BAD_ARG;
   return guard(h, [&] {
     if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_autotune before afmm_assemble"};
-    if (what < 0 || what > 7) throw Error{AFMM_BAD_ARG, "what: bit 0 windows, bit 1 M2L forms, bit 2 host passes"};
+    if (what < 0 || what > 15)
+      throw Error{AFMM_BAD_ARG, "what: bit 0 windows, bit 1 M2L forms, bit 2 host passes, bit 3 M2L tile shape"};
     const std::string key = tuning_key(h);
     Tuning t;
     if (cache_lookup(cache_path, key, t)) {
@@ -1610,20 +1631,20 @@ afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int*
       return;
     }
     if (from_cache) *from_cache = 0;
-    do_autotune(h, what == 0 ? 7 : what);
+    do_autotune(h, what == 0 ? 15 : what);
     cache_store(cache_path, key, h->plan.tune);
   });
 }
 
-afmm_status afmm_get_tuning(afmm_handle* h, int64_t* v5) {
-  if (!h || !v5) return AFMM_BAD_ARG;
-  tuning_to(h->plan.tune, v5);
+afmm_status afmm_get_tuning(afmm_handle* h, int64_t* v, int n) {
+  if (!h || !v || n < kTuningValues) return AFMM_BAD_ARG;
+  tuning_to(h->plan.tune, v);
   return AFMM_OK;
 }
 
-afmm_status afmm_set_tuning(afmm_handle* h, const int64_t* v5) {
-  if (!h || !v5) return AFMM_BAD_ARG;
-  return guard(h, [&] { h->plan.tune = tuning_from(v5); });
+afmm_status afmm_set_tuning(afmm_handle* h, const int64_t* v, int n) {
+  if (!h || !v || n < kTuningValues) return AFMM_BAD_ARG;
+  return guard(h, [&] { h->plan.tune = tuning_from(v); });
 }
 
 afmm_status afmm_get_device_alloc_count(int64_t* n) {

@@ -97,6 +97,7 @@ struct Tuning {
   uint32_t otf_mixed = 0;           // bit t: level t + 2 evaluated on the fly in the one-column mixed path
   uint32_t otf_batched = 0;         // bit t: level t + 2 evaluated on the fly in batched mixed passes
   int host_pass_cols = 0;           // columns per pass of host-pointer batched calls (0: automatic)
+  int m2l_t16 = 0;                  // 16-column stored M2L on transposed m16n8k4 tiles (else 8x8x4 tiles)
 };
 
 // L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned

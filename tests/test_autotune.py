@@ -16,8 +16,8 @@ MIXED_TOL = 1e-6
 
 def test_autotune_rejects_null_handle():
     assert A.lib().afmm_autotune(None, 0, None, None) == 1
-    assert A.lib().afmm_get_tuning(None, None) == 1
-    assert A.lib().afmm_set_tuning(None, None) == 1
+    assert A.lib().afmm_get_tuning(None, None, 6) == 1
+    assert A.lib().afmm_set_tuning(None, None, 6) == 1
 
 
 @pytest.mark.gpu
@@ -70,3 +70,8 @@ def test_set_tuning_values_and_forms():
         a.set_tuning(pf_fp64=7)
     with pytest.raises(A.AFMMError):
         a.set_tuning(host_pass_cols=17)
+    # the transposed m16n8k4 tiles of the 16-column stored M2L: FP64-batched
+    # columns still match the FP64 path to rounding, mixed within tolerance
+    a.set_tuning(m2l_t16=1, otf_mixed=0, otf_batched=0)
+    assert_rel(a.computeMatVecProduct(Q, precision="fp64_batched")[:, 1], y64, 1e-12)
+    assert_rel(a.computeMatVecProduct(Q, precision="mixed")[:, 1], y64, MIXED_TOL)
