@@ -52,6 +52,8 @@ def parse():
                     help="points of the reference CPU run (the workload's N: full size, with a parity check of the "
                          "FP64 GPU result against the reference's output)")
     ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
+    ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
+                    help="auto: run the library's autotuner during setup (default); default: built-in parameters")
     return ap.parse_args()
 
 
@@ -249,6 +251,8 @@ def run_ours(args):
         return float(np.mean(ms))
 
     if args.profile_once:
+        if args.tuning == "auto":
+            a.autotune()
         for name in paths:
             call(name)
         torch.cuda.synchronize()
@@ -258,6 +262,14 @@ def run_ours(args):
     torch.cuda.synchronize()
     clk = ClockSampler(local)
     clk.start()
+    # every path with the built-in launch parameters first, then (setup, not
+    # timed) the autotuner on this problem; the reported paths use its choice
+    t_default = {name: timed(name, args.steps, args.warmup) for name in paths}
+    tuning, tune_s = a.tuning(), 0.0
+    if args.tuning == "auto":
+        t0 = time.perf_counter()
+        tuning, _ = a.autotune()
+        tune_s = time.perf_counter() - t0
     t_dev = {}
     launches = {}
     stages = {}
@@ -359,6 +371,8 @@ def run_ours(args):
             "rel_err_fp64_batched_vs_fp64_max_col": err_fp64b,
             "rel_err_fp64_vs_dense_16_leaves": err_dense,
             "setup_s": setup_s, "setup_process_warmup_s": warm_s, "setup": a.setup_times(), "stages_ms": stages,
+            "tuning": {"mode": args.tuning, "values": tuning, "autotune_s": tune_s,
+                       "default_ms_per_step": t_default},
             "counts": counts,
             "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
             "clocks": clocks, "gpu_launches": int(launches["batched"]),
