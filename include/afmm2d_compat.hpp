@@ -53,13 +53,13 @@ class AFMM {
   std::vector<double> sorted_Properties;  // original index of each sorted point (:25)
 
   // loc: N x 2 column-major (Eigen::MatrixXd layout) unless interleaved.
-  AFMM(int N_, int M_, int tol_pow, const double* loc, afmm_kernel_id kernel = AFMM_KERNEL_LOG,
+  AFMM(int N_, int M_, int tol_pow, const double* loc, int kernel = AFMM_KERNEL_LOG,
        bool interleaved = false, double kparam = 0.01)
       : N(N_), MinParticlesInLeaf(M_), TOL_POW(tol_pow) {
     init(loc, interleaved ? AFMM_LOC_INTERLEAVED : AFMM_LOC_COLMAJOR, kernel, kparam);
   }
 #ifdef AFMM2D_COMPAT_EIGEN
-  AFMM(int N_, int M_, int tol_pow, Eigen::MatrixXd& loc, afmm_kernel_id kernel = AFMM_KERNEL_LOG,
+  AFMM(int N_, int M_, int tol_pow, Eigen::MatrixXd& loc, int kernel = AFMM_KERNEL_LOG,
        double kparam = 0.01)
       : N(N_), MinParticlesInLeaf(M_), TOL_POW(tol_pow) {
     init(loc.data(), AFMM_LOC_COLMAJOR, kernel, kparam);
@@ -91,20 +91,47 @@ class AFMM {
     return e;
   }
 
+  // Setup files (afmm_save / afmm_load): a later process skips the KD sort
+  // and the ACA; the loaded object's matvecs have the saved one's bits.
+  void save(const std::string& path) { afmm2d::check(afmm_save(h_, path.c_str()), h_); }
+  static AFMM* load(const std::string& path) {
+    afmm_handle* h = nullptr;
+    afmm2d::check(afmm_load(path.c_str(), &h), nullptr);
+    return new AFMM(h);
+  }
+  // Launch parameters timed on this problem (afmm_autotune); cache may be NULL.
+  bool autotune(const char* cache = nullptr) {
+    int hit = 0;
+    afmm2d::check(afmm_autotune(h_, 0, cache, &hit), h_);
+    return hit != 0;
+  }
+
   afmm_handle* handle() const { return h_; }
 
  private:
   afmm_handle* h_ = nullptr;
-  void init(const double* loc, int layout, afmm_kernel_id kernel, double kparam) {
-    afmm2d::check(afmm_create(N, MinParticlesInLeaf, TOL_POW, loc, layout, kernel, &kparam, 1, &h_), nullptr);
-    int L = 0;
-    afmm2d::check(afmm_get_nlevels(h_, &L), h_);
-    nLevels = (unsigned)L;
+  explicit AFMM(afmm_handle* h) : h_(h) {
+    int v[5] = {0, 0, 0, 0, 0};
+    afmm2d::check(afmm_get_params(h_, v, nullptr), h_);
+    N = v[0];
+    MinParticlesInLeaf = v[1];
+    TOL_POW = v[2];
+    nLevels = (unsigned)v[3];
+    read_sorted();
+  }
+  void read_sorted() {
     std::vector<int64_t> perm(N);
     afmm2d::check(afmm_get_permutation(h_, perm.data()), h_);
     sorted_Properties.assign(perm.begin(), perm.end());
     sorted_Locations.resize(2 * (size_t)N);
     afmm2d::check(afmm_get_sorted_locations(h_, sorted_Locations.data()), h_);
+  }
+  void init(const double* loc, int layout, int kernel, double kparam) {
+    afmm2d::check(afmm_create(N, MinParticlesInLeaf, TOL_POW, loc, layout, kernel, &kparam, 1, &h_), nullptr);
+    int L = 0;
+    afmm2d::check(afmm_get_nlevels(h_, &L), h_);
+    nLevels = (unsigned)L;
+    read_sorted();
   }
 };
 

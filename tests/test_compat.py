@@ -27,6 +27,17 @@ int main() {
   std::vector<double> y = afmm->computeMatVecProduct(b);
   double e = afmm->evaluateError(0, 1);
   std::printf("nLevels %u first %.17g err %.3e\n", afmm->nLevels, y[0], e);
+  afmm->save("afmm_setup.bin");
+  AFMM* again = AFMM::load("afmm_setup.bin");
+  std::vector<double> y2 = again->computeMatVecProduct(b);
+  bool same = again->N == N && again->nLevels == afmm->nLevels;
+  for (int j = 0; j < N; ++j) same = same && y2[j] == y[j];
+  std::printf("reload identical: %d\n", (int)same);
+  again->autotune();
+  std::vector<double> y3 = again->computeMatVecProduct(b);
+  for (int j = 0; j < N; ++j) same = same && y3[j] == y[j];
+  std::printf("tuned identical: %d\n", (int)same);
+  delete again;
   delete afmm;
   try {
     AFMM bad(100, 64, 8, loc.data());
@@ -54,6 +65,7 @@ def test_compat_header_builds(tmp_path):
 
 @pytest.mark.gpu
 def test_compat_driver_runs(tmp_path):
-    out = subprocess.run([str(build_driver(tmp_path))], capture_output=True, text=True, timeout=300)
+    out = subprocess.run([str(build_driver(tmp_path))], capture_output=True, text=True, timeout=300, cwd=tmp_path)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "nLevels 3" in out.stdout and "rejected: 1" in out.stdout
+    assert "reload identical: 1" in out.stdout and "tuned identical: 1" in out.stdout
