@@ -221,6 +221,9 @@ struct LevelDev {
   int32_t* wgrp_box = nullptr;   // row chunk (<= 32 skeleton rows of one box: a warp's lanes) -> box
   int32_t* wgrp_row = nullptr;   // row chunk -> first skeleton row
   long nwgroups = 0;
+  int32_t* nwgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
+  int32_t* nwgrp_row = nullptr;  // node-row chunk -> first node row
+  long nnwgroups = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)

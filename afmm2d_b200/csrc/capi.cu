@@ -249,6 +249,9 @@ void build_plan(afmm_handle* h) {
     v.wgrp_box = d.wgrp_box;
     v.wgrp_row = d.wgrp_row;
     v.nwgroups = d.nwgroups;
+    v.nwgrp_box = d.nwgrp_box;
+    v.nwgrp_row = d.nwgrp_row;
+    v.nnwgroups = d.nnwgroups;
     v.m2l_q = d.m2l_q;
     v.m2l_dec = d.m2l_dec;
     v.nrows = d.total_rank;
@@ -388,7 +391,7 @@ void create_layout(afmm_handle* h) {
   lf.node_ids = h->arena.alloc<int32_t>(N);
   AFMM_CUDA(cudaMemcpyAsync(lf.node_off, lf.h_node_off.data(), sizeof(int32_t) * (nleaf + 1), cudaMemcpyHostToDevice, s));
   AFMM_CUDA(cudaMemcpyAsync(lf.node_ids, ids.data(), sizeof(int32_t) * N, cudaMemcpyHostToDevice, s));
-  h->d_qs = h->arena.alloc<double>(N);
+  h->d_qs = h->arena.alloc<double>(N + 2);  // + 16 B: whole-piece L2 prefetches of source rows
   h->d_ys = h->arena.alloc<double>(N);
   h->d_q = h->arena.alloc<double>(N);
   h->d_y = h->arena.alloc<double>(N);
@@ -507,7 +510,7 @@ void finish_assemble(afmm_handle* h) {
     const double t_al = now_s();
     v.m2l = h->m2l_stored ? h->arena.alloc<double>(v.h_m2l_off[v.nbox] + 32) : nullptr;
     h->setup_phase[5].second += now_s() - t_al;
-    v.qhat = h->arena.alloc<double>(v.total_rank);
+    v.qhat = h->arena.alloc<double>(v.total_rank + 2);  // + 16 B: whole-piece L2 prefetches
     v.yhat = h->arena.alloc<double>(v.total_rank);
     // row -> box maps for the thread-per-row sweeps
     v.skel_box = h->arena.alloc<int32_t>(v.total_rank);
@@ -521,9 +524,10 @@ void finish_assemble(afmm_handle* h) {
     // ceil(n / kChunkRows) chunks of equal size rounded up to 8 rows; and
     // balanced chunks of at most 32 skeleton rows (a warp's lanes, the
     // one-column M2L)
-    for (int kind = 0; kind < 4; ++kind) {
-      const int span = kind == 0 ? 8 : (kind == 3 ? 32 : kChunkRows);
-      const bool nodes = kind == 2;
+    // (and the same of at most 32 node rows, the one-column L2L)
+    for (int kind = 0; kind < 5; ++kind) {
+      const int span = kind == 0 ? 8 : (kind >= 3 ? 32 : kChunkRows);
+      const bool nodes = kind == 2 || kind == 4;
       std::vector<int32_t> gb, gr;
       for (long b = 0; b < v.nbox; ++b) {
         const int rows = nodes ? v.h_node_off[b + 1] - v.h_node_off[b] : v.h_rank[b];
@@ -555,10 +559,14 @@ void finish_assemble(afmm_handle* h) {
         v.nncgroups = (long)gb.size();
         v.ncgrp_box = db;
         v.ncgrp_row = dr;
-      } else {
+      } else if (kind == 3) {
         v.nwgroups = (long)gb.size();
         v.wgrp_box = db;
         v.wgrp_row = dr;
+      } else {
+        v.nnwgroups = (long)gb.size();
+        v.nwgrp_box = db;
+        v.nwgrp_row = dr;
       }
     }
   }

@@ -199,14 +199,6 @@ __global__ void k_scatter(const double* __restrict__ ys, const int64_t* __restri
   if (i < n) y[perm[i]] = ys[i];
 }
 
-// M2M (src/AFMM2DTree.cpp:1129-1154): one thread per output (skeleton row of
-// the level), a warp's consecutive outputs reading the row-major L2P
-// contiguously.
-__global__ void k_m2m(LevelView v, const double* __restrict__ src_all, int leaf) {
-  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row < v.nrows) m2m_row(v, src_all, leaf, row);
-}
-
 // Row-major copy of L2P (per box, r fastest) for the M2M sweep.
 template <class T>
 __global__ void k_l2p_transpose(LevelView v, const T* __restrict__ cm, T* rm) {
@@ -308,17 +300,49 @@ __global__ void __launch_bounds__(128) k_m2l_apply_w(LevelSet ls) {
   if (act) v.yhat[r0 + lane] = acc;
 }
 
-// L2L (src/AFMM2DTree.cpp:1180-1197): one thread per node row of the level.
-__global__ void k_l2l(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys, int leaf) {
-  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g < v.nnodes) l2l_row(v, child_yhat, ys, leaf, g);
+// End of warp chunk g of a chunk table (the next chunk's first row, or the
+// end of the box).
+__device__ __forceinline__ int wchunk_end(const int32_t* first, long g, long n, int box_end) {
+  return g + 1 < n ? min(box_end, first[g + 1]) : box_end;
 }
+
+// M2M (m2m_row's arithmetic, so the same bits) with one warp per chunk of up
+// to 32 skeleton rows of one box: no warp straddles two boxes, and the box's
+// L2P block and source rows are brought into L2 up front.
+__global__ void __launch_bounds__(128) k_m2m_w(LevelView v, const double* __restrict__ src_all, int leaf) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= v.nwgroups) return;
+  const int b = v.wgrp_box[g];
+  const int r0 = v.wgrp_row[g];
+  const int end = wchunk_end(v.wgrp_row, g, v.nwgroups, v.skel_off[b] + v.rank[b]);
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const double* src = src_all + (leaf ? v.leaf_start[b] : v.node_off[b]);
+  prefetch_l2_region(v.l2p_rm + v.l2p_off[b], v.l2p_rm + v.l2p_off[b + 1], lane);
+  prefetch_l2_region(src, src + n, lane);
+  if (r0 + lane < end) m2m_row(v, src_all, leaf, r0 + lane);
+}
+
+// L2L (l2l_row's arithmetic) with one warp per chunk of up to 32 node rows of
+// one box, the box's L2P block brought into L2 up front.
+__global__ void __launch_bounds__(128) k_l2l_w(LevelView v, double* __restrict__ child_yhat, double* __restrict__ ys,
+                                               int leaf) {
+  const long g = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (g >= v.nnwgroups) return;
+  const int b = v.nwgrp_box[g];
+  const int g0 = v.nwgrp_row[g];
+  const int end = wchunk_end(v.nwgrp_row, g, v.nnwgroups, v.node_off[b + 1]);
+  prefetch_l2_region(v.l2p + v.l2p_off[b] + (g0 - v.node_off[b]), v.l2p + v.l2p_off[b + 1], lane);
+  if (g0 + lane < end) l2l_row(v, child_yhat, ys, leaf, g0 + lane);
+}
+
 
 void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* launches) {
   for (int j = p.L; j >= 2; --j) {
     const LevelView& v = p.lv[j];
     if (v.nrows == 0) continue;
-    k_m2m<<<(int)((v.nrows + 127) / 128), 128, 0, s>>>(v, j == p.L ? qs : p.lv[j + 1].qhat, j == p.L);
+    k_m2m_w<<<(int)((v.nwgroups * 32 + 127) / 128), 128, 0, s>>>(v, j == p.L ? qs : p.lv[j + 1].qhat, j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
@@ -328,7 +352,8 @@ void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launche
   for (int j = 2; j <= p.L; ++j) {
     const LevelView& v = p.lv[j];
     if (v.nnodes == 0) continue;
-    k_l2l<<<(int)((v.nnodes + 127) / 128), 128, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys, j == p.L);
+    k_l2l_w<<<(int)((v.nnwgroups * 32 + 127) / 128), 128, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys,
+                                                                  j == p.L);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }

@@ -51,6 +51,9 @@ struct LevelView {
   const int32_t* wgrp_box = nullptr;  // row chunk (<= 32 skeleton rows of one box) -> box
   const int32_t* wgrp_row = nullptr;  // row chunk -> first skeleton row
   long nwgroups = 0;
+  const int32_t* nwgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
+  const int32_t* nwgrp_row = nullptr;  // node-row chunk -> first node row
+  long nnwgroups = 0;
   uint32_t* m2l_q = nullptr;          // 32-bit fixed-point blocks (null when not stored)
   double2* m2l_dec = nullptr;         // per (box, slot) decode constants
   long nrows = 0;                     // skeleton rows (sum of ranks)

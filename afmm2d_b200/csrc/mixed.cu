@@ -97,7 +97,7 @@ void mixed_setup(MatvecPlan& p, std::vector<LevelDev>&, MixedState& ms, DevArena
 void mixed_reserve(MixedState& ms, int N, int nrhs, DevArena& arena) {
   if (ms.rhs_cap >= nrhs) return;
   ms.qs32 = arena.alloc<float>((size_t)N * nrhs);
-  ms.qs = arena.alloc<double>((size_t)N * nrhs);
+  ms.qs = arena.alloc<double>((size_t)N * nrhs + 2);  // + 16 B: whole-piece L2 prefetches
   ms.ys = arena.alloc<double>((size_t)N * nrhs);
   ms.rhs_cap = nrhs;
 }
