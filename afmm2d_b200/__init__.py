@@ -51,6 +51,7 @@ _SIGS = {
     "afmm_set_m2l_storage": [_vp, _i],
     "afmm_get_m2l_stored": [_vp, _vp],
     "afmm_set_m2l_fixed_point": [_vp, _i],
+    "afmm_set_aca_plan": [_vp, _i, _i],
     "afmm_get_m2l_fixed_point": [_vp, _vp],
     "afmm_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_get_setup_times": [_vp, _vp],
@@ -236,6 +237,11 @@ class AFMM:
         """Before assemble(): keep a 32-bit fixed-point copy of the stored M2L
         blocks for the mixed-precision paths (default on, when it fits)."""
         _check(lib().afmm_set_m2l_fixed_point(self._h, 1 if on else 0), self._h)
+
+    def set_aca_plan(self, cluster=0, ctas_per_sm=0):
+        """Before assemble(): CTAs per box and per SM of the ACA kernel
+        (0 = automatic); results do not depend on it, only the setup time."""
+        _check(lib().afmm_set_aca_plan(self._h, int(cluster), int(ctas_per_sm)), self._h)
 
     def m2l_fixed_point(self):
         v = ctypes.c_int()

@@ -48,8 +48,14 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
   int dev = 0, nsm = 148;
   AFMM_CUDA(cudaGetDevice(&dev));
   AFMM_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  const long want_ctas = 2L * nsm;
-  const size_t budget = in.nbox >= want_ctas ? 100 * 1024 : 200 * 1024;
+  long want_ctas = 2L * nsm;
+  size_t budget = in.nbox >= want_ctas ? 100 * 1024 : 200 * 1024;
+  if (in.ctas_per_sm == 1 || in.ctas_per_sm == 2) {  // set-up tuning overrides
+    budget = in.ctas_per_sm == 1 ? 200 * 1024 : 100 * 1024;
+    want_ctas = (long)in.ctas_per_sm * nsm;
+  }
+  if (in.cluster != 0 && (in.cluster < 1 || in.cluster > 16 || (in.cluster & (in.cluster - 1))))
+    throw Error{AFMM_BAD_ARG, "ACA cluster size must be a power of two up to 16"};
   int C = 1, chunk = 0, vcap = 0, ucap = 0;
   size_t smem = 0, gslot = 0;
   size_t off[AR_N] = {0};
@@ -83,7 +89,8 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     used += al(sizeof(double) * (size_t)ucap * n1max);
     size_t left = budget > used ? budget - used : 0;
     vcap = std::min<long>(rcap, (long)(left / (sizeof(double) * chunk)));
-    if (vcap >= std::min(rcap, 48) || C == 16 || in.nbox * C >= want_ctas) {
+    const bool pick = in.cluster ? C == in.cluster : (vcap >= std::min(rcap, 48) || C == 16 || in.nbox * C >= want_ctas);
+    if (pick) {
       in_smem[AR_V] = 1;
       off[AR_V] = used;
       used += al(sizeof(double) * (size_t)vcap * chunk);

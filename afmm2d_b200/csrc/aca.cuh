@@ -77,6 +77,8 @@ struct AcaLevelIn {
   double tol;
   KernelParams kp;
   int32_t* rank_out;        // nbox (device)
+  int cluster = 0;          // CTAs per box (power of two <= 16); 0: the planner's choice
+  int ctas_per_sm = 0;      // 1 (full shared-memory budget) or 2 (half); 0: the planner's choice
 };
 
 struct AcaLevelOut {

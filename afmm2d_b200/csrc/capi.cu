@@ -69,6 +69,7 @@ struct afmm_handle {
   int m2l_mode = AFMM_M2L_AUTO;  // afmm_m2l_storage
   bool m2l_stored = false;
   int m2l_q_mode = 1;            // also keep a 32-bit fixed-point copy for the mixed paths
+  int aca_cluster = 0, aca_ctas_per_sm = 0;  // ACA planner overrides (0: automatic)
   bool m2l_q_stored = false;
   KernelParams kp{};
   cudaStream_t stream = nullptr;
@@ -425,6 +426,8 @@ void do_assemble(afmm_handle* h) {
     in.h_node_off = v.h_node_off;
     in.tol = tol;
     in.kp = h->kp;
+    in.cluster = h->aca_cluster;
+    in.ctas_per_sm = h->aca_ctas_per_sm;
     int n1max = 0, n2max = 0;
     const std::vector<int32_t>& il = h->h_il[j];
     for (long b = 0; b < v.nbox; ++b) {
@@ -448,6 +451,7 @@ void do_assemble(afmm_handle* h) {
     h->setup_phase[0].second += out.aca_s;
     h->setup_phase[1].second += out.l2p_s;
     h->setup_phase.push_back({"aca_level" + std::to_string(j), out.aca_s});
+    h->setup_phase.push_back({"aca_cluster_level" + std::to_string(j), (double)out.cluster});
     v.skel_off = out.skel_off;
     v.skel_ids = out.skel_ids;
     v.cpiv_ids = out.cpiv_ids;
@@ -1483,6 +1487,17 @@ afmm_status afmm_set_m2l_storage(afmm_handle* h, int mode) {
     return AFMM_BAD_ARG;
   }
   h->m2l_mode = mode;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_aca_plan(afmm_handle* h, int cluster, int ctas_per_sm) {
+  if (!h) return AFMM_BAD_ARG;
+  if (h->assembled || cluster < 0 || cluster > 16 || (cluster & (cluster - 1)) || ctas_per_sm < 0 || ctas_per_sm > 2) {
+    h->err = "afmm_set_aca_plan: before afmm_assemble; cluster 0 or a power of two <= 16; ctas_per_sm 0, 1 or 2";
+    return AFMM_BAD_ARG;
+  }
+  h->aca_cluster = cluster;
+  h->aca_ctas_per_sm = ctas_per_sm;
   return AFMM_OK;
 }
 

@@ -138,6 +138,13 @@ afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored);
  * arithmetic: half the bytes of the FP64 blocks.  AFMM_PREC_FP64 and
  * AFMM_PREC_FP64_BATCHED always apply the FP64 blocks. */
 afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on);
+/* Launch plan of the ACA kernel for every level, before afmm_assemble: CTAs
+ * per box (a thread-block cluster of 1, 2, 4, 8 or 16; 0 = the planner's
+ * choice) and CTAs per SM (1: full shared-memory budget, 2: half; 0 = the
+ * planner's choice).  Ranks, skeletons and L2P do not depend on it; only the
+ * setup time does (afmm_get_setup_phases reports the time and cluster size
+ * of every level).  No reference counterpart. */
+afmm_status afmm_set_aca_plan(afmm_handle* h, int cluster, int ctas_per_sm);
 /* 1 when the assembled handle keeps the fixed-point copy. */
 afmm_status afmm_get_m2l_fixed_point(afmm_handle* h, int* stored);
 

@@ -216,3 +216,23 @@ def test_host_pipeline_matches_device_pointers(precision, nrhs):
     a.matvec_device(dq.data_ptr(), dy.data_ptr(), nrhs, ld, precision)
     np.testing.assert_array_equal(Y[:, :32768], dy.cpu().numpy()[:, :32768])
     assert np.all(Y[:, 32768:] == 7.0)
+
+
+@pytest.mark.gpu
+def test_aca_plan_does_not_change_results():
+    """The ACA launch plan (CTAs per box and per SM) changes only the setup
+    time: ranks, skeletons, pivot columns and the FP64 matvec are identical."""
+    pts, q, _ = workloads.make("mixture4m", N=65536)
+    base = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
+    base.assemble()
+    y0 = base.computeMatVecProduct(q)
+    for cluster, per_sm in [(1, 1), (2, 2), (4, 2), (16, 1)]:
+        a = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
+        a.set_aca_plan(cluster, per_sm)
+        a.assemble()
+        assert a.setup_times()[f"assemble_aca_cluster_level{a.nLevels}_s"] == cluster
+        for lev in range(2, a.nLevels + 1):
+            np.testing.assert_array_equal(a.ranks(lev), base.ranks(lev))
+            np.testing.assert_array_equal(a.skeletons(lev), base.skeletons(lev))
+            np.testing.assert_array_equal(a.charge_points(lev), base.charge_points(lev))
+        np.testing.assert_array_equal(a.computeMatVecProduct(q), y0)
