@@ -1,4 +1,4 @@
-"""Generates tests/golden/uniform1m_log_tol10.npz by running the REFERENCE at
+"""Generates tests/golden/full_size/uniform1m_log_tol10.npz by running the REFERENCE at
 full size: N = 1,048,576 points uniform in [0,1]^2, log kernel, M = 64,
 TOL_POW = 10, one charge vector N(0,1) (afmm2d_b200.workloads "uniform1m").
 
@@ -31,7 +31,7 @@ from oracle_lib import RefLib  # noqa: E402
 
 from afmm2d_b200 import workloads  # noqa: E402
 
-OUT = os.path.join(HERE, "uniform1m_log_tol10.npz")
+OUT = os.path.join(HERE, "full_size", "uniform1m_log_tol10.npz")
 SAMPLE_ROWS = 32768
 SAMPLE_SEED = 0xC2
 

@@ -32,7 +32,7 @@ def test_uniform1m_full_size_vs_reference():
     against the reference run at full size (fixture from
     tests/golden/make_uniform1m_fixture.py); potentials within 10^-TOL of the
     reference's at 32,768 sampled rows."""
-    f = np.load(os.path.join(HERE, "golden", "uniform1m_log_tol10.npz"))
+    f = np.load(os.path.join(HERE, "golden", "full_size", "uniform1m_log_tol10.npz"))
     pts, q, p = workloads.make("uniform1m")
     a = A.AFMM(len(pts), p["M"], p["tol"], pts, kernel=p["kernel"])
     assert a.nLevels == int(f["L"]) == 7
