@@ -667,21 +667,43 @@ void finish_assemble(afmm_handle* h) {
 //   per level j = L..2: i64 boxes, i64 skeleton rows, i64 L2P entries;
 //     i32 ranks [boxes]; i32 skeleton ids [rows]; i32 pivot columns [rows];
 //     f64 L2P [entries] (per box n_b x r_b, column-major)
-//   u64 FNV-1a digest (64-bit words, then the tail bytes) of all bytes before
+//   u64 FNV-1a digest of all bytes before (64-bit words, then the tail bytes)
 constexpr char kSetupMagic[8] = {'A', 'F', 'M', 'M', '2', 'D', 'B', '\n'};
 constexpr uint32_t kSetupVersion = 1;
 
+// FNV-1a over the byte stream taken 8 bytes at a time (little-endian
+// words), the last partial word byte by byte; independent of how the stream
+// is split into add() calls.
 struct Fnv64 {
+  static constexpr uint64_t kPrime = 1099511628211ull;
   uint64_t h = 1469598103934665603ull;
+  unsigned char buf[8];
+  int nb = 0;
+  void word(const unsigned char* b) {
+    uint64_t x;
+    std::memcpy(&x, b, 8);
+    h = (h ^ x) * kPrime;
+  }
   void add(const void* p, size_t n) {
     const unsigned char* b = (const unsigned char*)p;
-    size_t w = n / 8;
-    for (size_t i = 0; i < w; ++i) {
-      uint64_t x;
-      std::memcpy(&x, b + 8 * i, 8);
-      h = (h ^ x) * 1099511628211ull;
+    while (n && nb) {
+      buf[nb++] = *b++;
+      --n;
+      if (nb == 8) {
+        word(buf);
+        nb = 0;
+      }
     }
-    for (size_t i = 8 * w; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    for (; n >= 8; n -= 8, b += 8) word(b);
+    while (n) {
+      buf[nb++] = *b++;
+      --n;
+    }
+  }
+  uint64_t digest() {
+    for (int i = 0; i < nb; ++i) h = (h ^ buf[i]) * kPrime;
+    nb = 0;
+    return h;
   }
 };
 
@@ -703,7 +725,7 @@ struct SetupWriter {
     put(v.data(), sizeof(T) * v.size());
   }
   void finish() {
-    const uint64_t d = dig.h;
+    const uint64_t d = dig.digest();
     if (std::fwrite(&d, 8, 1, f) != 1 || std::fclose(f) != 0) {
       f = nullptr;
       throw Error{AFMM_BAD_ARG, "write failed"};
@@ -740,7 +762,7 @@ struct SetupReader {
   void finish() {
     uint64_t d = 0;
     if (std::fread(&d, 8, 1, f) != 1) throw Error{AFMM_BAD_ARG, "setup file is truncated"};
-    if (d != dig.h) throw Error{AFMM_BAD_ARG, "setup file digest mismatch (corrupted file)"};
+    if (d != dig.digest()) throw Error{AFMM_BAD_ARG, "setup file digest mismatch (corrupted file)"};
     if (std::fgetc(f) != EOF) throw Error{AFMM_BAD_ARG, "setup file has trailing bytes"};
   }
 };
