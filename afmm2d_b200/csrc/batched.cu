@@ -527,6 +527,23 @@ struct Pass {
     return n;
   }
 
+  // Near field of the pass: the mixed 16-column form on tcgen05 tiles when
+  // tuned so (leaves of at most 64 points), else mma.sync tiles (TF32x3 in
+  // mixed precision, FP64 in FP64-batched passes), FMA for 4 columns.
+  static void p2p(const MatvecPlan& p, BatchState& bs, const NearView& nv, int fp64, cudaStream_t s) {
+    const KernelTable& kt = kernel_table(p.kp.id);
+    if (RC == 16 && !fp64 && p.tune.p2p_tc && nv.nmax <= 64 && bs.err_dev) {
+      kt.p2p_tc16(nv, p.kp, bs.qhl, bs.ys, p.L, bs.err_dev, s);
+    } else if (fp64) {
+      if (RC < 8) throw Error{AFMM_BAD_ARG, "FP64 batched passes take 8 or 16 columns"};
+      kt.p2p_dmma[RC == 16](nv, p.kp, bs.qs, bs.ys, s);
+    } else if (RC >= 8) {
+      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, bs.ys, s);
+    } else {
+      kt.p2p_b4(nv, p.kp, bs.qs32, bs.ys, s);
+    }
+  }
+
   static void run(const MatvecPlan& p, BatchState& bs, const NearView& nv, const double* q, int64_t ldq, double* y,
                   int64_t ldy, int ncols, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
     constexpr int RM = RC >= 8 ? RC : 8;
@@ -563,15 +580,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "p2p");
-    const KernelTable& kt = kernel_table(p.kp.id);
-    if (fp64) {
-      if (RC < 8) throw Error{AFMM_BAD_ARG, "FP64 batched passes take 8 or 16 columns"};
-      kt.p2p_dmma[RC == 16](nv, p.kp, bs.qs, bs.ys, s);
-    } else if (RC >= 8) {
-      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, bs.ys, s);
-    } else {
-      kt.p2p_b4(nv, p.kp, bs.qs32, bs.ys, s);
-    }
+    p2p(p, bs, nv, fp64, s);
     ++*launches;
     if (tm) tm->mark(s, "scatter");
     k_scatter_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
@@ -581,6 +590,17 @@ struct Pass {
 };
 
 }  // namespace
+
+int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int fp64, cudaStream_t s) {
+  NearView nv = p.near;
+  nv.anchor = ms.leaf_anchor;
+  nv.rel = ms.rel;
+  nv.span = ms.leaf_span;
+  if (rc == 16) Pass<16>::p2p(p, bs, nv, fp64, s);
+  else if (rc == 8) Pass<8>::p2p(p, bs, nv, fp64, s);
+  else Pass<4>::p2p(p, bs, nv, fp64, s);
+  return 1;
+}
 
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {
   if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
@@ -607,6 +627,9 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
     hq[t] = bs.qhat[t + 2];
     hy[t] = bs.yhat[t + 2];
   }
+  AFMM_CUDA(cudaHostAlloc((void**)&bs.err_host, sizeof(int), cudaHostAllocMapped));
+  *bs.err_host = 0;
+  AFMM_CUDA(cudaHostGetDevicePointer((void**)&bs.err_dev, bs.err_host, 0));
   bs.d_qhat_lv = arena.alloc<const double*>(kMaxLevels);
   bs.d_yhat_lv = arena.alloc<double*>(kMaxLevels);
   AFMM_CUDA(cudaMemcpyAsync((void*)bs.d_qhat_lv, hq.data(), sizeof(double*) * kMaxLevels, cudaMemcpyHostToDevice, s));

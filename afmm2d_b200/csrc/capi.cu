@@ -978,6 +978,16 @@ void host_pipeline(afmm_handle* h, const double* q, double* y, int nrhs, int64_t
 }
 
 
+// A kernel whose bounded device wait gave up leaves the batch error flag set
+// (host-mapped): report it once the stream is synchronised.
+void check_device_flag(afmm_handle* h) {
+  AFMM_CUDA(cudaStreamSynchronize(h->stream));
+  if (h->batch.err_host && *(volatile int*)h->batch.err_host) {
+    *(volatile int*)h->batch.err_host = 0;
+    throw Error{AFMM_TIMEOUT, "a bounded device wait gave up (tcgen05 near field); the results are incomplete"};
+  }
+}
+
 // ------------------------------------------------------------ autotuner
 // Times the tunable launch parameters (Tuning) on the handle's own problem
 // with CUDA events on its stream and keeps the fastest: the L2 prefetch
@@ -1022,7 +1032,7 @@ std::string tuning_key(afmm_handle* h) {
          "|ranks=" + std::to_string(h->counts[2]) + "|entries=" + std::to_string(h->counts[4]);
 }
 
-constexpr int kTuningValues = 6;
+constexpr int kTuningValues = 7;
 
 void tuning_to(const Tuning& t, int64_t* v) {
   v[0] = t.pf_fp64;
@@ -1031,13 +1041,15 @@ void tuning_to(const Tuning& t, int64_t* v) {
   v[3] = t.otf_batched;
   v[4] = t.host_pass_cols;
   v[5] = t.m2l_t16;
+  v[6] = t.p2p_tc;
 }
 
 Tuning tuning_from(const int64_t* v) {
   if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[2] > 0xffffffffll || v[3] < 0 ||
-      v[3] > 0xffffffffll || v[4] < 0 || v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16) || v[5] < 0 || v[5] > 1)
+      v[3] > 0xffffffffll || v[4] < 0 || v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16) || v[5] < 0 || v[5] > 1 ||
+      v[6] < 0 || v[6] > 1)
     throw Error{AFMM_BAD_ARG,
-                "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16; shape 0 or 1)"};
+                "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16; switches 0 or 1)"};
   Tuning t;
   t.pf_fp64 = (uint32_t)v[0];
   t.pf_batched = (uint32_t)v[1];
@@ -1045,6 +1057,7 @@ Tuning tuning_from(const int64_t* v) {
   t.otf_batched = (uint32_t)v[3];
   t.host_pass_cols = (int)v[4];
   t.m2l_t16 = (int)v[5];
+  t.p2p_tc = (int)v[6];
   return t;
 }
 
@@ -1059,9 +1072,9 @@ bool cache_lookup(const char* path, const std::string& key, Tuning& t) {
     const size_t sp = l.find(' ');
     if (sp == std::string::npos || l.compare(0, sp, key) != 0 || sp != key.size()) continue;
     long long v[kTuningValues];
-    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]) ==
-        kTuningValues) {
-      int64_t w[kTuningValues] = {v[0], v[1], v[2], v[3], v[4], v[5]};
+    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5],
+                    &v[6]) == kTuningValues) {
+      int64_t w[kTuningValues] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6]};
       try {
         t = tuning_from(w);
         hit = true;  // the last matching line wins
@@ -1079,8 +1092,8 @@ void cache_store(const char* path, const std::string& key, const Tuning& t) {
   if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot write the tuning cache ") + path};
   int64_t v[kTuningValues];
   tuning_to(t, v);
-  std::fprintf(f, "%s %lld %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1], (long long)v[2],
-               (long long)v[3], (long long)v[4], (long long)v[5]);
+  std::fprintf(f, "%s %lld %lld %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1],
+               (long long)v[2], (long long)v[3], (long long)v[4], (long long)v[5], (long long)v[6]);
   std::fclose(f);
 }
 
@@ -1173,6 +1186,21 @@ void do_autotune(afmm_handle* h, int what) {
       }
     }
     p.tune.m2l_t16 = arg;
+  }
+  if ((what & 16) && p.near.nmax <= 64) {
+    // near field of 16-column mixed passes: tcgen05 or mma.sync tiles
+    float best = 1e30f;
+    int arg = p.tune.p2p_tc;
+    for (int tc : {0, 1}) {
+      p.tune.p2p_tc = tc;
+      const float ms = time_ms(s, reps, [&] { p2p_batched(p, h->mixed, h->batch, R, 0, s); });
+      if (ms < best) {
+        best = ms;
+        arg = tc;
+      }
+    }
+    p.tune.p2p_tc = arg;
+    check_device_flag(h);
   }
   if (what & 4) {
     // pass width of host-pointer batched calls: 16 columns as one pass or as
@@ -1359,7 +1387,7 @@ afmm_status afmm_matvec(afmm_handle* h, const double* q, double* y, int nrhs, in
                     [&](const double* qd, double* yd, int nc) { compute(qd, h->N, yd, h->N, nc); });
     }
     if (tm) tm->mark(s, "end");
-    AFMM_CUDA(cudaStreamSynchronize(s));
+    check_device_flag(h);
     if (tm) tm->collect(h->stage_ms);
   });
 }
@@ -1666,8 +1694,9 @@ afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int*
   if (!h) return AFMM_BAD_ARG;
   return guard(h, [&] {
     if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_autotune before afmm_assemble"};
-    if (what < 0 || what > 15)
-      throw Error{AFMM_BAD_ARG, "what: bit 0 windows, bit 1 M2L forms, bit 2 host passes, bit 3 M2L tile shape"};
+    if (what < 0 || what > 31)
+      throw Error{AFMM_BAD_ARG,
+                  "what: bit 0 windows, bit 1 M2L forms, bit 2 host passes, bit 3 M2L tile shape, bit 4 near field"};
     const std::string key = tuning_key(h);
     Tuning t;
     if (cache_lookup(cache_path, key, t)) {
@@ -1676,7 +1705,7 @@ afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int*
       return;
     }
     if (from_cache) *from_cache = 0;
-    do_autotune(h, what == 0 ? 15 : what);
+    do_autotune(h, what == 0 ? 31 : what);
     cache_store(cache_path, key, h->plan.tune);
   });
 }

@@ -26,26 +26,6 @@ __device__ __forceinline__ void ring_offset(int m, int s, int& dx, int& dy) {
   else { dx = -m; dy = m - t; }
 }
 
-__device__ __forceinline__ void cell_of(long k, int j, int& ix, int& iy) {
-  int x = 0, y = 0;
-  for (int l = j - 1; l >= 0; --l) {
-    int d = (int)((k >> (2 * l)) & 3);
-    x = 2 * x + (d == 1 || d == 2);
-    y = 2 * y + (d >= 2);
-  }
-  ix = x;
-  iy = y;
-}
-
-__device__ __forceinline__ long box_of(int ix, int iy, int j) {
-  long k = 0;
-  for (int l = j - 1; l >= 0; --l) {
-    int bx = (ix >> l) & 1, by = (iy >> l) & 1;
-    k = 4 * k + (by ? (bx ? 2 : 3) : (bx ? 1 : 0));
-  }
-  return k;
-}
-
 // One thread per (box, slot of the 48 ring slots).
 __global__ void k_lists(int j, long nbox, int32_t* nbr, int32_t* il) {
   long t = (long)blockIdx.x * blockDim.x + threadIdx.x;

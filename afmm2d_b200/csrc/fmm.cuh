@@ -101,7 +101,31 @@ struct Tuning {
   uint32_t otf_batched = 0;         // bit t: level t + 2 evaluated on the fly in batched mixed passes
   int host_pass_cols = 0;           // columns per pass of host-pointer batched calls (0: automatic)
   int m2l_t16 = 0;                  // 16-column stored M2L on transposed m16n8k4 tiles (else 8x8x4 tiles)
+  int p2p_tc = 0;                   // 16-column mixed near field on tcgen05 tiles (else mma.sync tiles)
 };
+
+// Grid cell (ix, iy) of box k at level j: the base-4 digits of k read as
+// child offsets 0:(0,0) 1:(1,0) 2:(1,1) 3:(0,1) (src/AFMM2DTree.cpp:978-986),
+// and the inverse.
+__device__ __forceinline__ void cell_of(long k, int j, int& ix, int& iy) {
+  int x = 0, y = 0;
+  for (int l = j - 1; l >= 0; --l) {
+    int d = (int)((k >> (2 * l)) & 3);
+    x = 2 * x + (d == 1 || d == 2);
+    y = 2 * y + (d >= 2);
+  }
+  ix = x;
+  iy = y;
+}
+
+__device__ __forceinline__ long box_of(int ix, int iy, int j) {
+  long k = 0;
+  for (int l = j - 1; l >= 0; --l) {
+    int bx = (ix >> l) & 1, by = (iy >> l) & 1;
+    k = 4 * k + (by ? (bx ? 2 : 3) : (bx ? 1 : 0));
+  }
+  return k;
+}
 
 // L2 prefetch of a global range: cp.async.bulk.prefetch.L2 (16-byte aligned
 // start, size a multiple of 16).  Issued by one lane.

@@ -17,7 +17,7 @@ namespace afmm {
 
 // Bumped whenever KernelTable or an argument type of its launchers changes:
 // a table compiled against other headers is refused at registration.
-constexpr int kKernelTableAbi = 1;
+constexpr int kKernelTableAbi = 2;
 
 struct KernelTable {
   int abi = kKernelTableAbi;
@@ -39,6 +39,10 @@ struct KernelTable {
   void (*p2p_b4)(const NearView&, const KernelParams&, const float*, double*, cudaStream_t) = nullptr;
   void (*p2p_mma[2])(const NearView&, const KernelParams&, const uint2*, double*, cudaStream_t) = {nullptr, nullptr};
   void (*p2p_dmma[2])(const NearView&, const KernelParams&, const double*, double*, cudaStream_t) = {nullptr, nullptr};
+  // mixed near field of 16-column passes on tcgen05 tiles (p2p_tc_k.cuh);
+  // leaves of at most 64 points; sets *err on a bounded-wait timeout
+  void (*p2p_tc16)(const NearView&, const KernelParams&, const uint2*, double*, int L, int* err,
+                   cudaStream_t) = nullptr;
   // ACA and L2P of one level (aca_k.cuh)
   void (*aca_occupancy)(int clusters, size_t smem, int* active) = nullptr;
   void (*aca_run)(const AcaArgs&, int cluster, int clusters, size_t smem, cudaStream_t) = nullptr;

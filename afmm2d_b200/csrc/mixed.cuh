@@ -35,11 +35,19 @@ struct BatchState {
   double* yhat[kMaxLevels] = {nullptr};
   const double** d_qhat_lv = nullptr;  // device copies indexed by level - 2
   double** d_yhat_lv = nullptr;
+  int* err_host = nullptr;  // host-mapped flag set by a kernel whose bounded wait gave up
+  int* err_dev = nullptr;   // its device address
+  ~BatchState() {
+    if (err_host) cudaFreeHost(err_host);
+  }
 };
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s);
 // The M2L stage alone of a batched pass of rc columns (on the batch buffers'
 // current outgoing charges); returns the launches made.
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s);
+// The near-field stage alone of a batched pass of rc columns (on the batch
+// buffers' current charges); returns the launches made.
+int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int fp64, cudaStream_t s);
 // y = K q for nrhs > 1 columns in passes of 4, 8 or 16 right-hand sides.
 // fp64 = 1: FP64 throughout (FP64 near field on the tensor cores), passes of 8
 // or 16 columns.

@@ -9,6 +9,7 @@
 #include "fmm_k.cuh"
 #include "kernel_table.cuh"
 #include "mixed_k.cuh"
+#include "p2p_tc_k.cuh"
 #include "set_k.cuh"
 
 namespace afmm {
@@ -29,6 +30,7 @@ KernelTable make_kernel_table(const char* name) {
   t.p2p_mma[1] = &batched_detail::p2p_mma_batched<K, 16>;
   t.p2p_dmma[0] = &batched_detail::p2p_dmma_batched<K, 8>;
   t.p2p_dmma[1] = &batched_detail::p2p_dmma_batched<K, 16>;
+  t.p2p_tc16 = &p2p_tc_detail::p2p_tc_batched16<K>;
   t.aca_occupancy = &aca_detail::AcaLaunch<K>::occupancy;
   t.aca_run = &aca_detail::AcaLaunch<K>::run;
   t.l2p_run = &aca_detail::L2pRun<K>::run;

@@ -16,8 +16,8 @@ MIXED_TOL = 1e-6
 
 def test_autotune_rejects_null_handle():
     assert A.lib().afmm_autotune(None, 0, None, None) == 1
-    assert A.lib().afmm_get_tuning(None, None, 6) == 1
-    assert A.lib().afmm_set_tuning(None, None, 6) == 1
+    assert A.lib().afmm_get_tuning(None, None, 7) == 1
+    assert A.lib().afmm_set_tuning(None, None, 7) == 1
 
 
 @pytest.mark.gpu

@@ -236,3 +236,25 @@ def test_aca_plan_does_not_change_results():
             np.testing.assert_array_equal(a.skeletons(lev), base.skeletons(lev))
             np.testing.assert_array_equal(a.charge_points(lev), base.charge_points(lev))
         np.testing.assert_array_equal(a.computeMatVecProduct(q), y0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,tol", [("one_over_r", 6), ("log", 10), ("gaussian", 8), ("one_over_r_scaled", 8)])
+def test_tcgen05_near_field(kernel, tol):
+    """The 16-column mixed near field on tcgen05 tiles (sibling leaf pairs,
+    tensor-memory accumulators) against the FP64 path and against the
+    mma.sync form, every kernel; leaves of 64 points."""
+    pts, _, _ = workloads.make("mixture4m", N=65536)
+    a = A.AFMM(65536, 64, tol, pts, kernel=kernel)
+    a.assemble()
+    Q = np.random.default_rng(6).standard_normal((65536, 16))
+    a.set_tuning(p2p_tc=0)
+    Ym = a.computeMatVecProduct(Q, precision="mixed")
+    a.set_tuning(p2p_tc=1)
+    Yt = a.computeMatVecProduct(Q, precision="mixed")
+    Yt2 = a.computeMatVecProduct(Q, precision="mixed")
+    np.testing.assert_array_equal(Yt, Yt2)  # deterministic
+    for c in (0, 5, 15):
+        y64 = a.computeMatVecProduct(Q[:, c])
+        assert_rel(Yt[:, c], y64, MIXED_TOL)
+        assert_rel(Yt[:, c], Ym[:, c], MIXED_TOL)
