@@ -134,6 +134,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
       for (int cx = xl - 1; cx <= xl + 2; ++cx) {
         if (cx < 0 || cy < 0 || cx >= side || cy >= side) continue;
         const long u = box_of(cx, cy, L);
+        // empty leaves take no slot: union slots with chunks stay consecutive,
+        // which the alternation of the two accumulators relies on
+        if (nv.leaf_cnt[u] == 0) continue;
         const int ok = (abs(cx - x1) <= 1 ? 1 : 0) | (abs(cx - x2) <= 1 ? 2 : 0);
         const double2 au = nv.anchor[u];
         s_usrc[nu] = nv.leaf_start[u];
@@ -299,9 +302,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
     }
     issued = i;
   }
-  // drain: every committed MMA complete, then the last one or two leaves' sums
+  // drain: the commits of the last two chunks (not waited for in the loop)
+  // arrive, then the last one or two leaves' sums
   bool ok = true;
-  if (issued >= 0) ok = mbar_wait(smem_addr(&s_mbar[issued & 1]), (uint32_t)(issued >> 1) & 1u);
+  if (issued >= 1) ok = mbar_wait(smem_addr(&s_mbar[(issued - 1) & 1]), (uint32_t)((issued - 1) >> 1) & 1u);
+  if (issued >= 0) ok = mbar_wait(smem_addr(&s_mbar[issued & 1]), (uint32_t)(issued >> 1) & 1u) && ok;
   const bool fail = __syncthreads_or(!ok) || s_fail;
   fence_after();
   if (!fail && nch > 0) {
