@@ -323,7 +323,7 @@ def test_fp64_batched_matches_fp64_columns(kernel, nrhs):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("kernel", ["log", "one_over_r"])
+@pytest.mark.parametrize("kernel", ["log", "one_over_r", "one_over_r_scaled", "gaussian"])
 def test_m2l_on_the_fly_matches_stored_blocks(kernel):
     """Without stored M2L blocks every precision evaluates the entries on the
     fly in FP64; the results agree with the stored-block handle to FP64
