@@ -7,6 +7,7 @@
 // with afmm_register_kernel (AFMM_REGISTER_KERNEL).  Kernel-independent code
 // calls kernel_table(id).<stage>(...).
 #pragma once
+#include <stddef.h>
 #include <stdint.h>
 
 #include "aca.cuh"
@@ -17,10 +18,22 @@ namespace afmm {
 
 // Bumped whenever KernelTable or an argument type of its launchers changes:
 // a table compiled against other headers is refused at registration.
-constexpr int kKernelTableAbi = 2;
+constexpr int kKernelTableAbi = 3;
+
+// Fingerprint of the layouts of the launchers' argument types (sizes and a
+// few field offsets), recorded in every table where it is compiled: a table
+// whose launchers were compiled against headers with other layouts is
+// refused at registration even when the version above was not bumped.
+constexpr uint32_t layout_mix(uint32_t h, size_t v) { return (h ^ (uint32_t)v) * 16777619u; }
+constexpr uint32_t kArgLayout = layout_mix(
+    layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(2166136261u,
+    sizeof(LevelView)), offsetof(LevelView, m2l_q)), offsetof(LevelView, ptile_par)), sizeof(LevelSet)),
+    offsetof(LevelSet, src)), sizeof(NearView)), sizeof(KernelParams)), sizeof(AcaArgs)), sizeof(L2pArgs)),
+    sizeof(SetPlan));
 
 struct KernelTable {
   int abi = kKernelTableAbi;
+  uint32_t layout = kArgLayout;
   const char* name = nullptr;
   // M2L blocks K(R_b, R_c) of one level, setup arithmetic (fmm_k.cuh)
   void (*m2l_assemble)(const LevelView&, const KernelParams&, cudaStream_t) = nullptr;

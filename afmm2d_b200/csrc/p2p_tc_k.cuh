@@ -27,6 +27,7 @@
 #include <stdint.h>
 
 #include "batched_k.cuh"
+#include "tcgen05.cuh"
 
 namespace afmm {
 
@@ -48,63 +49,8 @@ constexpr uint32_t kCoreK = 128;                  // bytes between K-adjacent co
 constexpr uint32_t kCoreRows = (kChunk / 4) * 128;  // bytes between 8-row groups (1 KB)
 constexpr size_t kSmem = 2 * (size_t)kStage + (size_t)kUnionMax * kLeafMax * sizeof(float2) + 1024;
 constexpr uint32_t kTmemCols = 32;  // two 16-column FP32 accumulators
-constexpr long long kWaitCycles = 2000000000ll;  // ~1 s at 2 GHz
 
-// tcgen05 instruction descriptor: D FP32, A and B TF32, both K-major, N = 16, M = 128.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((16u >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-// Shared-memory matrix descriptor, K-major without swizzle: start address,
-// byte offset between K-adjacent core matrices (LBO) and between 8-row groups
-// (SBO), descriptor version 1.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t mbar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar) : "memory");
-}
-
-__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// Waits until the phase of parity `parity` of the mbarrier has completed;
-// false after ~1 s.
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (true) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P;\n\tmbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\tselp.b32 %0, 1, 0, P;\n\t}\n"
-        : "=r"(done)
-        : "r"(mbar), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (clock64() - t0 > kWaitCycles) return false;
-  }
-}
-
-// 16 consecutive FP32 accumulator columns of this thread's tensor-memory lane.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int n = 0; n < 16; ++n) v[n] = __uint_as_float(r[n]);
-}
+using namespace tc;
 
 template <class K>
 __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParams kp, const uint2* __restrict__ qhl,
@@ -156,16 +102,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
     s_nu = nu;
     s_nch = nch;
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[0])));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&s_mbar[1])));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_init(smem_addr(&s_mbar[0]), 1);
+    mbar_init(smem_addr(&s_mbar[1]), 1);
+    mbar_init_fence();
   }
   __syncwarp();
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&s_tmem)),
-                 "r"(kTmemCols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
+  if (warp == 0) tmem_alloc(&s_tmem, kTmemCols);
   fence_before();
   __syncthreads();
   fence_after();
@@ -282,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
                          (size_t)kg * kCoreK + (size_t)(n & 7) * 16;
       *reinterpret_cast<uint4*>(b) = make_uint4(w[0], w[1], w[2], w[3]);
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_async_smem();
     fence_before();
     __syncthreads();
     if (tid == 0) {
@@ -294,9 +236,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
         const uint32_t ko = (uint32_t)kk * 2 * kCoreK;  // 8 sources = two K-adjacent core matrices
         const uint64_t dah = smem_desc(aH + ko, kCoreK, kCoreRows), dal = smem_desc(aL + ko, kCoreK, kCoreRows);
         const uint64_t dbh = smem_desc(bH + ko, kCoreK, kCoreRows), dbl = smem_desc(bL + ko, kCoreK, kCoreRows);
-        mma_tf32(d, dah, dbh, (s_chfirst[i] && kk == 0) ? 0u : 1u);
-        mma_tf32(d, dah, dbl, 1u);
-        mma_tf32(d, dal, dbh, 1u);
+        mma_tf32(d, dah, dbh, kIdescTf32M128N16, (s_chfirst[i] && kk == 0) ? 0u : 1u);
+        mma_tf32(d, dah, dbl, kIdescTf32M128N16, 1u);
+        mma_tf32(d, dal, dbh, kIdescTf32M128N16, 1u);
       }
       mma_commit(smem_addr(&s_mbar[st]));
     }
@@ -329,7 +271,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+    tmem_dealloc(tmem, kTmemCols);
   }
 }
 
