@@ -21,7 +21,6 @@
 
 #include "batched_common.cuh"
 #include "kernel_table.cuh"
-#include "m2l_tc_k.cuh"
 #include "mixed.cuh"
 
 namespace afmm {
@@ -495,8 +494,7 @@ struct Pass {
   // FP64 otherwise; kernel-independent), or the entries on the fly (the
   // kernel's table)
   // (the levels of the tuning mask, in mixed precision, on the fly as well)
-  static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, int* err,
-                 cudaStream_t s) {
+  static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, cudaStream_t s) {
     constexpr int RM = RC >= 8 ? RC : 8;
     if (p.levels.row0[p.levels.nlev] == 0) return 0;  // every box of ACA rank 0: no far field
     const bool q32 = RC >= 8 && !fp64 && p.levels.lv[0].m2l_q != nullptr;
@@ -510,12 +508,7 @@ struct Pass {
       // stored blocks: one HBM read of the blocks serves all RC columns
       // (mixed precision: the 32-bit fixed-point copy, half the bytes)
       const long warps = st.cgrp0[st.nlev];
-      if (RC == 16 && q32 && p.tune.m2l_tc && err) {
-        // tcgen05 TF32 tiles, one CTA per row tile of a parent's children
-        allow_smem(m2l_tc_detail::k_m2l_tc, m2l_tc_detail::kSmem);
-        m2l_tc_detail::k_m2l_tc<<<(int)st.pt0[st.nlev], m2l_tc_detail::kThreads, m2l_tc_detail::kSmem, s>>>(st, qh, yh,
-                                                                                                          err);
-      } else if (RC == 16 && p.tune.m2l_t16) {
+      if (RC == 16 && p.tune.m2l_t16) {
         if (q32) k_m2l_stored_mma_t16<true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
         else k_m2l_stored_mma_t16<false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       } else if (q32) {
@@ -572,7 +565,7 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "m2l");
-    *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
+    *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];
@@ -610,9 +603,9 @@ int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int
 }
 
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {
-  if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
-  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
-  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
+  if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
 }
 
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s) {

@@ -34,6 +34,15 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "points*RHS/s per matvec at N=4M (mixture, 1/r, TOL 6), mixed batched vs FP64 GPU"
+
+
+def metric_name(workload, N, p, nrhs):
+    """The headline metric string for the default workload; for another one
+    the same quantity named by that workload's own sizes."""
+    if workload == "mixture4m" and N == 1 << 22 and nrhs == 16:
+        return METRIC
+    return (f"points*RHS/s per matvec at N={N} ({workload}, {p['kernel']}, TOL {p['tol']}), "
+            f"mixed batched ({nrhs} RHS) vs FP64 GPU")
 UNIT = "points*RHS/s"
 CPU_SAMPLE_N = 65536
 
@@ -54,7 +63,17 @@ def parse():
     ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
     ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
                     help="auto: run the library's autotuner during setup (default); default: built-in parameters")
+    ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
+                    help="tuning value applied after --tuning (repeatable; keys as AFMM.tuning(), e.g. p2p_tc=1)")
     return ap.parse_args()
+
+
+def tuning_overrides(args):
+    out = {}
+    for kv in args.set:
+        k, _, v = kv.partition("=")
+        out[k.strip()] = int(v, 0)
+    return out
 
 
 def rank_info():
@@ -166,7 +185,10 @@ def run_reference(args):
     if res is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libafmm2d_ref.so was not built"}))
         return
-    line = {"impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
+    from afmm2d_b200 import workloads
+    wp = workloads.WORKLOADS[args.workload]
+    metric = metric_name(args.workload, args.N or wp["N"], wp, getattr(args, "nrhs", 16))
+    line = {"impl": "reference", "metric": metric, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded)", "config": {"workload": args.workload, "N": n, "sample_of_N": 1 << 22},
@@ -250,9 +272,12 @@ def run_ours(args):
             a.set_profiling(False)
         return float(np.mean(ms))
 
+    overrides = tuning_overrides(args)
     if args.profile_once:
         if args.tuning == "auto":
             a.autotune()
+        if overrides:
+            a.set_tuning(**overrides)
         for name in paths:
             call(name)
         torch.cuda.synchronize()
@@ -270,6 +295,9 @@ def run_ours(args):
         t0 = time.perf_counter()
         tuning, _ = a.autotune()
         tune_s = time.perf_counter() - t0
+    if overrides:
+        a.set_tuning(**overrides)
+        tuning = a.tuning()
     t_dev = {}
     launches = {}
     stages = {}
@@ -356,7 +384,8 @@ def run_ours(args):
               "achieved": m2l_bytes / (s64["m2l"] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
               "algorithmic_bytes": m2l_bytes, "ms": s64["m2l"]}
     roof64["frac"] = roof64["achieved"] / hbm
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    line = {"metric": metric_name(args.workload, N, p, R), "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_dev["batched"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic (seeded)",
             "config": {"workload": args.workload, "N": N, "kernel": p["kernel"], "M": p["M"], "TOL_POW": p["tol"],
@@ -371,7 +400,7 @@ def run_ours(args):
             "rel_err_fp64_batched_vs_fp64_max_col": err_fp64b,
             "rel_err_fp64_vs_dense_16_leaves": err_dense,
             "setup_s": setup_s, "setup_process_warmup_s": warm_s, "setup": a.setup_times(), "stages_ms": stages,
-            "tuning": {"mode": args.tuning, "values": tuning, "autotune_s": tune_s,
+            "tuning": {"mode": args.tuning, "overrides": overrides, "values": tuning, "autotune_s": tune_s,
                        "default_ms_per_step": t_default},
             "counts": counts,
             "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
