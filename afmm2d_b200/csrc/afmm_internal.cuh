@@ -224,6 +224,9 @@ struct LevelDev {
   int32_t* nwgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
   int32_t* nwgrp_row = nullptr;  // node-row chunk -> first node row
   long nnwgroups = 0;
+  int32_t* ptile_par = nullptr;  // parent row tile (<= 128 rows of the parent's four children) -> parent
+  int32_t* ptile_row = nullptr;  // parent row tile -> first row in the children's concatenated rows
+  long nptiles = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)

@@ -21,6 +21,7 @@
 
 #include "batched_common.cuh"
 #include "kernel_table.cuh"
+#include "m2l_tc_k.cuh"
 #include "mixed.cuh"
 
 namespace afmm {
@@ -452,6 +453,135 @@ __global__ void __launch_bounds__(128) k_l2l_mma(LevelView v, const double* __re
 #undef AFMM_L2L
 }
 
+// Sweeps of the levels with few boxes, split along K: a CTA of kSplit warps
+// per chunk, warp w multiplying the w-th share of the chunk's K range (node
+// rows for M2M, the box's rank for L2L); the partial tiles meet in shared
+// memory and are added in warp order, so the result does not depend on
+// scheduling.  The upper levels have a handful of boxes whose K loops are
+// the longest of the tree: one warp per chunk would leave most SMs idle.
+constexpr int kSplit = 8;
+constexpr long kSplitBelow = 8192;  // levels of fewer chunks take the split kernels
+
+// Shared doubles of the partial tiles of a CTA (the largest chunk, 5 tiles):
+// [warp][tile][column tile][fragment][lane].
+template <int RC>
+constexpr int split_part_doubles() {
+  return kSplit * 5 * (RC / 8) * 2 * 32;
+}
+
+template <int RC, int NT, bool ADD>
+__device__ __forceinline__ void split_reduce_store(double (&c)[NT][RC / 8][2], double* __restrict__ part,
+                                                   double* __restrict__ out, const bool (&rowok)[NT], int trow,
+                                                   int tsrc, int w, int lane) {
+  constexpr int kTile = (RC / 8) * 2 * 32;
+#pragma unroll
+  for (int u = 0; u < NT; ++u)
+#pragma unroll
+    for (int t = 0; t < RC / 8; ++t) {
+      part[(w * NT + u) * kTile + (t * 2) * 32 + lane] = c[u][t][0];
+      part[(w * NT + u) * kTile + (t * 2 + 1) * 32 + lane] = c[u][t][1];
+    }
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int u = 0; u < NT; ++u)
+#pragma unroll
+      for (int t = 0; t < RC / 8; ++t) {
+        double s0 = part[u * kTile + (t * 2) * 32 + lane], s1 = part[u * kTile + (t * 2 + 1) * 32 + lane];
+        for (int x = 1; x < kSplit; ++x) {
+          s0 += part[(x * NT + u) * kTile + (t * 2) * 32 + lane];
+          s1 += part[(x * NT + u) * kTile + (t * 2 + 1) * 32 + lane];
+        }
+        c[u][t][0] = s0;
+        c[u][t][1] = s1;
+      }
+    store_tiles<RC, NT, ADD>(c, out, rowok, trow, tsrc);
+  }
+}
+
+// K share [kb, ke) of warp w out of K, in multiples of 4.
+__device__ __forceinline__ void split_range(int K, int w, int& kb, int& ke) {
+  const int per = ((K + 4 * kSplit - 1) / (4 * kSplit)) * 4;
+  kb = min(K, w * per);
+  ke = min(K, kb + per);
+}
+
+template <int RC, int NT>
+__device__ __forceinline__ void m2m_chunk_split(const LevelView& v, const double* __restrict__ src_all, int leaf,
+                                                double* __restrict__ qhat, int b, int r0, int w, int lane,
+                                                double* part) {
+  const int r = v.rank[b];
+  const int i0 = r0 - v.skel_off[b];
+  const int nrow = min(8 * NT, r - i0);
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const int trow = lane >> 2, tsrc = lane & 3;
+  bool rowok[NT];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  int kb, ke;
+  split_range(n, w, kb, ke);
+  const double* src = src_all + (long)(leaf ? v.leaf_start[b] : v.node_off[b]) * RC;
+  const double* A = v.l2p_rm + v.l2p_off[b] + (long)kb * r;
+  prefetch_l2_region(A, A + (long)(ke - kb) * r, lane);
+  prefetch_l2_region(src + (long)kb * RC, src + (long)ke * RC, lane);
+  double c[NT][RC / 8][2];
+  zero_tiles<RC, NT>(c);
+  mma_rows<RC, NT>(c, A + i0 + trow, r, ke - kb, src + (long)kb * RC, rowok, trow, tsrc);
+  split_reduce_store<RC, NT, false>(c, part, qhat + (long)r0 * RC, rowok, trow, tsrc, w, lane);
+}
+
+template <int RC, int NT>
+__device__ __forceinline__ void l2l_chunk_split(const LevelView& v, const double* __restrict__ yhat,
+                                                double* __restrict__ child_yhat, double* __restrict__ ys, int leaf,
+                                                int b, int g0, int w, int lane, double* part) {
+  const int r = v.rank[b];
+  const int n = v.node_off[b + 1] - v.node_off[b];
+  const int i0 = g0 - v.node_off[b];
+  const int nrow = min(8 * NT, n - i0);
+  const int trow = lane >> 2, tsrc = lane & 3;
+  bool rowok[NT];
+#pragma unroll
+  for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
+  int kb, ke;
+  split_range(r, w, kb, ke);
+  const double* A = v.l2p + v.l2p_off[b] + (long)kb * n;
+  prefetch_l2_region(A + i0, A + (long)(ke - kb) * n, lane);
+  double c[NT][RC / 8][2];
+  zero_tiles<RC, NT>(c);
+  mma_rows<RC, NT>(c, A + i0 + trow, n, ke - kb, yhat + (long)(v.skel_off[b] + kb) * RC, rowok, trow, tsrc);
+  if (leaf)
+    split_reduce_store<RC, NT, false>(c, part, ys + (long)(v.leaf_start[b] + i0) * RC, rowok, trow, tsrc, w, lane);
+  else
+    split_reduce_store<RC, NT, true>(c, part, child_yhat + (long)g0 * RC, rowok, trow, tsrc, w, lane);
+}
+
+template <int RC>
+__global__ void __launch_bounds__(32 * kSplit) k_m2m_mma_split(LevelView v, const double* __restrict__ src_all,
+                                                               int leaf, double* __restrict__ qhat) {
+  __shared__ double part[split_part_doubles<RC>()];
+  const long g = blockIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = v.cgrp_box[g];
+  const int r0 = v.cgrp_row[g];
+#define AFMM_M2M(NT) m2m_chunk_split<RC, NT>(v, src_all, leaf, qhat, b, r0, w, lane, part)
+  AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2M)
+#undef AFMM_M2M
+}
+
+template <int RC>
+__global__ void __launch_bounds__(32 * kSplit) k_l2l_mma_split(LevelView v, const double* __restrict__ yhat,
+                                                               double* __restrict__ child_yhat,
+                                                               double* __restrict__ ys, int leaf) {
+  __shared__ double part[split_part_doubles<RC>()];
+  const long g = blockIdx.x;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = v.ncgrp_box[g];
+  const int g0 = v.ncgrp_row[g];
+#define AFMM_L2L(NT) l2l_chunk_split<RC, NT>(v, yhat, child_yhat, ys, leaf, b, g0, w, lane, part)
+  AFMM_NT_SWITCH(chunk_tiles(v.ncgrp_row, g, v.nncgroups, v.node_off[b + 1]), AFMM_L2L)
+#undef AFMM_L2L
+}
+
 template <int RC, bool Q32>
 __global__ void __launch_bounds__(128) k_m2l_stored_mma(LevelSet ls, const double* const* __restrict__ qhat_lv,
                                                         double* const* __restrict__ yhat_lv) {
@@ -494,7 +624,8 @@ struct Pass {
   // FP64 otherwise; kernel-independent), or the entries on the fly (the
   // kernel's table)
   // (the levels of the tuning mask, in mixed precision, on the fly as well)
-  static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, cudaStream_t s) {
+  static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, int* err,
+                 cudaStream_t s) {
     constexpr int RM = RC >= 8 ? RC : 8;
     if (p.levels.row0[p.levels.nlev] == 0) return 0;  // every box of ACA rank 0: no far field
     const bool q32 = RC >= 8 && !fp64 && p.levels.lv[0].m2l_q != nullptr;
@@ -508,7 +639,12 @@ struct Pass {
       // stored blocks: one HBM read of the blocks serves all RC columns
       // (mixed precision: the 32-bit fixed-point copy, half the bytes)
       const long warps = st.cgrp0[st.nlev];
-      if (RC == 16 && p.tune.m2l_t16) {
+      if (RC == 16 && q32 && p.tune.m2l_tc && err) {
+        // tcgen05 TF32 tiles, one CTA per row tile of a parent's children
+        allow_smem(m2l_tc_detail::k_m2l_tc, m2l_tc_detail::kSmem);
+        m2l_tc_detail::k_m2l_tc<<<(int)st.pt0[st.nlev], m2l_tc_detail::kThreads, m2l_tc_detail::kSmem, s>>>(st, qh, yh,
+                                                                                                          err);
+      } else if (RC == 16 && p.tune.m2l_t16) {
         if (q32) k_m2l_stored_mma_t16<true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
         else k_m2l_stored_mma_t16<false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       } else if (q32) {
@@ -556,7 +692,10 @@ struct Pass {
     for (int j = p.L; j >= 2; --j) {
       const LevelView& v = p.lv[j];
       if (v.nrows == 0) continue;
-      if (RC >= 8)
+      if (RC >= 8 && v.ncgroups < kSplitBelow)
+        k_m2m_mma_split<RM><<<(int)v.ncgroups, 32 * kSplit, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
+                                                                    bs.qhat[j]);
+      else if (RC >= 8)
         k_m2m_mma<RM><<<nbk(v.ncgroups * 32, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
                                                                bs.qhat[j]);
       else
@@ -565,12 +704,15 @@ struct Pass {
       ++*launches;
     }
     if (tm) tm->mark(s, "m2l");
-    *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+    *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];
       if (v.nnodes == 0) continue;
-      if (RC >= 8)
+      if (RC >= 8 && v.nncgroups < kSplitBelow)
+        k_l2l_mma_split<RM><<<(int)v.nncgroups, 32 * kSplit, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
+                                                                     bs.ys, j == p.L);
+      else if (RC >= 8)
         k_l2l_mma<RM><<<nbk(v.nncgroups * 32, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
                                                                 bs.ys, j == p.L);
       else
@@ -603,9 +745,9 @@ int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int
 }
 
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {
-  if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
-  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
-  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, s);
+  if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
+  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
+  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
 }
 
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s) {

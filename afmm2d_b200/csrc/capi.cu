@@ -253,6 +253,9 @@ void build_plan(afmm_handle* h) {
     v.nwgrp_box = d.nwgrp_box;
     v.nwgrp_row = d.nwgrp_row;
     v.nnwgroups = d.nnwgroups;
+    v.ptile_par = d.ptile_par;
+    v.ptile_row = d.ptile_row;
+    v.nptiles = d.nptiles;
     v.m2l_q = d.m2l_q;
     v.m2l_dec = d.m2l_dec;
     v.nrows = d.total_rank;
@@ -263,6 +266,7 @@ void build_plan(afmm_handle* h) {
   p.levels.grp0[0] = 0;
   p.levels.cgrp0[0] = 0;
   p.levels.wgrp0[0] = 0;
+  p.levels.pt0[0] = 0;
   for (int j = 2; j <= h->L; ++j) {
     p.levels.lv[p.levels.nlev] = p.lv[j];
     p.levels.src[p.levels.nlev] = p.levels.nlev;
@@ -270,6 +274,7 @@ void build_plan(afmm_handle* h) {
     p.levels.grp0[p.levels.nlev + 1] = p.levels.grp0[p.levels.nlev] + p.lv[j].ngroups;
     p.levels.cgrp0[p.levels.nlev + 1] = p.levels.cgrp0[p.levels.nlev] + p.lv[j].ncgroups;
     p.levels.wgrp0[p.levels.nlev + 1] = p.levels.wgrp0[p.levels.nlev] + p.lv[j].nwgroups;
+    p.levels.pt0[p.levels.nlev + 1] = p.levels.pt0[p.levels.nlev] + p.lv[j].nptiles;
     ++p.levels.nlev;
   }
   for (int j = 0; j <= h->L; ++j) {
@@ -571,6 +576,28 @@ void finish_assemble(afmm_handle* h) {
         v.nnwgroups = (long)gb.size();
         v.nwgrp_box = db;
         v.nwgrp_row = dr;
+      }
+    }
+    {
+      // row tiles of the tcgen05 M2L: per parent box, the four children's
+      // skeleton rows concatenated and cut into ceil(R / 128) balanced tiles
+      std::vector<int32_t> tp, tr;
+      for (long P = 0; P < v.nbox / 4; ++P) {
+        int R = 0;
+        for (int c = 0; c < 4; ++c) R += v.h_rank[4 * P + c];
+        const int nt = (R + 127) / 128;
+        for (int t = 0; t < nt; ++t) {
+          tp.push_back((int32_t)P);
+          tr.push_back((int32_t)((long)t * R / nt));
+        }
+      }
+      v.nptiles = (long)tp.size();
+      v.ptile_par = h->arena.alloc<int32_t>(std::max<size_t>(tp.size(), 1));
+      v.ptile_row = h->arena.alloc<int32_t>(std::max<size_t>(tr.size(), 1));
+      if (!tp.empty()) {
+        AFMM_CUDA(cudaMemcpyAsync(v.ptile_par, tp.data(), sizeof(int32_t) * tp.size(), cudaMemcpyHostToDevice, s));
+        AFMM_CUDA(cudaMemcpyAsync(v.ptile_row, tr.data(), sizeof(int32_t) * tr.size(), cudaMemcpyHostToDevice, s));
+        AFMM_CUDA(cudaStreamSynchronize(s));
       }
     }
   }
@@ -1032,7 +1059,8 @@ std::string tuning_key(afmm_handle* h) {
          "|ranks=" + std::to_string(h->counts[2]) + "|entries=" + std::to_string(h->counts[4]);
 }
 
-constexpr int kTuningValues = 7;
+constexpr int kTuningValues = 8;
+constexpr int kTuningValuesMin = 7;  // callers written before the eighth value (m2l_tc) pass 7
 
 void tuning_to(const Tuning& t, int64_t* v) {
   v[0] = t.pf_fp64;
@@ -1042,12 +1070,13 @@ void tuning_to(const Tuning& t, int64_t* v) {
   v[4] = t.host_pass_cols;
   v[5] = t.m2l_t16;
   v[6] = t.p2p_tc;
+  v[7] = t.m2l_tc;
 }
 
 Tuning tuning_from(const int64_t* v) {
   if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[2] > 0xffffffffll || v[3] < 0 ||
       v[3] > 0xffffffffll || v[4] < 0 || v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16) || v[5] < 0 || v[5] > 1 ||
-      v[6] < 0 || v[6] > 1)
+      v[6] < 0 || v[6] > 1 || v[7] < 0 || v[7] > 1)
     throw Error{AFMM_BAD_ARG,
                 "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16; switches 0 or 1)"};
   Tuning t;
@@ -1058,6 +1087,7 @@ Tuning tuning_from(const int64_t* v) {
   t.host_pass_cols = (int)v[4];
   t.m2l_t16 = (int)v[5];
   t.p2p_tc = (int)v[6];
+  t.m2l_tc = (int)v[7];
   return t;
 }
 
@@ -1072,9 +1102,9 @@ bool cache_lookup(const char* path, const std::string& key, Tuning& t) {
     const size_t sp = l.find(' ');
     if (sp == std::string::npos || l.compare(0, sp, key) != 0 || sp != key.size()) continue;
     long long v[kTuningValues];
-    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5],
-                    &v[6]) == kTuningValues) {
-      int64_t w[kTuningValues] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6]};
+    if (std::sscanf(l.c_str() + sp, "%lld %lld %lld %lld %lld %lld %lld %lld", &v[0], &v[1], &v[2], &v[3], &v[4],
+                    &v[5], &v[6], &v[7]) == kTuningValues) {
+      int64_t w[kTuningValues] = {v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7]};
       try {
         t = tuning_from(w);
         hit = true;  // the last matching line wins
@@ -1092,8 +1122,8 @@ void cache_store(const char* path, const std::string& key, const Tuning& t) {
   if (!f) throw Error{AFMM_BAD_ARG, std::string("cannot write the tuning cache ") + path};
   int64_t v[kTuningValues];
   tuning_to(t, v);
-  std::fprintf(f, "%s %lld %lld %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1],
-               (long long)v[2], (long long)v[3], (long long)v[4], (long long)v[5], (long long)v[6]);
+  std::fprintf(f, "%s %lld %lld %lld %lld %lld %lld %lld %lld\n", key.c_str(), (long long)v[0], (long long)v[1],
+               (long long)v[2], (long long)v[3], (long long)v[4], (long long)v[5], (long long)v[6], (long long)v[7]);
   std::fclose(f);
 }
 
@@ -1174,7 +1204,10 @@ void do_autotune(afmm_handle* h, int what) {
     p.tune.otf_batched = ob;
   }
   if ((what & 8) && nlev > 0 && (fp64b || q32)) {
-    // tile shape of the 16-column stored M2L (the levels kept stored)
+    // tile shape of the 16-column stored M2L on FP64 tiles (the levels kept
+    // stored): 8x8x4 or transposed m16n8k4.  The tcgen05 TF32 form
+    // (m2l_tc) is not a candidate: its FP32 far field leaves the mixed
+    // tolerance on deep trees, so it stays an explicit choice.
     float best = 1e30f;
     int arg = p.tune.m2l_t16;
     for (int t16 : {0, 1}) {
@@ -1711,14 +1744,21 @@ afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int*
 }
 
 afmm_status afmm_get_tuning(afmm_handle* h, int64_t* v, int n) {
-  if (!h || !v || n < kTuningValues) return AFMM_BAD_ARG;
-  tuning_to(h->plan.tune, v);
+  if (!h || !v || n < kTuningValuesMin) return AFMM_BAD_ARG;
+  int64_t w[kTuningValues];
+  tuning_to(h->plan.tune, w);
+  std::copy(w, w + std::min(n, kTuningValues), v);
   return AFMM_OK;
 }
 
 afmm_status afmm_set_tuning(afmm_handle* h, const int64_t* v, int n) {
-  if (!h || !v || n < kTuningValues) return AFMM_BAD_ARG;
-  return guard(h, [&] { h->plan.tune = tuning_from(v); });
+  if (!h || !v || n < kTuningValuesMin) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    int64_t w[kTuningValues];
+    tuning_to(h->plan.tune, w);  // values the caller does not pass stay as they are
+    std::copy(v, v + std::min(n, kTuningValues), w);
+    h->plan.tune = tuning_from(w);
+  });
 }
 
 afmm_status afmm_get_device_alloc_count(int64_t* n) {

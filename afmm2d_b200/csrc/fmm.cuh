@@ -54,6 +54,9 @@ struct LevelView {
   const int32_t* nwgrp_box = nullptr;  // node-row chunk (<= 32 node rows of one box) -> box
   const int32_t* nwgrp_row = nullptr;  // node-row chunk -> first node row
   long nnwgroups = 0;
+  const int32_t* ptile_par = nullptr;  // parent row tile (<= 128 rows of 4 children) -> parent box
+  const int32_t* ptile_row = nullptr;  // parent row tile -> first row of the children's concatenated rows
+  long nptiles = 0;
   uint32_t* m2l_q = nullptr;          // 32-bit fixed-point blocks (null when not stored)
   double2* m2l_dec = nullptr;         // per (box, slot) decode constants
   long nrows = 0;                     // skeleton rows (sum of ranks)
@@ -69,6 +72,7 @@ struct LevelSet {
   long grp0[kMaxLevels + 1] = {0};   // prefix of row-group counts
   long cgrp0[kMaxLevels + 1] = {0};  // prefix of row-chunk counts
   long wgrp0[kMaxLevels + 1] = {0};  // prefix of warp row-chunk counts
+  long pt0[kMaxLevels + 1] = {0};    // prefix of parent row-tile counts
   int src[kMaxLevels] = {0};         // index of entry j among levels 2..L (per-level device tables)
   uint32_t pf_ahead = 12 * 1024;     // L2 prefetch window of the stored-block M2L kernels (bytes)
 };
@@ -87,6 +91,7 @@ inline LevelSet level_subset(const LevelSet& ls, uint32_t mask, bool keep) {
     o.grp0[n + 1] = o.grp0[n] + (ls.grp0[t + 1] - ls.grp0[t]);
     o.cgrp0[n + 1] = o.cgrp0[n] + (ls.cgrp0[t + 1] - ls.cgrp0[t]);
     o.wgrp0[n + 1] = o.wgrp0[n] + (ls.wgrp0[t + 1] - ls.wgrp0[t]);
+    o.pt0[n + 1] = o.pt0[n] + (ls.pt0[t + 1] - ls.pt0[t]);
     ++o.nlev;
   }
   return o;
@@ -102,6 +107,8 @@ struct Tuning {
   int host_pass_cols = 0;           // columns per pass of host-pointer batched calls (0: automatic)
   int m2l_t16 = 0;                  // 16-column stored M2L on transposed m16n8k4 tiles (else 8x8x4 tiles)
   int p2p_tc = 0;                   // 16-column mixed near field on tcgen05 tiles (else mma.sync tiles)
+  int m2l_tc = 0;  // 16-column mixed stored M2L on tcgen05 TF32 tiles (else FP64 tiles): an FP32 far
+                   // field, outside the mixed tolerance on deep trees; never chosen by the autotuner
 };
 
 // Grid cell (ix, iy) of box k at level j: the base-4 digits of k read as

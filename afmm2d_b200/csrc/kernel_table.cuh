@@ -26,9 +26,10 @@ constexpr int kKernelTableAbi = 3;
 // refused at registration even when the version above was not bumped.
 constexpr uint32_t layout_mix(uint32_t h, size_t v) { return (h ^ (uint32_t)v) * 16777619u; }
 constexpr uint32_t kArgLayout = layout_mix(
-    layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(2166136261u,
-    sizeof(LevelView)), offsetof(LevelView, m2l_q)), sizeof(LevelSet)), offsetof(LevelSet, src)),
-    sizeof(NearView)), sizeof(KernelParams)), sizeof(AcaArgs)), sizeof(L2pArgs)), sizeof(SetPlan));
+    layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(layout_mix(2166136261u,
+    sizeof(LevelView)), offsetof(LevelView, m2l_q)), offsetof(LevelView, ptile_par)), sizeof(LevelSet)),
+    offsetof(LevelSet, src)), sizeof(NearView)), sizeof(KernelParams)), sizeof(AcaArgs)), sizeof(L2pArgs)),
+    sizeof(SetPlan));
 
 struct KernelTable {
   int abi = kKernelTableAbi;

@@ -75,3 +75,10 @@ def test_set_tuning_values_and_forms():
     a.set_tuning(m2l_t16=1, otf_mixed=0, otf_batched=0)
     assert_rel(a.computeMatVecProduct(Q, precision="fp64_batched")[:, 1], y64, 1e-12)
     assert_rel(a.computeMatVecProduct(Q, precision="mixed")[:, 1], y64, MIXED_TOL)
+    # seven values (callers older than the eighth) leave the eighth as it is
+    a.set_tuning(m2l_tc=1)
+    v = np.array(list(a.tuning().values())[:7], np.int64)
+    assert A.lib().afmm_set_tuning(a._h, v.ctypes.data_as(ctypes.c_void_p), 7) == 0
+    assert a.tuning()["m2l_tc"] == 1
+    with pytest.raises(A.AFMMError):
+        a.set_tuning(m2l_tc=2)

@@ -258,3 +258,36 @@ def test_tcgen05_near_field(kernel, tol):
         y64 = a.computeMatVecProduct(Q[:, c])
         assert_rel(Yt[:, c], y64, MIXED_TOL)
         assert_rel(Yt[:, c], Ym[:, c], MIXED_TOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,tol,wl", [("one_over_r", 6, "mixture4m"), ("log", 10, "uniform1m"),
+                                           ("gaussian", 8, "mixture4m"), ("one_over_r_scaled", 8, "mixture4m")])
+def test_tcgen05_m2l(kernel, tol, wl):
+    """The 16-column mixed stored M2L on tcgen05 tiles (row tiles of a
+    parent's children, sources over the union of their lists, fixed-point
+    blocks decoded to FP32) against the FP64 path and against the FP64-tile
+    form; at TOL 10 the ranks exceed 32 (several stages per source box) and
+    a parent's children exceed 128 rows (several tiles per parent).  The
+    FP64-batched passes do not use it."""
+    pts, _, _ = workloads.make(wl, N=65536)
+    a = A.AFMM(65536, 64, tol, pts, kernel=kernel)
+    a.assemble()
+    Q = np.random.default_rng(7).standard_normal((65536, 16))
+    a.set_tuning(m2l_tc=0, otf_batched=0)
+    Ym = a.computeMatVecProduct(Q, precision="mixed")
+    Yb = a.computeMatVecProduct(Q, precision="fp64_batched")
+    a.set_tuning(m2l_tc=1)
+    assert a.tuning()["m2l_tc"] == 1
+    Yt = a.computeMatVecProduct(Q, precision="mixed")
+    np.testing.assert_array_equal(Yt, a.computeMatVecProduct(Q, precision="mixed"))  # deterministic
+    np.testing.assert_array_equal(a.computeMatVecProduct(Q, precision="fp64_batched"), Yb)
+    for c in (0, 5, 15):
+        y64 = a.computeMatVecProduct(Q[:, c])
+        assert_rel(Yt[:, c], y64, MIXED_TOL)
+        assert_rel(Yt[:, c], Ym[:, c], MIXED_TOL)
+    # with the near field on tcgen05 tiles as well
+    a.set_tuning(p2p_tc=1)
+    Ytt = a.computeMatVecProduct(Q, precision="mixed")
+    for c in (0, 15):
+        assert_rel(Ytt[:, c], a.computeMatVecProduct(Q[:, c]), MIXED_TOL)
