@@ -453,23 +453,31 @@ __global__ void __launch_bounds__(128) k_l2l_mma(LevelView v, const double* __re
 #undef AFMM_L2L
 }
 
-// Sweeps of the levels with few boxes, split along K: a CTA of kSplit warps
-// per chunk, warp w multiplying the w-th share of the chunk's K range (node
-// rows for M2M, the box's rank for L2L); the partial tiles meet in shared
-// memory and are added in warp order, so the result does not depend on
-// scheduling.  The upper levels have a handful of boxes whose K loops are
-// the longest of the tree: one warp per chunk would leave most SMs idle.
-constexpr int kSplit = 8;
-constexpr long kSplitBelow = 8192;  // levels of fewer chunks take the split kernels
+// Sweeps of the levels with few boxes, split along K: a CTA of S warps per
+// chunk, warp w multiplying the w-th share of the chunk's K range (node rows
+// for M2M, the box's rank for L2L); the partial tiles meet in shared memory
+// and are added in warp order, so the result does not depend on scheduling.
+// The upper levels have a handful of boxes whose K loops are the longest of
+// the tree: one warp per chunk would leave most SMs idle.
+
+// Warps per chunk for a level of `chunks` chunks (0: one warp per chunk, the
+// unsplit kernels).  M2M's K (the children's ranks) is several times L2L's
+// (the box's own rank), so M2M splits more levels.
+inline int split_warps(long chunks, bool m2m) {
+  if (chunks < 2048) return 8;
+  if (m2m && chunks < 8192) return 8;
+  if (m2m && chunks < 32768) return 2;
+  return 0;
+}
 
 // Shared doubles of the partial tiles of a CTA (the largest chunk, 5 tiles):
 // [warp][tile][column tile][fragment][lane].
-template <int RC>
+template <int RC, int S>
 constexpr int split_part_doubles() {
-  return kSplit * 5 * (RC / 8) * 2 * 32;
+  return S * 5 * (RC / 8) * 2 * 32;
 }
 
-template <int RC, int NT, bool ADD>
+template <int RC, int NT, int S, bool ADD>
 __device__ __forceinline__ void split_reduce_store(double (&c)[NT][RC / 8][2], double* __restrict__ part,
                                                    double* __restrict__ out, const bool (&rowok)[NT], int trow,
                                                    int tsrc, int w, int lane) {
@@ -488,7 +496,7 @@ __device__ __forceinline__ void split_reduce_store(double (&c)[NT][RC / 8][2], d
 #pragma unroll
       for (int t = 0; t < RC / 8; ++t) {
         double s0 = part[u * kTile + (t * 2) * 32 + lane], s1 = part[u * kTile + (t * 2 + 1) * 32 + lane];
-        for (int x = 1; x < kSplit; ++x) {
+        for (int x = 1; x < S; ++x) {
           s0 += part[(x * NT + u) * kTile + (t * 2) * 32 + lane];
           s1 += part[(x * NT + u) * kTile + (t * 2 + 1) * 32 + lane];
         }
@@ -499,14 +507,15 @@ __device__ __forceinline__ void split_reduce_store(double (&c)[NT][RC / 8][2], d
   }
 }
 
-// K share [kb, ke) of warp w out of K, in multiples of 4.
+// K share [kb, ke) of warp w of S out of K, in multiples of 4.
+template <int S>
 __device__ __forceinline__ void split_range(int K, int w, int& kb, int& ke) {
-  const int per = ((K + 4 * kSplit - 1) / (4 * kSplit)) * 4;
+  const int per = ((K + 4 * S - 1) / (4 * S)) * 4;
   kb = min(K, w * per);
   ke = min(K, kb + per);
 }
 
-template <int RC, int NT>
+template <int RC, int NT, int S>
 __device__ __forceinline__ void m2m_chunk_split(const LevelView& v, const double* __restrict__ src_all, int leaf,
                                                 double* __restrict__ qhat, int b, int r0, int w, int lane,
                                                 double* part) {
@@ -519,7 +528,7 @@ __device__ __forceinline__ void m2m_chunk_split(const LevelView& v, const double
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
   int kb, ke;
-  split_range(n, w, kb, ke);
+  split_range<S>(n, w, kb, ke);
   const double* src = src_all + (long)(leaf ? v.leaf_start[b] : v.node_off[b]) * RC;
   const double* A = v.l2p_rm + v.l2p_off[b] + (long)kb * r;
   prefetch_l2_region(A, A + (long)(ke - kb) * r, lane);
@@ -527,10 +536,10 @@ __device__ __forceinline__ void m2m_chunk_split(const LevelView& v, const double
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   mma_rows<RC, NT>(c, A + i0 + trow, r, ke - kb, src + (long)kb * RC, rowok, trow, tsrc);
-  split_reduce_store<RC, NT, false>(c, part, qhat + (long)r0 * RC, rowok, trow, tsrc, w, lane);
+  split_reduce_store<RC, NT, S, false>(c, part, qhat + (long)r0 * RC, rowok, trow, tsrc, w, lane);
 }
 
-template <int RC, int NT>
+template <int RC, int NT, int S>
 __device__ __forceinline__ void l2l_chunk_split(const LevelView& v, const double* __restrict__ yhat,
                                                 double* __restrict__ child_yhat, double* __restrict__ ys, int leaf,
                                                 int b, int g0, int w, int lane, double* part) {
@@ -543,41 +552,42 @@ __device__ __forceinline__ void l2l_chunk_split(const LevelView& v, const double
 #pragma unroll
   for (int u = 0; u < NT; ++u) rowok[u] = u * 8 + trow < nrow;
   int kb, ke;
-  split_range(r, w, kb, ke);
+  split_range<S>(r, w, kb, ke);
   const double* A = v.l2p + v.l2p_off[b] + (long)kb * n;
   prefetch_l2_region(A + i0, A + (long)(ke - kb) * n, lane);
   double c[NT][RC / 8][2];
   zero_tiles<RC, NT>(c);
   mma_rows<RC, NT>(c, A + i0 + trow, n, ke - kb, yhat + (long)(v.skel_off[b] + kb) * RC, rowok, trow, tsrc);
   if (leaf)
-    split_reduce_store<RC, NT, false>(c, part, ys + (long)(v.leaf_start[b] + i0) * RC, rowok, trow, tsrc, w, lane);
+    split_reduce_store<RC, NT, S, false>(c, part, ys + (long)(v.leaf_start[b] + i0) * RC, rowok, trow, tsrc, w,
+                                         lane);
   else
-    split_reduce_store<RC, NT, true>(c, part, child_yhat + (long)g0 * RC, rowok, trow, tsrc, w, lane);
+    split_reduce_store<RC, NT, S, true>(c, part, child_yhat + (long)g0 * RC, rowok, trow, tsrc, w, lane);
 }
 
-template <int RC>
-__global__ void __launch_bounds__(32 * kSplit) k_m2m_mma_split(LevelView v, const double* __restrict__ src_all,
-                                                               int leaf, double* __restrict__ qhat) {
-  __shared__ double part[split_part_doubles<RC>()];
+template <int RC, int S>
+__global__ void __launch_bounds__(32 * S) k_m2m_mma_split(LevelView v, const double* __restrict__ src_all, int leaf,
+                                                          double* __restrict__ qhat) {
+  __shared__ double part[split_part_doubles<RC, S>()];
   const long g = blockIdx.x;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = v.cgrp_box[g];
   const int r0 = v.cgrp_row[g];
-#define AFMM_M2M(NT) m2m_chunk_split<RC, NT>(v, src_all, leaf, qhat, b, r0, w, lane, part)
+#define AFMM_M2M(NT) m2m_chunk_split<RC, NT, S>(v, src_all, leaf, qhat, b, r0, w, lane, part)
   AFMM_NT_SWITCH(chunk_tiles(v.cgrp_row, g, v.ncgroups, v.skel_off[b] + v.rank[b]), AFMM_M2M)
 #undef AFMM_M2M
 }
 
-template <int RC>
-__global__ void __launch_bounds__(32 * kSplit) k_l2l_mma_split(LevelView v, const double* __restrict__ yhat,
-                                                               double* __restrict__ child_yhat,
-                                                               double* __restrict__ ys, int leaf) {
-  __shared__ double part[split_part_doubles<RC>()];
+template <int RC, int S>
+__global__ void __launch_bounds__(32 * S) k_l2l_mma_split(LevelView v, const double* __restrict__ yhat,
+                                                          double* __restrict__ child_yhat, double* __restrict__ ys,
+                                                          int leaf) {
+  __shared__ double part[split_part_doubles<RC, S>()];
   const long g = blockIdx.x;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int b = v.ncgrp_box[g];
   const int g0 = v.ncgrp_row[g];
-#define AFMM_L2L(NT) l2l_chunk_split<RC, NT>(v, yhat, child_yhat, ys, leaf, b, g0, w, lane, part)
+#define AFMM_L2L(NT) l2l_chunk_split<RC, NT, S>(v, yhat, child_yhat, ys, leaf, b, g0, w, lane, part)
   AFMM_NT_SWITCH(chunk_tiles(v.ncgrp_row, g, v.nncgroups, v.node_off[b + 1]), AFMM_L2L)
 #undef AFMM_L2L
 }
@@ -692,9 +702,12 @@ struct Pass {
     for (int j = p.L; j >= 2; --j) {
       const LevelView& v = p.lv[j];
       if (v.nrows == 0) continue;
-      if (RC >= 8 && v.ncgroups < kSplitBelow)
-        k_m2m_mma_split<RM><<<(int)v.ncgroups, 32 * kSplit, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
-                                                                    bs.qhat[j]);
+      const double* src = j == p.L ? bs.qs : bs.qhat[j + 1];
+      const int sw = RC >= 8 ? split_warps(v.ncgroups, true) : 0;
+      if (sw == 8)
+        k_m2m_mma_split<RM, 8><<<(int)v.ncgroups, 256, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
+      else if (sw == 2)
+        k_m2m_mma_split<RM, 2><<<(int)v.ncgroups, 64, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
       else if (RC >= 8)
         k_m2m_mma<RM><<<nbk(v.ncgroups * 32, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
                                                                bs.qhat[j]);
@@ -709,9 +722,9 @@ struct Pass {
     for (int j = 2; j <= p.L; ++j) {
       const LevelView& v = p.lv[j];
       if (v.nnodes == 0) continue;
-      if (RC >= 8 && v.nncgroups < kSplitBelow)
-        k_l2l_mma_split<RM><<<(int)v.nncgroups, 32 * kSplit, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
-                                                                     bs.ys, j == p.L);
+      if (RC >= 8 && split_warps(v.nncgroups, false) == 8)
+        k_l2l_mma_split<RM, 8><<<(int)v.nncgroups, 256, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
+                                                                bs.ys, j == p.L);
       else if (RC >= 8)
         k_l2l_mma<RM><<<nbk(v.nncgroups * 32, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
                                                                 bs.ys, j == p.L);
