@@ -61,6 +61,7 @@ _SIGS = {
     "afmm_get_stream": [_vp, _vp],
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
     "afmm_measure_fma_peaks": [_vp, _vp],
+    "afmm_measure_fp64_pipes": [_vp, _vp, _vp],
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_get_device_alloc_count": [_vp],
     "afmm_autotune": [_vp, _i, ctypes.c_char_p, _vp],
@@ -134,6 +135,13 @@ def measure_fma_peaks():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(lib().afmm_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def measure_fp64_pipes():
+    """(DMMA, DFMA, both together) FP64 throughput of the current device in TFLOP/s."""
+    a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _check(lib().afmm_measure_fp64_pipes(ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+    return a.value, b.value, c.value
 
 
 _plugins = []

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "aca.cuh"
@@ -207,6 +208,66 @@ double fma_peak_tflops() {
   cudaEventDestroy(e1);
   AFMM_LAUNCH_CHECK();
   return 2.0 * 8.0 * (double)blocks * threads * iters / (ms * 1e-3) / 1e12;
+}
+
+// FP64 tensor (mma.sync m8n8k4) and FP64 FMA throughput: MODE 0 issues 8
+// independent DMMA chains per warp, MODE 1 16 independent FMA chains per
+// thread, MODE 2 both in the same loop (whether the two share a datapath).
+template <int MODE>
+__global__ void k_fp64_pipes(int iters, double* out) {
+  double c[8][2], f[16];
+  const double a = 0.999999, b = 1e-7;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) c[i][0] = c[i][1] = threadIdx.x * 1e-9;
+#pragma unroll
+  for (int i = 0; i < 16; ++i) f[i] = threadIdx.x * 1e-9 + i;
+  for (int it = 0; it < iters; ++it) {
+    if (MODE != 1) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+        asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                     : "+d"(c[i][0]), "+d"(c[i][1])
+                     : "d"(a), "d"(b));
+    }
+    if (MODE != 0) {
+#pragma unroll
+      for (int i = 0; i < 16; ++i) f[i] = fma(f[i], a, b);
+    }
+  }
+  double s = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += c[i][0] + c[i][1];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) s += f[i];
+  if (s == -1.0) out[0] = s;  // never true; keeps the chains live
+}
+
+// TFLOP/s of k_fp64_pipes<MODE>: {DMMA part, FMA part}.
+template <int MODE>
+std::pair<double, double> fp64_pipes_tflops() {
+  int dev = 0, sms = 0;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  AFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  DevArena tmp;
+  double* out = tmp.alloc<double>(1);
+  const int blocks = sms * 4, threads = 256, iters = 4096;
+  k_fp64_pipes<MODE><<<blocks, threads>>>(16, out);  // warm-up
+  cudaEvent_t e0, e1;
+  AFMM_CUDA(cudaEventCreate(&e0));
+  AFMM_CUDA(cudaEventCreate(&e1));
+  AFMM_CUDA(cudaEventRecord(e0));
+  k_fp64_pipes<MODE><<<blocks, threads>>>(iters, out);
+  AFMM_CUDA(cudaEventRecord(e1));
+  AFMM_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  AFMM_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  AFMM_LAUNCH_CHECK();
+  const double warps = (double)blocks * threads / 32, s = ms * 1e-3 * 1e12;
+  const double mma = MODE != 1 ? warps * iters * 8 * 512.0 / s : 0.0;
+  const double fma_ = MODE != 0 ? (double)blocks * threads * iters * 16 * 2.0 / s : 0.0;
+  return {mma, fma_};
 }
 
 void build_plan(afmm_handle* h) {
@@ -1680,6 +1741,17 @@ afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops) {
     check_device();
     *fp64_tflops = fma_peak_tflops<double>();
     *fp32_tflops = fma_peak_tflops<float>();
+  });
+}
+
+afmm_status afmm_measure_fp64_pipes(double* dmma_tflops, double* dfma_tflops, double* both_tflops) {
+  if (!dmma_tflops || !dfma_tflops || !both_tflops) return AFMM_BAD_ARG;
+  return guard(nullptr, [&] {
+    check_device();
+    *dmma_tflops = fp64_pipes_tflops<0>().first;
+    *dfma_tflops = fp64_pipes_tflops<1>().second;
+    const auto b = fp64_pipes_tflops<2>();
+    *both_tflops = b.first + b.second;
   });
 }
 

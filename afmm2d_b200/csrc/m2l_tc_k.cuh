@@ -25,9 +25,9 @@
 //
 // Accuracy: the far field's sums cancel and the L2P weights amplify their
 // rounding, so FP32 products and sums are not enough on deep trees (measured
-// 3.1e-5 of the FP64 path on the 4,194,304-point mixture at TOL 6, 6.6e-6 on
-// 1,048,576 uniform points at TOL 10, against 4.6e-7 / 4.3e-8 for the FP64
-// tiles).  It is an explicit choice (tuning value m2l_tc), never the
+// 6.2e-5 of the FP64 path on the 4,194,304-point mixture at TOL 6, max over
+// 16 columns, and 6.6e-6 on 1,048,576 uniform points at TOL 10, against
+// 5.1e-7 / 4.3e-8 for the FP64 tiles).  It is an explicit choice (tuning value m2l_tc), never the
 // autotuner's.
 #pragma once
 #include <stdint.h>

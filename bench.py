@@ -340,6 +340,7 @@ def run_ours(args):
     value = world * N * R / (t_dev["batched"] * 1e-3)
     hbm, bf16, peak_kind = load_peaks()
     fp64_peak, fp32_peak = A.measure_fma_peaks()
+    dmma_peak, dfma_peak, both_peak = A.measure_fp64_pipes()
     # roofline of the dominant kernel of the headline (batched) path, its
     # duration averaged over the timed steps (stage events on the launching
     # stream); algorithmic bytes / flops per launch from the assembled counts
@@ -384,6 +385,17 @@ def run_ours(args):
               "achieved": m2l_bytes / (s64["m2l"] * 1e-3) / 1e9, "peak": hbm, "peak_kind": peak_kind,
               "algorithmic_bytes": m2l_bytes, "ms": s64["m2l"]}
     roof64["frac"] = roof64["achieved"] / hbm
+    # the batched stored M2L on FP64 tensor tiles is bound by the FP64
+    # datapath, not by HBM: its FP64 flops against the live DMMA peak
+    roof_dmma = None
+    if dom == "m2l" and not tuning.get("m2l_tc") and not tuning.get("otf_batched"):
+        fl = 2.0 * R * counts["m2l_entries"]
+        roof_dmma = {"bound": "tensor", "kernel": "k_m2l_stored_mma (FP64 mma.sync m8n8k4 tiles)", "unit": "TFLOP/s",
+                     "achieved": fl / (sb[dom] * 1e-3) / 1e12, "peak": dmma_peak,
+                     "peak_kind": "measured live (register-only m8n8k4 DMMA loop)", "algorithmic_flops": fl,
+                     "flop_definition": "2*nrhs flops per stored M2L entry (tile padding not counted)",
+                     "ms": sb[dom]}
+        roof_dmma["frac"] = roof_dmma["achieved"] / dmma_peak
     line = {"metric": metric_name(args.workload, N, p, R), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_dev["batched"], "higher_is_better": True, "scaling": "weak",
@@ -404,6 +416,8 @@ def run_ours(args):
                        "default_ms_per_step": t_default},
             "counts": counts,
             "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
+            "fp64_pipes_tflops": {"dmma": dmma_peak, "dfma": dfma_peak, "dmma_and_dfma_together": both_peak},
+            "roofline_dmma_m2l": roof_dmma,
             "clocks": clocks, "gpu_launches": int(launches["batched"]),
             "e2e": {"value": world * N * R / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N * R,
                     "d2h_bytes_per_step": 8 * N * R, "ms_per_step": t_e2e * 1e3, "nrhs": R}}

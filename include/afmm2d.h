@@ -222,6 +222,13 @@ afmm_status afmm_kernel_eval(int kernel_id, double a, double param, int64_t n, c
  * denominators of the compute-bound kernels.  Replaces no reference interface. */
 afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
 
+/* Measures this device's FP64 tensor throughput (mma.sync m8n8k4, the tiles
+ * of the batched sweeps, M2L and FP64 near field), its FP64 FMA throughput,
+ * and both issued together (TFLOP/s; a total no higher than either alone
+ * means one shared FP64 datapath): the denominators of the FP64-tile
+ * kernels.  Replaces no reference interface. */
+afmm_status afmm_measure_fp64_pipes(double* dmma_tflops, double* dfma_tflops, double* both_tflops);
+
 /* KD-tree permutation without any device allocation.  It has no counterpart
  * in the reference; it computes the same permutation as afmm_create /
  * afmm_get_permutation.  For callers that cannot allocate GPU memory: a

@@ -90,3 +90,20 @@ def test_no_device_is_reported_without_gpu():
 def test_python_mirror_raises_on_bad_config():
     with pytest.raises(A.AFMMError):
         A.AFMM(100, 64, 8, np.zeros((100, 2)))
+
+
+def test_measurement_helpers_reject_null_pointers():
+    lib = A.lib()
+    assert lib.afmm_measure_fma_peaks(None, None) == 1
+    assert lib.afmm_measure_fp64_pipes(None, None, None) == 1
+
+
+@pytest.mark.gpu
+def test_measurement_helpers_report_positive_peaks():
+    """The roofline denominators the bench measures live: FP64 / FP32 FMA,
+    FP64 tensor (DMMA) and both FP64 forms issued together."""
+    fp64, fp32 = A.measure_fma_peaks()
+    dmma, dfma, both = A.measure_fp64_pipes()
+    for v in (fp64, fp32, dmma, dfma, both):
+        assert np.isfinite(v) and v > 1.0
+    assert fp32 > fp64
