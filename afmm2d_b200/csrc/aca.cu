@@ -31,7 +31,8 @@
 
 namespace afmm {
 
-void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStream_t s, int64_t* launches) {
+void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, AcaScratch& scratch, cudaStream_t s,
+               int64_t* launches) {
   const int n1max = std::max(in.n1max, 1);
   const int n2max = std::max(in.n2max, 1);
   const int rcap = std::max(1, std::min(n1max, n2max));
@@ -122,15 +123,21 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     a.in_smem[t] = in_smem[t];
   }
   a.gslot = gslot;
-  DevArena scratch;
-  a.gscr = gslot > 0 ? scratch.alloc<unsigned char>((size_t)ncl * C * gslot) : nullptr;
-  a.vspill = vsp > 0 ? scratch.alloc<double>((size_t)ncl * C * vsp * chunk) : nullptr;
-  a.uspill = usp > 0 ? scratch.alloc<double>((size_t)ncl * C * usp * n1max) : nullptr;
+  const size_t n_gscr = gslot > 0 ? (size_t)ncl * C * gslot : 0;
+  const size_t n_vsp = vsp > 0 ? (size_t)ncl * C * vsp * chunk : 0;
+  const size_t n_usp = usp > 0 ? (size_t)ncl * C * usp * n1max : 0;
+  const size_t n_piv = (size_t)in.nbox * rcap;
+  DevScratch& w = scratch.work;
+  w.reserve(DevScratch::need({n_gscr, sizeof(double) * n_vsp, sizeof(double) * n_usp, sizeof(int32_t) * n_piv,
+                              sizeof(int32_t) * n_piv}));
+  a.gscr = n_gscr ? w.take<unsigned char>(n_gscr) : nullptr;
+  a.vspill = n_vsp ? w.take<double>(n_vsp) : nullptr;
+  a.uspill = n_usp ? w.take<double>(n_usp) : nullptr;
   out.rcap = rcap;
   out.rank = in.rank_out;
   a.rank_out = in.rank_out;
-  int32_t* rowpiv = scratch.alloc<int32_t>((size_t)in.nbox * rcap);
-  int32_t* colpiv = scratch.alloc<int32_t>((size_t)in.nbox * rcap);
+  int32_t* rowpiv = w.take<int32_t>(n_piv);
+  int32_t* colpiv = w.take<int32_t>(n_piv);
   a.rowpiv = rowpiv;
   a.colpiv = colpiv;
   const auto t0 = std::chrono::steady_clock::now();
@@ -195,7 +202,9 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStre
     p.gscratch = nullptr;
     if (global_factor) {
       grid = (int)std::min<long>(in.nbox, 148 * 8);
-      p.gscratch = scratch.alloc<double>((size_t)grid * rmax * rmax);
+      const size_t n_fac = (size_t)grid * rmax * rmax;
+      scratch.factors.reserve(DevScratch::need({sizeof(double) * n_fac}));
+      p.gscratch = scratch.factors.take<double>(n_fac);
     }
     kernel_table(in.kp.id).l2p_run(p, sm, global_factor, grid, s);
     *launches += 1;

@@ -95,8 +95,15 @@ struct AcaLevelOut {
   double aca_s = 0, l2p_s = 0;  // wall clock of the two phases
 };
 
+// Working memory of the ACA and L2P kernels, kept across the levels of one
+// assemble: spill slots and pivots, and the L2P's global factor slots.
+struct AcaScratch {
+  DevScratch work, factors;
+};
+
 // Runs the ACA and L2P kernels for one level; outputs are allocated in
-// `arena`.  Synchronises `s`.
-void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, cudaStream_t s, int64_t* launches);
+// `arena`, the kernels' working memory carved from `scratch`.  Synchronises `s`.
+void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, AcaScratch& scratch, cudaStream_t s,
+               int64_t* launches);
 
 }  // namespace afmm

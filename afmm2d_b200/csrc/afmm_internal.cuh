@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -192,6 +193,47 @@ struct DevArena {
   ~DevArena() {
     for (void* p : ptrs)
       if (p) cudaFree(p);
+  }
+};
+
+// One grow-only device buffer carved into aligned pieces, reused by a
+// sequence of launches (the ACA levels of one assemble): an allocation only
+// when a request exceeds the capacity, instead of a cudaMalloc / cudaFree
+// pair (a device-wide synchronisation) per level.
+struct DevScratch {
+  void* base = nullptr;
+  size_t cap = 0, used = 0;
+  // Makes the buffer at least `bytes` long (contents not kept) and restarts carving.
+  void reserve(size_t bytes) {
+    used = 0;
+    if (bytes <= cap) return;
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&base, bytes);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error{AFMM_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed"};
+    }
+    device_alloc_counter().fetch_add(1, std::memory_order_relaxed);
+    cap = bytes;
+  }
+  // The next n elements of T (256-byte aligned); reserve() must have made room.
+  template <class T>
+  T* take(size_t n) {
+    const size_t off = (used + 255) & ~(size_t)255;
+    if (off + n * sizeof(T) > cap) throw Error{AFMM_BAD_ARG, "scratch request beyond its reservation"};
+    used = off + n * sizeof(T);
+    return reinterpret_cast<T*>(static_cast<unsigned char*>(base) + off);
+  }
+  // Bytes that pieces of the given sizes need together.
+  static size_t need(std::initializer_list<size_t> sizes) {
+    size_t t = 0;
+    for (size_t s : sizes) t = ((t + 255) & ~(size_t)255) + s;
+    return t + 256;
+  }
+  ~DevScratch() {
+    if (base) cudaFree(base);
   }
 };
 

@@ -471,6 +471,7 @@ void do_assemble(afmm_handle* h) {
   cudaStream_t s = h->stream;
   const int L = h->L;
   double tol = std::pow(10, -1.0 * h->tol_pow);  // src/ACA.cpp:7
+  AcaScratch aca_scratch;  // working memory of every level's ACA and L2P, grown as needed
   for (int j = L; j >= 2; --j) {
     const double t_lv = now_s();
     LevelDev& v = h->lv[j];
@@ -512,7 +513,7 @@ void do_assemble(afmm_handle* h) {
     AcaLevelOut out;
     const double t_call = now_s();
     h->setup_phase[6].second += t_call - t_lv;
-    aca_level(in, out, h->arena, s, &h->launches);
+    aca_level(in, out, h->arena, aca_scratch, s, &h->launches);
     h->setup_phase[7].second += now_s() - t_call - out.aca_s - out.l2p_s;
     h->setup_phase[0].second += out.aca_s;
     h->setup_phase[1].second += out.l2p_s;
