@@ -351,7 +351,7 @@ class AFMM:
     def autotune(self, what=0, cache=None):
         """Times the launch parameters on this problem and keeps the fastest
         (what: bit 0 prefetch windows, bit 1 per-level M2L forms, bit 2 host
-        pass width, bit 3 M2L tile shape (FP64 tiles), bit 4 tcgen05 near field; 0 = all).  With `cache` (a file path) a stored result for
+        pass width, bit 3 M2L form (FP64 tiles or tcgen05 integer products), bit 4 tcgen05 near field; 0 = all).  With `cache` (a file path) a stored result for
         the same device and problem structure is reused.  Returns
         (tuning dict, from_cache)."""
         hit = ctypes.c_int()

@@ -269,6 +269,9 @@ struct LevelDev {
   int32_t* ptile_par = nullptr;  // parent row tile (<= 128 rows of the parent's four children) -> parent
   int32_t* ptile_row = nullptr;  // parent row tile -> first row in the children's concatenated rows
   long nptiles = 0;
+  int32_t* tile_box = nullptr;  // row tile (<= 128 skeleton rows of one box, multiple of 8) -> box
+  int32_t* tile_row = nullptr;  // row tile -> first row within the box
+  long ntiles = 0;
   int32_t* skel_off = nullptr;  // nbox+1 prefix over ranks
   int32_t* skel_ids = nullptr;  // skeleton (incoming check points), sorted-point ids
   int32_t* cpiv_ids = nullptr;  // pivot columns (incoming charge points)
@@ -284,6 +287,16 @@ struct LevelDev {
   // decodes it with one FMA (see decode_q32).
   uint32_t* m2l_q = nullptr;
   double2* m2l_dec = nullptr;
+  // The fixed-point blocks as byte planes for the integer tensor-core M2L
+  // (m2l_i8_k.cuh): box b's blocks start at m2l_s + m2l_s_off[b].  The
+  // charges' byte planes of a pass (qs8, per box from qs8_off[b] x 2 KB) with
+  // their per-column exponents and sums.
+  unsigned char* m2l_s = nullptr;
+  int64_t* m2l_s_off = nullptr;
+  unsigned char* qs8 = nullptr;
+  int32_t* qs8_off = nullptr;
+  int32_t* qs_exp = nullptr;
+  int64_t* qs_sum = nullptr;
   double* qhat = nullptr;       // outgoing charges, skel_off layout
   double* yhat = nullptr;       // incoming potentials, skel_off layout
   // host copies

@@ -21,6 +21,7 @@
 
 #include "batched_common.cuh"
 #include "kernel_table.cuh"
+#include "m2l_i8_k.cuh"
 #include "m2l_tc_k.cuh"
 #include "mixed.cuh"
 
@@ -628,6 +629,14 @@ __global__ void __launch_bounds__(128) k_m2l_stored_mma_t16(LevelSet ls, const d
 
 inline int nbk(long n, int t) { return (int)((n + t - 1) / t); }
 
+// Streaming multiprocessors of the current device.
+inline int sm_count() {
+  int dev = 0, n = 0;
+  AFMM_CUDA(cudaGetDevice(&dev));
+  AFMM_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+  return n;
+}
+
 template <int RC>
 struct Pass {
   // M2L of every level: the stored blocks (fixed point in mixed precision,
@@ -649,7 +658,19 @@ struct Pass {
       // stored blocks: one HBM read of the blocks serves all RC columns
       // (mixed precision: the 32-bit fixed-point copy, half the bytes)
       const long warps = st.cgrp0[st.nlev];
-      if (RC == 16 && q32 && p.tune.m2l_tc && err) {
+      if (RC == 16 && q32 && p.tune.m2l_tc == 2 && err && st.lv[0].m2l_s != nullptr) {
+        // exact integer products on tcgen05: the charges' byte planes of this
+        // pass, then persistent CTAs over the 128-row tiles
+        using namespace m2l_i8_detail;
+        const long nb = st.b0[st.nlev];
+        k_qhat_slice<<<nbk(nb * 32, 128), 128, 0, s>>>(st, qh);
+        AFMM_LAUNCH_CHECK();
+        ++n;
+        allow_smem(k_m2l_i8, kSmem);
+        const long items = st.t0[st.nlev];
+        const int grid = (int)std::min<long>(items, 2L * sm_count());
+        if (grid > 0) k_m2l_i8<<<grid, kThreads, kSmem, s>>>(st, yh, err);
+      } else if (RC == 16 && q32 && p.tune.m2l_tc == 1 && err) {
         // tcgen05 TF32 tiles, one CTA per row tile of a parent's children
         allow_smem(m2l_tc_detail::k_m2l_tc, m2l_tc_detail::kSmem);
         m2l_tc_detail::k_m2l_tc<<<(int)st.pt0[st.nlev], m2l_tc_detail::kThreads, m2l_tc_detail::kSmem, s>>>(st, qh, yh,
@@ -755,6 +776,12 @@ int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int
   else if (rc == 8) Pass<8>::p2p(p, bs, nv, fp64, s);
   else Pass<4>::p2p(p, bs, nv, fp64, s);
   return 1;
+}
+
+void m2l_slice(const LevelView& v, cudaStream_t s) {
+  if (v.nbox == 0) return;
+  m2l_i8_detail::k_m2l_slice<<<(int)v.nbox, 256, 0, s>>>(v);
+  AFMM_LAUNCH_CHECK();
 }
 
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {

@@ -72,6 +72,7 @@ struct afmm_handle {
   int m2l_q_mode = 1;            // also keep a 32-bit fixed-point copy for the mixed paths
   int aca_cluster = 0, aca_ctas_per_sm = 0;  // ACA planner overrides (0: automatic)
   bool m2l_q_stored = false;
+  bool m2l_s_stored = false;     // byte-plane copy for the integer tensor-core M2L
   KernelParams kp{};
   cudaStream_t stream = nullptr;
   DevArena arena;
@@ -317,6 +318,15 @@ void build_plan(afmm_handle* h) {
     v.ptile_par = d.ptile_par;
     v.ptile_row = d.ptile_row;
     v.nptiles = d.nptiles;
+    v.tile_box = d.tile_box;
+    v.tile_row = d.tile_row;
+    v.ntiles = d.ntiles;
+    v.m2l_s = d.m2l_s;
+    v.m2l_s_off = d.m2l_s_off;
+    v.qs8 = d.qs8;
+    v.qs8_off = d.qs8_off;
+    v.qs_exp = d.qs_exp;
+    v.qs_sum = d.qs_sum;
     v.m2l_q = d.m2l_q;
     v.m2l_dec = d.m2l_dec;
     v.nrows = d.total_rank;
@@ -328,6 +338,8 @@ void build_plan(afmm_handle* h) {
   p.levels.cgrp0[0] = 0;
   p.levels.wgrp0[0] = 0;
   p.levels.pt0[0] = 0;
+  p.levels.t0[0] = 0;
+  p.levels.b0[0] = 0;
   for (int j = 2; j <= h->L; ++j) {
     p.levels.lv[p.levels.nlev] = p.lv[j];
     p.levels.src[p.levels.nlev] = p.levels.nlev;
@@ -336,6 +348,8 @@ void build_plan(afmm_handle* h) {
     p.levels.cgrp0[p.levels.nlev + 1] = p.levels.cgrp0[p.levels.nlev] + p.lv[j].ncgroups;
     p.levels.wgrp0[p.levels.nlev + 1] = p.levels.wgrp0[p.levels.nlev] + p.lv[j].nwgroups;
     p.levels.pt0[p.levels.nlev + 1] = p.levels.pt0[p.levels.nlev] + p.lv[j].nptiles;
+    p.levels.t0[p.levels.nlev + 1] = p.levels.t0[p.levels.nlev] + p.lv[j].ntiles;
+    p.levels.b0[p.levels.nlev + 1] = p.levels.b0[p.levels.nlev] + p.lv[j].nbox;
     ++p.levels.nlev;
   }
   for (int j = 0; j <= h->L; ++j) {
@@ -539,6 +553,62 @@ void do_assemble(afmm_handle* h) {
 // skel_xy, l2p and their host copies of every level 2..L): M2L block sizes
 // and storage, row tables, M2L blocks (FP64 and fixed point), the row-major
 // L2P copy, the mixed-precision set-up and the structure counts.
+// Byte planes of the fixed-point blocks (integer tensor-core M2L) and the
+// per-pass buffers of the charges' planes, when they fit beside the rest.
+// Per box the blocks follow in slot order, block (b, slot) taking
+// ceil(r_c / 16) x 4 x ceil(r_b / 8) x 128 bytes; per box the charges take
+// ceil(r / 32) x 2 KB.
+void build_byte_planes(afmm_handle* h, double l2p_total, double rows_total) {
+  cudaStream_t s = h->stream;
+  const int L = h->L;
+  std::vector<std::vector<int64_t>> soff(L + 1), qoff(L + 1);
+  double need = 0.0;
+  for (int j = 2; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
+    const std::vector<int32_t>& il = h->h_il[j];
+    soff[j].assign(v.nbox + 1, 0);
+    qoff[j].assign(v.nbox + 1, 0);
+    for (long b = 0; b < v.nbox; ++b) {
+      const int rb = v.h_rank[b];
+      int64_t bytes = 0;
+      for (int t = 0; t < 40 && rb > 0; ++t) {
+        const int c = il[b * 40 + t];
+        const int rc = c >= 0 ? v.h_rank[c] : 0;
+        if (rc > 0) bytes += (int64_t)((rc + 15) / 16) * 4 * ((rb + 7) / 8) * 128;
+      }
+      soff[j][b + 1] = soff[j][b] + bytes;
+      qoff[j][b + 1] = qoff[j][b] + (rb + 31) / 32;
+    }
+    need += (double)soff[j][v.nbox] + 2048.0 * (double)qoff[j][v.nbox] + 12.0 * 16 * (double)v.nbox;
+  }
+  size_t free_b = 0, total_b = 0;
+  AFMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  const double reserve = 8.0 * l2p_total + (double)h->N * (16 * 8 * 4 + 64) + rows_total * 16 * 8 * 2 + 2e9;
+  if (need > (double)free_b - reserve) return;
+  const double t_ph = now_s();
+  for (int j = 2; j <= L; ++j) {
+    LevelDev& v = h->lv[j];
+    v.m2l_s_off = h->arena.alloc<int64_t>(v.nbox + 1);
+    v.m2l_s = h->arena.alloc<unsigned char>((size_t)soff[j][v.nbox] + 256);
+    std::vector<int32_t> q32(qoff[j].begin(), qoff[j].end());
+    v.qs8_off = h->arena.alloc<int32_t>(v.nbox + 1);
+    v.qs8 = h->arena.alloc<unsigned char>((size_t)qoff[j][v.nbox] * 2048 + 256);
+    v.qs_exp = h->arena.alloc<int32_t>((size_t)v.nbox * 16);
+    v.qs_sum = h->arena.alloc<int64_t>((size_t)v.nbox * 16);
+    AFMM_CUDA(cudaMemcpyAsync(v.m2l_s_off, soff[j].data(), sizeof(int64_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+    AFMM_CUDA(cudaMemcpyAsync(v.qs8_off, q32.data(), sizeof(int32_t) * (v.nbox + 1), cudaMemcpyHostToDevice, s));
+    AFMM_CUDA(cudaStreamSynchronize(s));
+  }
+  build_plan(h);
+  for (int j = 2; j <= L; ++j) {
+    m2l_slice(h->plan.lv[j], s);
+    ++h->launches;
+  }
+  AFMM_CUDA(cudaStreamSynchronize(s));
+  h->m2l_s_stored = true;
+  h->setup_phase[2].second += now_s() - t_ph;
+}
+
 void finish_assemble(afmm_handle* h) {
   cudaStream_t s = h->stream;
   const int L = h->L;
@@ -595,9 +665,10 @@ void finish_assemble(afmm_handle* h) {
     // ceil(n / kChunkRows) chunks of equal size rounded up to 8 rows; and
     // balanced chunks of at most 32 skeleton rows (a warp's lanes, the
     // one-column M2L)
-    // (and the same of at most 32 node rows, the one-column L2L)
-    for (int kind = 0; kind < 5; ++kind) {
-      const int span = kind == 0 ? 8 : (kind >= 3 ? 32 : kChunkRows);
+    // (and the same of at most 32 node rows, the one-column L2L); and tiles
+    // of 128 skeleton rows (the last shorter: the integer tensor-core M2L)
+    for (int kind = 0; kind < 6; ++kind) {
+      const int span = kind == 0 ? 8 : (kind == 5 ? 128 : (kind >= 3 ? 32 : kChunkRows));
       const bool nodes = kind == 2 || kind == 4;
       std::vector<int32_t> gb, gr;
       for (long b = 0; b < v.nbox; ++b) {
@@ -606,9 +677,10 @@ void finish_assemble(afmm_handle* h) {
         const int nch = (rows + span - 1) / span;
         int step = nch > 0 ? (rows + nch - 1) / nch : 0;
         if (kind == 1 || kind == 2) step = (step + 7) / 8 * 8;
+        if (kind == 5) step = span;  // whole 128-row tiles, the last one shorter
         for (int i = 0; i < rows; i += (kind == 0 ? 8 : step)) {
           gb.push_back((int32_t)b);
-          gr.push_back(first + i);
+          gr.push_back(kind == 5 ? i : first + i);  // 128-row tiles: the row within the box
         }
       }
       int32_t* db = h->arena.alloc<int32_t>(gb.size());
@@ -634,6 +706,10 @@ void finish_assemble(afmm_handle* h) {
         v.nwgroups = (long)gb.size();
         v.wgrp_box = db;
         v.wgrp_row = dr;
+      } else if (kind == 5) {
+        v.ntiles = (long)gb.size();
+        v.tile_box = db;
+        v.tile_row = dr;
       } else {
         v.nnwgroups = (long)gb.size();
         v.nwgrp_box = db;
@@ -703,6 +779,7 @@ void finish_assemble(afmm_handle* h) {
       AFMM_CUDA(cudaStreamSynchronize(s));
       h->m2l_q_stored = true;
       h->setup_phase[2].second += now_s() - t_ph;
+      build_byte_planes(h, l2p_total, rows_total);
     }
   }
   t_ph = now_s();
@@ -1138,7 +1215,7 @@ void tuning_to(const Tuning& t, int64_t* v) {
 Tuning tuning_from(const int64_t* v) {
   if (v[0] < 0 || v[0] > (1 << 20) || v[1] < 0 || v[1] > (1 << 20) || v[2] < 0 || v[2] > 0xffffffffll || v[3] < 0 ||
       v[3] > 0xffffffffll || v[4] < 0 || v[4] > kBatchMax || (v[0] % 16) || (v[1] % 16) || v[5] < 0 || v[5] > 1 ||
-      v[6] < 0 || v[6] > 1 || v[7] < 0 || v[7] > 1)
+      v[6] < 0 || v[6] > 1 || v[7] < 0 || v[7] > 2)
     throw Error{AFMM_BAD_ARG,
                 "tuning values out of range (windows: multiples of 16 up to 1 MiB; pass width <= 16; switches 0 or 1)"};
   Tuning t;
@@ -1266,21 +1343,26 @@ void do_autotune(afmm_handle* h, int what) {
     p.tune.otf_batched = ob;
   }
   if ((what & 8) && nlev > 0 && (fp64b || q32)) {
-    // tile shape of the 16-column stored M2L on FP64 tiles (the levels kept
-    // stored): 8x8x4 or transposed m16n8k4.  The tcgen05 TF32 form
-    // (m2l_tc) is not a candidate: its FP32 far field leaves the mixed
-    // tolerance on deep trees, so it stays an explicit choice.
+    // form of the 16-column stored M2L (the levels kept stored): FP64 tiles
+    // 8x8x4 or transposed m16n8k4, or exact integer products on tcgen05 from
+    // the byte planes (m2l_tc = 2).  The tcgen05 TF32 form (m2l_tc = 1) is not
+    // a candidate: its FP32 far field leaves the mixed tolerance on deep
+    // trees, so it stays an explicit choice.
     float best = 1e30f;
-    int arg = p.tune.m2l_t16;
-    for (int t16 : {0, 1}) {
-      p.tune.m2l_t16 = t16;
+    int arg = p.tune.m2l_t16, arg_tc = p.tune.m2l_tc == 1 ? 0 : p.tune.m2l_tc;
+    for (int form = 0; form < (h->m2l_s_stored ? 3 : 2); ++form) {
+      p.tune.m2l_t16 = form == 1;
+      p.tune.m2l_tc = form == 2 ? 2 : 0;
       const float ms = time_ms(s, reps, [&] { m2l_batched(p, h->batch, R, 0, s); });
       if (ms < best) {
         best = ms;
-        arg = t16;
+        arg = p.tune.m2l_t16;
+        arg_tc = p.tune.m2l_tc;
       }
     }
     p.tune.m2l_t16 = arg;
+    p.tune.m2l_tc = arg_tc;
+    check_device_flag(h);
   }
   if ((what & 16) && p.near.nmax <= 64) {
     // near field of 16-column mixed passes: tcgen05 or mma.sync tiles

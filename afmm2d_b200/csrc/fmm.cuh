@@ -57,6 +57,15 @@ struct LevelView {
   const int32_t* ptile_par = nullptr;  // parent row tile (<= 128 rows of 4 children) -> parent box
   const int32_t* ptile_row = nullptr;  // parent row tile -> first row of the children's concatenated rows
   long nptiles = 0;
+  const int32_t* tile_box = nullptr;  // row tile (<= 128 skeleton rows of one box) -> box
+  const int32_t* tile_row = nullptr;  // row tile -> first row within the box (a multiple of 8)
+  long ntiles = 0;
+  unsigned char* m2l_s = nullptr;      // byte-plane blocks (m2l_i8_k.cuh; null when not stored)
+  const int64_t* m2l_s_off = nullptr;
+  unsigned char* qs8 = nullptr;        // charges' byte planes of the current pass
+  const int32_t* qs8_off = nullptr;
+  int32_t* qs_exp = nullptr;
+  int64_t* qs_sum = nullptr;
   uint32_t* m2l_q = nullptr;          // 32-bit fixed-point blocks (null when not stored)
   double2* m2l_dec = nullptr;         // per (box, slot) decode constants
   long nrows = 0;                     // skeleton rows (sum of ranks)
@@ -73,6 +82,8 @@ struct LevelSet {
   long cgrp0[kMaxLevels + 1] = {0};  // prefix of row-chunk counts
   long wgrp0[kMaxLevels + 1] = {0};  // prefix of warp row-chunk counts
   long pt0[kMaxLevels + 1] = {0};    // prefix of parent row-tile counts
+  long t0[kMaxLevels + 1] = {0};     // prefix of 128-row tile counts
+  long b0[kMaxLevels + 1] = {0};     // prefix of box counts
   int src[kMaxLevels] = {0};         // index of entry j among levels 2..L (per-level device tables)
   uint32_t pf_ahead = 12 * 1024;     // L2 prefetch window of the stored-block M2L kernels (bytes)
 };
@@ -92,6 +103,8 @@ inline LevelSet level_subset(const LevelSet& ls, uint32_t mask, bool keep) {
     o.cgrp0[n + 1] = o.cgrp0[n] + (ls.cgrp0[t + 1] - ls.cgrp0[t]);
     o.wgrp0[n + 1] = o.wgrp0[n] + (ls.wgrp0[t + 1] - ls.wgrp0[t]);
     o.pt0[n + 1] = o.pt0[n] + (ls.pt0[t + 1] - ls.pt0[t]);
+    o.t0[n + 1] = o.t0[n] + (ls.t0[t + 1] - ls.t0[t]);
+    o.b0[n + 1] = o.b0[n] + (ls.b0[t + 1] - ls.b0[t]);
     ++o.nlev;
   }
   return o;
@@ -107,8 +120,9 @@ struct Tuning {
   int host_pass_cols = 0;           // columns per pass of host-pointer batched calls (0: automatic)
   int m2l_t16 = 0;                  // 16-column stored M2L on transposed m16n8k4 tiles (else 8x8x4 tiles)
   int p2p_tc = 0;                   // 16-column mixed near field on tcgen05 tiles (else mma.sync tiles)
-  int m2l_tc = 0;  // 16-column mixed stored M2L on tcgen05 TF32 tiles (else FP64 tiles): an FP32 far
-                   // field, outside the mixed tolerance on deep trees; never chosen by the autotuner
+  int m2l_tc = 0;  // 16-column mixed stored M2L on tcgen05: 2 exact integer products from the byte
+                   // planes; 1 TF32 tiles, an FP32 far field outside the mixed tolerance on deep trees,
+                   // never chosen by the autotuner; 0 FP64 tiles
 };
 
 // Grid cell (ix, iy) of box k at level j: the base-4 digits of k read as

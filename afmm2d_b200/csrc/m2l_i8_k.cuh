@@ -1,0 +1,494 @@
+// M2L of 16-column mixed passes on the 5th-generation tensor cores with
+// exact integer products (tcgen05.mma.kind::i8, int32 accumulators in tensor
+// memory), from the same 32-bit fixed-point entries as the FP64-tile kernels.
+//
+// Arithmetic.  An entry of block (b, slot s) is (u - 2^31) 2^k with u the
+// stored 32-bit word (m2l_q) and 2^k the block's scale.  Each column n of the
+// source box's outgoing charges is put in 32-bit fixed point for this pass:
+// X = round(x 2^(31 - e)) with 2^e the column's largest magnitude rounded up
+// (|X| < 2^31).  Then
+//   sum_k (u_k - 2^31) X_k = sum_{i,j} 2^(8(i+j)) sum_k u_k[i] X_k[j] - 2^31 sum_k X_k
+// with u_k[i] the unsigned bytes of u and X_k[j] the bytes of X (the top one
+// signed): every byte product and its K sum are exact in int32 (|sum| <
+// 4 K 2^16 for K <= 1024).  The 13 byte-pair products with i + j >= 2 run as
+// int8 MMAs into five accumulators (one per weight 2^(8(i+j))); the three
+// dropped ones weigh at most 2^-40 of a product's magnitude.  Per source box
+// the accumulators are read (tcgen05.ld), combined in FP64 with the offset
+// term and the two power-of-two scales, and added into FP64 row sums.  The
+// result differs from the FP64-tile kernels only by the charges' 32-bit
+// rounding and the dropped byte products.
+//
+// Storage (built once from m2l_q, k_m2l_slice): each block as byte planes in
+// the K-major shared-memory layout of the MMA -- 8-row x 16-byte core
+// matrices, [16-column chunk kc][byte plane p][8-row group rg][128 B], rows
+// padded to 8 and columns to 16 with zeros -- so every stage is a handful of
+// contiguous bulk copies.  The charges' planes (k_qhat_slice, every pass):
+// per source box [32-row stage][16-row half][plane][8-column group][128 B],
+// rows padded to 32 with zeros.
+//
+// Mapping: persistent CTAs (two per SM), each taking work items (a box and
+// up to 128 of its skeleton rows: the MMA's M) in a fixed order; six warps in
+// three roles.  Warp 0 (one lane) streams each stage's A planes (up to 8 bulk
+// copies) and B planes (one copy) into a ring of shared-memory stages
+// (cp.async.bulk with mbarrier transaction counts); warp 1 (one lane) issues
+// the 13 MMAs of a stage (K = 32 sources) and commits them to the stage's
+// "empty" barrier, and after a source box's last stage to an accumulator
+// barrier; warps 2-5 read the accumulators of a finished source box (two
+// accumulator sets alternate by source box, so the MMAs of the next box
+// proceed meanwhile).  Every mbarrier wait is bounded (~1 s): on a timeout
+// the CTA sets *err, stops, waits (bounded) for its copies and MMAs, frees
+// its tensor memory and returns.
+#pragma once
+#include <stdint.h>
+
+#include "fmm.cuh"
+#include "tcgen05.cuh"
+
+namespace afmm {
+
+namespace m2l_i8_detail {
+
+using namespace tc;
+
+constexpr int kThreads = 192;           // warp 0 loads, warp 1 MMAs, warps 2-5 epilogue
+constexpr int kStages = 6;
+constexpr uint32_t kPlaneA = 16 * 128;  // one (16-column chunk, plane) of A: 16 row groups
+constexpr uint32_t kBytesA = 2 * 4 * kPlaneA;  // 16 KB: two column chunks x four planes
+constexpr uint32_t kBytesB = 2048;             // 32 rows x 16 columns x four planes
+constexpr uint32_t kStage = kBytesA + kBytesB;
+constexpr size_t kSmem = (size_t)kStages * kStage + 128;
+constexpr uint32_t kTmemCols = 256;  // two sets of five 16-column int32 accumulators
+constexpr uint32_t kSetCols = 128;
+
+// tcgen05 instruction descriptor, kind::i8: D int32, A unsigned 8-bit, B
+// unsigned (b_signed = 0) or signed (1) 8-bit, both K-major, N = 16, M = 128.
+__host__ __device__ constexpr uint32_t idesc_i8(int b_signed) {
+  return (2u << 4) | (0u << 7) | ((uint32_t)b_signed << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// Bulk copy global -> this CTA's shared memory, completing on `mbar`'s
+// transaction count (16-byte aligned addresses, size a multiple of 16).
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+// 16 consecutive int32 accumulator columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16_i(uint32_t taddr, int32_t (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int n = 0; n < 16; ++n) v[n] = (int32_t)r[n];
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// Sliced bytes of block (b, slot) with r_b rows and r_c columns.
+__device__ __forceinline__ long long block_bytes(int rb, int rc) {
+  return (long long)ceil_div(rc, 16) * 4 * ceil_div(rb, 8) * 128;
+}
+
+// The slots of box b as a warp sees them: lane l holds slot l (and slot
+// 32 + l for l < 8): its source box, rank and the byte offset of its sliced
+// block within the box's region (prefix over the slots in order).
+struct SlotTable {
+  int srcA, srcB, rcA, rcB;
+  long long offA, offB;
+};
+
+__device__ __forceinline__ SlotTable slot_table(const LevelView& v, long b, int rb, int lane) {
+  SlotTable t;
+  t.srcA = v.il[b * 40 + lane];
+  t.srcB = lane < 8 ? v.il[b * 40 + 32 + lane] : -1;
+  t.rcA = (t.srcA >= 0 && rb > 0) ? v.rank[t.srcA] : 0;
+  t.rcB = (t.srcB >= 0 && rb > 0) ? v.rank[t.srcB] : 0;
+  const long long nA = t.rcA ? block_bytes(rb, t.rcA) : 0, nB = t.rcB ? block_bytes(rb, t.rcB) : 0;
+  long long sA = nA, sB = nB;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const long long ta = __shfl_up_sync(0xffffffffu, sA, o), tb = __shfl_up_sync(0xffffffffu, sB, o);
+    if (lane >= o) {
+      sA += ta;
+      sB += tb;
+    }
+  }
+  const long long totA = __shfl_sync(0xffffffffu, sA, 31);
+  t.offA = sA - nA;
+  t.offB = totA + sB - nB;
+  return t;
+}
+
+// Slot s's (source box, rank, block offset), broadcast from the table.
+__device__ __forceinline__ void slot_get(const SlotTable& t, int s, int& src, int& rc, long long& off) {
+  const int l = s & 31;
+  src = __shfl_sync(0xffffffffu, s < 32 ? t.srcA : t.srcB, l);
+  rc = __shfl_sync(0xffffffffu, s < 32 ? t.rcA : t.rcB, l);
+  off = __shfl_sync(0xffffffffu, s < 32 ? t.offA : t.offB, l);
+}
+
+// Work item g of the level set: level index, box, first row of its 128-row tile.
+__device__ __forceinline__ void item_of(const LevelSet& ls, long g, int& j, int& b, int& r0) {
+  j = 0;
+  while (j + 1 < ls.nlev && g >= ls.t0[j + 1]) ++j;
+  const long i = g - ls.t0[j];
+  b = ls.lv[j].tile_box[i];
+  r0 = ls.lv[j].tile_row[i];
+}
+
+// ---------------------------------------------------------------- slicing
+// Sliced copy of every block of one level from the fixed-point words: one
+// CTA per box, threads over the box's bytes.
+__global__ void __launch_bounds__(256) k_m2l_slice(LevelView v) {
+  const long b = blockIdx.x;
+  const int rb = v.rank[b];
+  if (rb == 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ int s_src[40], s_rc[40];
+  __shared__ long long s_off[41], s_qoff[41];
+  if (warp == 0) {
+    const SlotTable t = slot_table(v, b, rb, lane);
+    s_src[lane] = t.srcA;
+    s_rc[lane] = t.rcA;
+    s_off[lane] = t.offA;
+    if (lane < 8) {
+      s_src[32 + lane] = t.srcB;
+      s_rc[32 + lane] = t.rcB;
+      s_off[32 + lane] = t.offB;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long q = 0;  // word offset of each slot's fixed-point block (the m2l_off order)
+    for (int s = 0; s < 40; ++s) {
+      s_qoff[s] = q;
+      q += (long long)rb * s_rc[s];
+    }
+  }
+  __syncthreads();
+  const int RG = ceil_div(rb, 8);
+  unsigned char* dst = v.m2l_s + v.m2l_s_off[b];
+  const uint32_t* src = v.m2l_q + v.m2l_off[b];
+  for (int s = 0; s < 40; ++s) {
+    const int rc = s_rc[s];
+    if (rc == 0) continue;
+    const int KC = ceil_div(rc, 16);
+    unsigned char* d = dst + s_off[s];
+    const uint32_t* q = src + s_qoff[s];
+    // one thread per (column chunk, row) writes that row's 16 bytes in every plane
+    for (int e = threadIdx.x; e < KC * RG * 8; e += blockDim.x) {
+      const int kc = e / (RG * 8), row = e - kc * (RG * 8);
+      uint32_t w[4][4];
+#pragma unroll
+      for (int c = 0; c < 16; ++c) {
+        const int k = kc * 16 + c;
+        const uint32_t u = (row < rb && k < rc) ? q[(long long)k * rb + row] : 0u;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+          const uint32_t byte = (u >> (8 * p)) & 0xffu;
+          if ((c & 3) == 0) w[p][c >> 2] = byte;
+          else w[p][c >> 2] |= byte << (8 * (c & 3));
+        }
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        *reinterpret_cast<uint4*>(d + ((long long)(kc * 4 + p) * RG + (row >> 3)) * 128 + (row & 7) * 16) =
+            make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
+    }
+  }
+}
+
+// The charges of every stored level in 32-bit fixed point, sliced: one warp
+// per source box (lane = column for the column maxima and sums).
+__global__ void __launch_bounds__(128) k_qhat_slice(LevelSet ls, const double* const* __restrict__ qhat_lv) {
+  const long gw = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (gw >= ls.b0[ls.nlev]) return;  // whole warps only
+  int j = 0;
+  while (j + 1 < ls.nlev && gw >= ls.b0[j + 1]) ++j;
+  const LevelView& v = ls.lv[j];
+  const long c = gw - ls.b0[j];
+  const int r = v.rank[c];
+  if (r == 0) return;
+  const double* x = qhat_lv[ls.src[j]] + (long)v.skel_off[c] * 16;
+  unsigned char* out = v.qs8 + (long long)v.qs8_off[c] * 2048;
+  // column n = lane & 15; the two half-warps split the rows
+  const int n = lane & 15, h = lane >> 4;
+  double mx = 0.0;
+  int nan = 0;
+  for (int k = h; k < r; k += 2) {
+    const double q = x[(long)k * 16 + n];
+    mx = fmax(mx, fabs(q));
+    nan |= q != q;
+  }
+  mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
+  nan |= __shfl_xor_sync(0xffffffffu, nan, 16);
+  // a non-finite charge makes the column decode to NaN, as the FP64 tiles would
+  const bool bad = nan || !(mx <= 1.7976931348623157e308);
+  int e = 0;
+  if (!bad && mx > 0.0) frexp(mx, &e);  // mx in [2^(e-1), 2^e)
+  long long sum = 0;
+  const int ns = ceil_div(r, 32);
+  for (int st = 0; st < ns; ++st)
+    for (int kh = 0; kh < 2; ++kh) {
+      // this lane: column n, rows st*32 + kh*16 + (h*8 .. h*8 + 7)
+      uint32_t w[4][2] = {{0u, 0u}, {0u, 0u}, {0u, 0u}, {0u, 0u}};
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int k = st * 32 + kh * 16 + h * 8 + t;
+        int32_t X = 0;
+        if (k < r && !bad && mx > 0.0) {
+          double q = rint(scalbn(x[(long)k * 16 + n], 31 - e));
+          q = fmin(fmax(q, -2147483647.0), 2147483647.0);
+          X = (int32_t)q;
+        }
+        sum += X;
+        const uint32_t ux = (uint32_t)X;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) w[p][t >> 2] |= ((ux >> (8 * p)) & 0xffu) << (8 * (t & 3));
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+        *reinterpret_cast<uint2*>(out + ((long long)(st * 2 + kh) * 4 + p) * 256 + (n >> 3) * 128 + (n & 7) * 16 +
+                                  h * 8) = make_uint2(w[p][0], w[p][1]);
+    }
+  sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+  if (h == 0) {
+    v.qs_exp[c * 16 + n] = bad ? 0x7fff : e;
+    v.qs_sum[c * 16 + n] = sum;
+  }
+}
+
+// ------------------------------------------------------------------- M2L
+__global__ void __launch_bounds__(kThreads, 2) k_m2l_i8(LevelSet ls, double* const* __restrict__ yhat_lv, int* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t s_full[kStages], s_empty[kStages], s_accf[2], s_acce[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // 128-byte aligned stage ring (no swizzle: the descriptors need 16 bytes)
+  const uint32_t ring = (smem_addr(smem_raw) + 127u) & ~127u;
+  if (tid == 0) {
+    for (int i = 0; i < kStages; ++i) {
+      mbar_init(smem_addr(&s_full[i]), 1);
+      mbar_init(smem_addr(&s_empty[i]), 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(smem_addr(&s_accf[i]), 1);
+      mbar_init(smem_addr(&s_acce[i]), 4);
+    }
+    s_fail = 0;
+    mbar_init_fence();
+  }
+  if (warp == 1) tmem_alloc(&s_tmem, kTmemCols);
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = s_tmem;
+  const long nitems = ls.t0[ls.nlev];
+  bool ok = true;
+
+  if (warp == 0) {
+    // ------------------------------------------------ loads (lane 0 issues)
+    long G = 0;  // stages issued so far
+    for (long g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+      int j, b, r0;
+      item_of(ls, g, j, b, r0);
+      const LevelView& v = ls.lv[j];
+      const int rb = v.rank[b];
+      const int RG = ceil_div(rb, 8), rg0 = r0 >> 3, rgt = min(16, RG - rg0);
+      const SlotTable t = slot_table(v, b, rb, lane);
+      const unsigned char* A0 = v.m2l_s + v.m2l_s_off[b];
+      const unsigned char* Bl = v.qs8;
+      for (int s = 0; s < 40 && ok; ++s) {
+        int c, rc;
+        long long off;
+        slot_get(t, s, c, rc, off);
+        if (rc == 0) continue;
+        const int KC = ceil_div(rc, 16), ns = ceil_div(rc, 32);
+        const long long qoff = rc ? (long long)v.qs8_off[c] : 0;
+        for (int st = 0; st < ns; ++st, ++G) {
+          const int slot = (int)(G % kStages);
+          const uint32_t par = (uint32_t)((G / kStages) & 1) ^ 1u;
+          bool w = true;
+          if (lane == 0) w = mbar_wait(smem_addr(&s_empty[slot]), par);
+          if (!__shfl_sync(0xffffffffu, (int)w, 0)) {
+            ok = false;
+            break;
+          }
+          if (lane == 0) {
+            const uint32_t sA = ring + (uint32_t)slot * kStage, sB = sA + kBytesA;
+            const int nkc = min(2, KC - 2 * st);
+            const uint32_t bytes = (uint32_t)nkc * 4 * rgt * 128 + kBytesB;
+            mbar_expect_tx(smem_addr(&s_full[slot]), bytes);
+            for (int kh = 0; kh < nkc; ++kh)
+              for (int p = 0; p < 4; ++p) {
+                const unsigned char* src = A0 + off + ((long long)((2 * st + kh) * 4 + p) * RG + rg0) * 128;
+                bulk_g2s(sA + (uint32_t)(kh * 4 + p) * kPlaneA, src, (uint32_t)rgt * 128, smem_addr(&s_full[slot]));
+              }
+            bulk_g2s(sB, Bl + (qoff + st) * 2048, kBytesB, smem_addr(&s_full[slot]));
+          }
+        }
+      }
+    }
+    // drain: every issued stage's copies have landed
+    if (lane == 0) {
+      for (long k = G > kStages ? G - kStages : 0; k < G; ++k)
+        if (!mbar_wait(smem_addr(&s_full[k % kStages]), (uint32_t)((k / kStages) & 1))) ok = false;
+    }
+    ok = __shfl_sync(0xffffffffu, (int)ok, 0);
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMAs (lane 0 issues)
+    long G = 0, m = 0;  // stages consumed, source boxes started
+    for (long g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+      int j, b, r0;
+      item_of(ls, g, j, b, r0);
+      const LevelView& v = ls.lv[j];
+      const int rb = v.rank[b];
+      const SlotTable t = slot_table(v, b, rb, lane);
+      for (int s = 0; s < 40 && ok; ++s) {
+        int c, rc;
+        long long off;
+        slot_get(t, s, c, rc, off);
+        if (rc == 0) continue;
+        const int ns = ceil_div(rc, 32);
+        const int set = (int)(m & 1);
+        bool w = true;
+        if (lane == 0 && m >= 2) w = mbar_wait(smem_addr(&s_acce[set]), (uint32_t)(((m >> 1) - 1) & 1));
+        if (!__shfl_sync(0xffffffffu, (int)w, 0)) {
+          ok = false;
+          break;
+        }
+        fence_after();
+        for (int st = 0; st < ns; ++st, ++G) {
+          const int slot = (int)(G % kStages);
+          if (lane == 0) w = mbar_wait(smem_addr(&s_full[slot]), (uint32_t)((G / kStages) & 1));
+          if (!__shfl_sync(0xffffffffu, (int)w, 0)) {
+            ok = false;
+            break;
+          }
+          fence_after();
+          if (lane == 0) {
+            const uint32_t sA = ring + (uint32_t)slot * kStage, sB = sA + kBytesA;
+            const uint32_t d0 = tmem + (uint32_t)set * kSetCols;
+            uint32_t started = 0;  // bit w: accumulator w already written in this source box
+            if (st > 0) started = 0x1fu;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+              for (int jb = 0; jb < 4; ++jb) {
+                if (i + jb < 2) continue;
+                const int wc = i + jb - 2;
+                const uint64_t da = smem_desc(sA + (uint32_t)i * kPlaneA, 4 * kPlaneA, 128);
+                const uint64_t db = smem_desc(sB + (uint32_t)jb * 256, 4 * 256, 128);
+                mma_i8(d0 + (uint32_t)wc * 16, da, db, idesc_i8(jb == 3 ? 1 : 0), (started >> wc) & 1u);
+                started |= 1u << wc;
+              }
+            mma_commit(smem_addr(&s_empty[slot]));
+            if (st == ns - 1) mma_commit(smem_addr(&s_accf[set]));
+          }
+          __syncwarp();
+        }
+        ++m;
+      }
+    }
+    // drain: the last stage's MMAs are complete
+    if (lane == 0 && G > 0)
+      if (!mbar_wait(smem_addr(&s_empty[(G - 1) % kStages]), (uint32_t)(((G - 1) / kStages) & 1))) ok = false;
+    ok = __shfl_sync(0xffffffffu, (int)ok, 0);
+  } else {
+    // ------------------------------------------------ epilogue (warps 2-5)
+    const int quarter = warp & 3;  // tensor-memory lanes 32q .. 32q + 31
+    const int row_in_tile = quarter * 32 + lane;
+    constexpr double kW[5] = {65536.0, 16777216.0, 4294967296.0, 1099511627776.0, 281474976710656.0};  // 2^(8(w+2))
+    long m = 0;
+    for (long g = blockIdx.x; g < nitems && ok; g += gridDim.x) {
+      int j, b, r0;
+      item_of(ls, g, j, b, r0);
+      const LevelView& v = ls.lv[j];
+      const int rb = v.rank[b];
+      const SlotTable t = slot_table(v, b, rb, lane);
+      // a warp whose 32 lanes are all past the tile's rows only releases the accumulators
+      const bool live = r0 + quarter * 32 < min(rb, r0 + 128);
+      double acc[16];
+#pragma unroll
+      for (int n = 0; n < 16; ++n) acc[n] = 0.0;
+      for (int s = 0; s < 40 && ok; ++s) {
+        int c, rc;
+        long long off;
+        slot_get(t, s, c, rc, off);
+        if (rc == 0) continue;
+        const int set = (int)(m & 1);
+        const bool w = mbar_wait(smem_addr(&s_accf[set]), (uint32_t)((m >> 1) & 1));
+        if (!__all_sync(0xffffffffu, w)) {
+          ok = false;
+          break;
+        }
+        fence_after();
+        int32_t a[5][16];
+        if (live) {
+          const uint32_t base = tmem + ((uint32_t)(32 * quarter) << 16) + (uint32_t)set * kSetCols;
+#pragma unroll
+          for (int wc = 0; wc < 5; ++wc) tmem_ld16_i(base + (uint32_t)wc * 16, a[wc]);
+          tmem_wait_ld();
+        }
+        fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_addr(&s_acce[set]));
+        if (live) {
+          // combine: sum_w 2^(8(w+2)) a_w - 2^31 S, times 2^k 2^(e - 31)
+          const double2 dec = v.m2l_dec[(long)b * 40 + s];
+#pragma unroll
+          for (int n = 0; n < 16; ++n) {
+            double tsum = -2147483648.0 * (double)v.qs_sum[(long)c * 16 + n];
+#pragma unroll
+            for (int wc = 4; wc >= 0; --wc) tsum = fma((double)a[wc][n], kW[wc], tsum);
+            const int e = v.qs_exp[(long)c * 16 + n];
+            const double sc = e == 0x7fff ? __longlong_as_double(0x7ff8000000000000ll) : ldexp(dec.x, e - 31);
+            acc[n] = fma(tsum, sc, acc[n]);
+          }
+        }
+        ++m;
+      }
+      const int row = r0 + row_in_tile;
+      if (ok && row_in_tile < 128 && row < rb && row < r0 + 128) {
+        double2* o = reinterpret_cast<double2*>(yhat_lv[ls.src[j]] + ((long)v.skel_off[b] + row) * 16);
+#pragma unroll
+        for (int n = 0; n < 8; ++n) o[n] = make_double2(acc[2 * n], acc[2 * n + 1]);
+      }
+    }
+  }
+  if (!ok) s_fail = 1;  // benign race: every writer stores 1
+  fence_before();
+  __syncthreads();
+  if (s_fail && tid == 0) *(volatile int*)err = 1;  // host-mapped flag
+  if (warp == 1) {
+    fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+}  // namespace m2l_i8_detail
+
+}  // namespace afmm

@@ -45,6 +45,10 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
 // The M2L stage alone of a batched pass of rc columns (on the batch buffers'
 // current outgoing charges); returns the launches made.
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s);
+
+// Byte-plane copy of one level's fixed-point blocks for the integer
+// tensor-core M2L (m2l_i8_k.cuh); v.m2l_s and v.m2l_s_off must be set.
+void m2l_slice(const LevelView& v, cudaStream_t s);
 // The near-field stage alone of a batched pass of rc columns (on the batch
 // buffers' current charges); returns the launches made.
 int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int fp64, cudaStream_t s);

@@ -254,7 +254,8 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
  * launch parameters `what` selects (bit 0: L2 prefetch windows of the
  * stored-block M2L kernels; bit 1: per level, stored blocks or entries on
  * the fly in the mixed paths; bit 2: pass width of host-pointer batched
- * calls; bit 3: tile shape of the 16-column stored M2L on FP64 tiles; bit 4: tcgen05 or
+ * calls; bit 3: form of the 16-column stored M2L (FP64 tiles or tcgen05
+ * integer products); bit 4: tcgen05 or
  * mma.sync near field of 16-column mixed passes; 0 = all) and keeps the
  * fastest in the handle.  With a cache_path
  * (may be NULL), a line keyed by the device name and the problem's structure
@@ -268,8 +269,10 @@ afmm_status afmm_kd_permutation_noalloc(int N, int min_particles_in_leaf, const 
  * (bit t = level t + 2), the same for batched mixed passes, host pass width
  * (0 = automatic), 16-column stored M2L on transposed m16n8k4 tiles (1) or
  * on 8x8x4 tiles (0), 16-column mixed near field on tcgen05 tiles (1) or on
- * mma.sync tiles (0), 16-column mixed stored M2L on tcgen05 TF32 tiles from
- * the fixed-point blocks (1) or on FP64 tiles (0)]; values past n are left
+ * mma.sync tiles (0), 16-column mixed stored M2L on tcgen05 with exact
+ * integer products from byte planes of the fixed-point blocks (2), on
+ * tcgen05 TF32 tiles (1: an FP32 far field, outside the mixed tolerance on
+ * deep trees) or on FP64 tiles (0)]; values past n are left
  * unchanged by afmm_set_tuning.  A tcgen05 kernel whose bounded wait gives up
  * makes the matvec return AFMM_TIMEOUT. */
 afmm_status afmm_autotune(afmm_handle* h, int what, const char* cache_path, int* from_cache);

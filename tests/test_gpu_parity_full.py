@@ -291,3 +291,29 @@ def test_tcgen05_m2l(kernel, tol, wl):
     Ytt = a.computeMatVecProduct(Q, precision="mixed")
     for c in (0, 15):
         assert_rel(Ytt[:, c], a.computeMatVecProduct(Q[:, c]), MIXED_TOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,tol,wl", [("one_over_r", 6, "mixture4m"), ("log", 10, "uniform1m"),
+                                           ("log", 12, "mixture4m"), ("gaussian", 8, "mixture4m")])
+def test_tcgen05_integer_m2l(kernel, tol, wl):
+    """The 16-column mixed stored M2L as exact integer products on tcgen05
+    (byte planes of the fixed-point blocks and of the charges, m2l_tc = 2)
+    agrees with the FP64-tile form on the same fixed-point blocks to the
+    charges' 32-bit rounding, and with the FP64 path within the mixed
+    tolerance; deterministic.  TOL 10 / 12 give ranks above 32 (several
+    stages per source box) and above 128 (several row tiles per box)."""
+    pts, _, _ = workloads.make(wl, N=65536)
+    a = A.AFMM(65536, 64, tol, pts, kernel=kernel)
+    a.assemble()
+    Q = np.random.default_rng(8).standard_normal((65536, 16))
+    a.set_tuning(m2l_tc=0, otf_batched=0)
+    Ym = a.computeMatVecProduct(Q, precision="mixed")
+    Yb = a.computeMatVecProduct(Q, precision="fp64_batched")
+    a.set_tuning(m2l_tc=2)
+    Yi = a.computeMatVecProduct(Q, precision="mixed")
+    np.testing.assert_array_equal(Yi, a.computeMatVecProduct(Q, precision="mixed"))
+    np.testing.assert_array_equal(a.computeMatVecProduct(Q, precision="fp64_batched"), Yb)
+    for c in (0, 7, 15):
+        assert_rel(Yi[:, c], Ym[:, c], 1e-8)
+        assert_rel(Yi[:, c], a.computeMatVecProduct(Q[:, c]), MIXED_TOL)
