@@ -243,8 +243,9 @@ class AFMM:
 
     def set_m2l_fixed_point(self, on):
         """Before assemble(): keep a 32-bit fixed-point copy of the stored M2L
-        blocks for the mixed-precision paths (default on, when it fits)."""
-        _check(lib().afmm_set_m2l_fixed_point(self._h, 1 if on else 0), self._h)
+        blocks for the mixed-precision paths (default on, when it fits); 2
+        also keeps its byte planes for the integer tcgen05 M2L (m2l_tc = 2)."""
+        _check(lib().afmm_set_m2l_fixed_point(self._h, int(on)), self._h)
 
     def set_aca_plan(self, cluster=0, ctas_per_sm=0):
         """Before assemble(): CTAs per box and per SM of the ACA kernel

@@ -69,7 +69,7 @@ struct afmm_handle {
   int device = 0;
   int m2l_mode = AFMM_M2L_AUTO;  // afmm_m2l_storage
   bool m2l_stored = false;
-  int m2l_q_mode = 1;            // also keep a 32-bit fixed-point copy for the mixed paths
+  int m2l_q_mode = 1;            // 1: also keep a 32-bit fixed-point copy for the mixed paths; 2: and its byte planes
   int aca_cluster = 0, aca_ctas_per_sm = 0;  // ACA planner overrides (0: automatic)
   bool m2l_q_stored = false;
   bool m2l_s_stored = false;     // byte-plane copy for the integer tensor-core M2L
@@ -779,7 +779,7 @@ void finish_assemble(afmm_handle* h) {
       AFMM_CUDA(cudaStreamSynchronize(s));
       h->m2l_q_stored = true;
       h->setup_phase[2].second += now_s() - t_ph;
-      build_byte_planes(h, l2p_total, rows_total);
+      if (h->m2l_q_mode == 2) build_byte_planes(h, l2p_total, rows_total);
     }
   }
   t_ph = now_s();
@@ -1006,7 +1006,7 @@ SetupImage read_setup(const char* path) {
   im.a = par[0];
   im.param = par[1];
   if (im.N < 1 || im.M < 1 || im.L < 2 || im.L >= kMaxLevels || im.L != n_levels(im.N, im.M) || im.m2l_mode < 0 ||
-      im.m2l_mode > 2)
+      im.m2l_mode > 2 || im.q_mode < 0 || im.q_mode > 2)
     throw Error{AFMM_BAD_ARG, "setup file header is inconsistent"};
   if (!kernel_known(im.kernel_id))
     throw Error{AFMM_BAD_ARG, "setup file uses kernel id " + std::to_string(im.kernel_id) + ", which is not registered"};
@@ -1734,7 +1734,11 @@ afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on) {
     h->err = "afmm_set_m2l_fixed_point after afmm_assemble";
     return AFMM_BAD_ARG;
   }
-  h->m2l_q_mode = on ? 1 : 0;
+  if (on < 0 || on > 2) {
+    h->err = "afmm_set_m2l_fixed_point: mode is 0, 1 or 2";
+    return AFMM_BAD_ARG;
+  }
+  h->m2l_q_mode = on;
   return AFMM_OK;
 }
 

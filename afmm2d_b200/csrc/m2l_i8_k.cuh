@@ -38,6 +38,13 @@
 // proceed meanwhile).  Every mbarrier wait is bounded (~1 s): on a timeout
 // the CTA sets *err, stops, waits (bounded) for its copies and MMAs, frees
 // its tensor memory and returns.
+//
+// Measured: exact (5.1e-7 of the FP64 path at the 4,194,304-point mixture,
+// as the FP64 tiles) but 33.4 ms against 4.21 ms for the FP64 tiles: its
+// 41M MMAs of 128 x 16 x 32 take ~240 SM cycles each (the TF32 near field's
+// 128 x 16 x 8 ones ~290), so with 16 right-hand sides the MMA count, not
+// the bytes or the tensor throughput, sets the time.  Opt-in: fixed-point
+// mode 2 keeps the byte planes, tuning value m2l_tc = 2 selects it.
 #pragma once
 #include <stdint.h>
 

@@ -231,6 +231,8 @@ def run_ours(args):
     warm_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     a = A.AFMM(N, p["M"], p["tol"], pts, kernel=p["kernel"])
+    if tuning_overrides(args).get("m2l_tc") == 2:
+        a.set_m2l_fixed_point(2)  # the integer tcgen05 M2L applies byte planes kept at assembly
     a.assemble()
     setup_s = time.perf_counter() - t0
     counts = a.counts()

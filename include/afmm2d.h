@@ -136,7 +136,9 @@ afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored);
  * power-of-two scale; its entries are stored as 32-bit integers of that
  * scale, within 2^-31 of the block's largest entry, and applied in FP64
  * arithmetic: half the bytes of the FP64 blocks.  AFMM_PREC_FP64 and
- * AFMM_PREC_FP64_BATCHED always apply the FP64 blocks. */
+ * AFMM_PREC_FP64_BATCHED always apply the FP64 blocks.  Mode 2 also keeps
+ * the copy as byte planes for the exact integer tcgen05 M2L (tuning value
+ * m2l_tc = 2; about 1.3x the fixed-point bytes more). */
 afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on);
 /* Launch plan of the ACA kernel for every level, before afmm_assemble: CTAs
  * per box (a thread-block cluster of 1, 2, 4, 8 or 16; 0 = the planner's

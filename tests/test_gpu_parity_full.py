@@ -305,6 +305,7 @@ def test_tcgen05_integer_m2l(kernel, tol, wl):
     stages per source box) and above 128 (several row tiles per box)."""
     pts, _, _ = workloads.make(wl, N=65536)
     a = A.AFMM(65536, 64, tol, pts, kernel=kernel)
+    a.set_m2l_fixed_point(2)
     a.assemble()
     Q = np.random.default_rng(8).standard_normal((65536, 16))
     a.set_tuning(m2l_tc=0, otf_batched=0)
