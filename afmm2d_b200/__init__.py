@@ -62,6 +62,9 @@ _SIGS = {
     "afmm_kernel_eval": [_i, ctypes.c_double, ctypes.c_double, _i64, _vp, _vp, _vp, _i],
     "afmm_measure_fma_peaks": [_vp, _vp],
     "afmm_measure_fp64_pipes": [_vp, _vp, _vp],
+    "afmm_set_shard": [_vp, _i, _i],
+    "afmm_get_shard": [_vp, _vp, _vp, _vp],
+    "afmm_shard_range": [_i, _i, _i, _vp, _vp, _vp],
     "afmm_kd_permutation_noalloc": [_i, _i, _vp, _vp, _vp, _vp],
     "afmm_get_device_alloc_count": [_vp],
     "afmm_autotune": [_vp, _i, ctypes.c_char_p, _vp],
@@ -135,6 +138,15 @@ def measure_fma_peaks():
     a, b = ctypes.c_double(), ctypes.c_double()
     _check(lib().afmm_measure_fma_peaks(ctypes.byref(a), ctypes.byref(b)))
     return a.value, b.value
+
+
+def shard_range(nlevels, index, count):
+    """(level, k0, k1): the boxes [k0, k1) of `level` that shard `index` of
+    `count` owns on a tree of `nlevels` levels (no device needed)."""
+    lev, a, b = ctypes.c_int(), ctypes.c_int64(), ctypes.c_int64()
+    _check(lib().afmm_shard_range(int(nlevels), int(index), int(count), ctypes.byref(lev), ctypes.byref(a),
+                                  ctypes.byref(b)))
+    return lev.value, a.value, b.value
 
 
 def measure_fp64_pipes():
@@ -240,6 +252,18 @@ class AFMM:
         """M2L block storage before assemble(): "auto" (store when they fit),
         "store", or "on_the_fly" (entries evaluated in FP64 by every matvec)."""
         _check(lib().afmm_set_m2l_storage(self._h, self.M2L_STORAGE[mode]), self._h)
+
+    def set_shard(self, index, count):
+        """After assemble(): compute only shard `index` of `count` (its
+        subtrees' potentials; zeros elsewhere), so that the shards' outputs
+        sum to the whole product.  count = 1 restores the whole problem."""
+        _check(lib().afmm_set_shard(self._h, int(index), int(count)), self._h)
+
+    def shard(self):
+        """(index, count, level) of the handle's shard."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(lib().afmm_get_shard(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)), self._h)
+        return a.value, b.value, c.value
 
     def set_m2l_fixed_point(self, on):
         """Before assemble(): keep a 32-bit fixed-point copy of the stored M2L

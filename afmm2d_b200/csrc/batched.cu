@@ -650,7 +650,7 @@ struct Pass {
     const bool q32 = RC >= 8 && !fp64 && p.levels.lv[0].m2l_q != nullptr;
     const bool stored = RC >= 8 && (q32 || p.levels.lv[0].m2l != nullptr);
     const uint32_t otf = !stored ? 0xffffffffu : (fp64 ? 0u : p.tune.otf_batched);
-    LevelSet st = level_subset(p.levels, otf, false);
+    LevelSet st = level_subset(p.levels_m2l, otf, false);  // a shard's boxes at the sharded levels
     const LevelSet fly = level_subset(p.levels, otf, true);
     st.pf_ahead = p.tune.pf_batched;
     int n = 0;
@@ -715,6 +715,9 @@ struct Pass {
                   int64_t ldy, int ncols, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
     constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
+    if (p.shard_count > 1) {  // points outside the shard's leaves come out as zeros
+      AFMM_CUDA(cudaMemsetAsync(bs.ys, 0, sizeof(double) * (size_t)N * RC, s));
+    }
     if (tm) tm->mark(s, "gather");
     k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl, fp64);
     AFMM_LAUNCH_CHECK();
@@ -741,9 +744,10 @@ struct Pass {
     *launches += m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
     if (tm) tm->mark(s, "l2l");
     for (int j = 2; j <= p.L; ++j) {
-      const LevelView& v = p.lv[j];
+      const LevelView& v = p.lv_down[j];  // a shard's subtrees at the sharded levels
       if (v.nnodes == 0) continue;
-      if (RC >= 8 && split_warps(v.nncgroups, false) == 8)
+      // the split follows the whole level, so a shard's rows get the same bits
+      if (RC >= 8 && split_warps(p.lv[j].nncgroups, false) == 8)
         k_l2l_mma_split<RM, 8><<<(int)v.nncgroups, 256, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
                                                                 bs.ys, j == p.L);
       else if (RC >= 8)
@@ -823,7 +827,7 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
 void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const double* q, int64_t ldq, double* y,
                     int64_t ldy, int nrhs, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
   if (!ms.ready || !bs.ready) throw Error{AFMM_BAD_ARG, "batched operators are not set up"};
-  NearView nv = p.near;
+  NearView nv = p.near_own;
   nv.anchor = ms.leaf_anchor;
   nv.rel = ms.rel;
   nv.span = ms.leaf_span;

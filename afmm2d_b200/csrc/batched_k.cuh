@@ -62,7 +62,7 @@ __global__ void k_p2p_b(NearView nv, KernelParams kp, const float* __restrict__ 
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
-  const long b = blockIdx.x;
+  const long b = nv.leaf0 + blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const float a32 = (float)kp.a, p32 = (float)kp.param;
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_coff[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
-  const long b = blockIdx.x;
+  const long b = nv.leaf0 + blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const float a32 = (float)kp.a, p32 = (float)kp.param;
@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(128) k_p2p_dmma(NearView nv, KernelParams kp, 
   constexpr int NTT = 4;  // 8-row target tiles per warp
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_coff[10], s_ns;
-  const long b = blockIdx.x;
+  const long b = nv.leaf0 + blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   if (threadIdx.x == 0) {

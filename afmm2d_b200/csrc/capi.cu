@@ -71,6 +71,7 @@ struct afmm_handle {
   bool m2l_stored = false;
   int m2l_q_mode = 1;            // 1: also keep a 32-bit fixed-point copy for the mixed paths; 2: and its byte planes
   int aca_cluster = 0, aca_ctas_per_sm = 0;  // ACA planner overrides (0: automatic)
+  int shard_index = 0, shard_count = 1;      // afmm_set_shard
   bool m2l_q_stored = false;
   bool m2l_s_stored = false;     // byte-plane copy for the integer tensor-core M2L
   KernelParams kp{};
@@ -271,6 +272,60 @@ std::pair<double, double> fp64_pipes_tflops() {
   return {mma, fma_};
 }
 
+// Narrows a box-ordered chunk table (box ids, first rows, count) to the
+// chunks of boxes [bl, bh).
+void narrow_table(const int32_t*& box, const int32_t*& row, long& n, long bl, long bh) {
+  if (n == 0) return;
+  std::vector<int32_t> hb((size_t)n);
+  AFMM_CUDA(cudaMemcpy(hb.data(), box, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost));
+  const long c0 = std::lower_bound(hb.begin(), hb.end(), (int32_t)bl) - hb.begin();
+  const long c1 = std::lower_bound(hb.begin(), hb.end(), (int32_t)bh) - hb.begin();
+  box += c0;
+  row += c0;
+  n = c1 - c0;
+}
+
+// The plan's shard views (MatvecPlan::levels_m2l, lv_down, near_own) for the
+// handle's shard: at the sharded level and below, the M2L and L2L chunk
+// tables narrowed to the shard's subtrees and the near field to its leaves.
+void apply_shard(afmm_handle* h) {
+  MatvecPlan& p = h->plan;
+  p.levels_m2l = p.levels;
+  p.near_own = p.near;
+  for (int j = 0; j <= h->L; ++j) p.lv_down[j] = p.lv[j];
+  p.shard_index = 0;
+  p.shard_count = 1;
+  p.shard_level = 0;
+  if (h->shard_count <= 1) return;
+  int lev = 0;
+  long k0 = 0, k1 = 0;
+  if (!shard_range(h->L, h->shard_index, h->shard_count, lev, k0, k1))
+    throw Error{AFMM_BAD_ARG, "the tree has fewer leaves than shards"};
+  for (int j = lev; j <= h->L; ++j) {
+    const long sc = 1L << (2 * (j - lev)), bl = k0 * sc, bh = k1 * sc;
+    LevelView& d = p.lv_down[j];
+    narrow_table(d.ncgrp_box, d.ncgrp_row, d.nncgroups, bl, bh);
+    narrow_table(d.nwgrp_box, d.nwgrp_row, d.nnwgroups, bl, bh);
+    if (j >= 2) {
+      LevelView m = p.lv[j];
+      narrow_table(m.cgrp_box, m.cgrp_row, m.ncgroups, bl, bh);
+      narrow_table(m.wgrp_box, m.wgrp_row, m.nwgroups, bl, bh);
+      p.levels_m2l.lv[j - 2] = m;
+    }
+  }
+  LevelSet& ls = p.levels_m2l;
+  for (int t = 0; t < ls.nlev; ++t) {
+    ls.cgrp0[t + 1] = ls.cgrp0[t] + ls.lv[t].ncgroups;
+    ls.wgrp0[t + 1] = ls.wgrp0[t] + ls.lv[t].nwgroups;
+  }
+  const long sl = 1L << (2 * (h->L - lev));
+  p.near_own.leaf0 = k0 * sl;
+  p.near_own.nleaf = (k1 - k0) * sl;
+  p.shard_index = h->shard_index;
+  p.shard_count = h->shard_count;
+  p.shard_level = lev;
+}
+
 void build_plan(afmm_handle* h) {
   MatvecPlan& p = h->plan;
   p.N = h->N;
@@ -363,6 +418,7 @@ void build_plan(afmm_handle* h) {
   nv.leaf_start = h->d_leaf_start;
   nv.leaf_cnt = h->d_leaf_cnt;
   nv.nbr = h->lv[h->L].nbr;
+  apply_shard(h);
 }
 
 void create_layout(afmm_handle* h);
@@ -1742,6 +1798,42 @@ afmm_status afmm_set_m2l_fixed_point(afmm_handle* h, int on) {
   return AFMM_OK;
 }
 
+afmm_status afmm_shard_range(int nlevels, int index, int count, int* level, int64_t* k0, int64_t* k1) {
+  if (!level || !k0 || !k1) return AFMM_BAD_ARG;
+  int lev = 0;
+  long a = 0, b = 0;
+  if (!shard_range(nlevels, index, count, lev, a, b)) {
+    g_err = "afmm_shard_range: need 0 <= index < count and at least count leaves";
+    return AFMM_BAD_ARG;
+  }
+  *level = lev;
+  *k0 = a;
+  *k1 = b;
+  return AFMM_OK;
+}
+
+afmm_status afmm_set_shard(afmm_handle* h, int index, int count) {
+  if (!h) return AFMM_BAD_ARG;
+  return guard(h, [&] {
+    if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_set_shard before afmm_assemble"};
+    int lev = 0;
+    long a = 0, b = 0;
+    if (count < 1 || index < 0 || index >= count || (count > 1 && !shard_range(h->L, index, count, lev, a, b)))
+      throw Error{AFMM_BAD_ARG, "afmm_set_shard: need 0 <= index < count and at least count leaves"};
+    h->shard_index = index;
+    h->shard_count = count;
+    apply_shard(h);
+  });
+}
+
+afmm_status afmm_get_shard(afmm_handle* h, int* index, int* count, int* level) {
+  if (!h || !index || !count || !level) return AFMM_BAD_ARG;
+  *index = h->plan.shard_index;
+  *count = h->plan.shard_count;
+  *level = h->plan.shard_level;
+  return AFMM_OK;
+}
+
 afmm_status afmm_get_m2l_fixed_point(afmm_handle* h, int* stored) {
   if (!h || !stored) return AFMM_BAD_ARG;
   *stored = h->m2l_q_stored ? 1 : 0;
@@ -1951,6 +2043,7 @@ afmm_status afmm_set_create(afmm_handle* const* handles, int n, afmm_set** out) 
       if (!h->assembled) throw Error{AFMM_NOT_ASSEMBLED, "afmm_set_create: handle not assembled"};
       if (h->kernel_id != handles[0]->kernel_id) throw Error{AFMM_BAD_ARG, "afmm_set_create: mixed kernel ids"};
       if (!h->m2l_stored) throw Error{AFMM_BAD_ARG, "afmm_set_create: a handle has no stored M2L blocks"};
+      if (h->shard_count > 1) throw Error{AFMM_BAD_ARG, "afmm_set_create: a handle is sharded"};
       if (h->device != dev) throw Error{AFMM_BAD_ARG, "afmm_set_create: handle on another device"};
       probs.push_back({&h->plan, p2p_shape(h->plan.near.nmax)});
     }

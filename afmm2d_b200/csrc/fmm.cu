@@ -330,7 +330,7 @@ void sweep_m2m(const MatvecPlan& p, const double* qs, cudaStream_t s, int64_t* l
 
 void sweep_l2l(const MatvecPlan& p, double* ys, cudaStream_t s, int64_t* launches) {
   for (int j = 2; j <= p.L; ++j) {
-    const LevelView& v = p.lv[j];
+    const LevelView& v = p.lv_down[j];  // a shard's subtrees at the sharded levels
     if (v.nnodes == 0) continue;
     k_l2l_w<<<(int)((v.nnwgroups * 32 + 127) / 128), 128, 0, s>>>(v, j < p.L ? p.lv[j + 1].yhat : nullptr, ys,
                                                                   j == p.L);
@@ -346,7 +346,7 @@ void m2l_apply(const MatvecPlan& p, cudaStream_t s) {
     m2l_apply_otf(p, p.levels, s);
     return;
   }
-  LevelSet ls = p.levels;
+  LevelSet ls = p.levels_m2l;  // a shard's boxes at the sharded levels
   ls.pf_ahead = p.tune.pf_fp64;
   const long warps = ls.wgrp0[ls.nlev];
   k_m2l_apply_w<false><<<(int)((warps * 32 + 127) / 128), 128, 0, s>>>(ls);
@@ -369,6 +369,7 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   const int N = p.N;
   const int gb = (N + 255) / 256;
   if (tm) tm->mark(s, "gather");
+  if (p.shard_count > 1) AFMM_CUDA(cudaMemsetAsync(p.ys, 0, sizeof(double) * (size_t)N, s));
   k_gather<<<gb, 256, 0, s>>>(q, p.perm, N, p.qs);
   AFMM_LAUNCH_CHECK();
   ++*launches;
@@ -380,7 +381,7 @@ void matvec_fp64(const MatvecPlan& p, const double* q, double* y, cudaStream_t s
   if (tm) tm->mark(s, "l2l");
   sweep_l2l(p, p.ys, s, launches);
   if (tm) tm->mark(s, "p2p");
-  kernel_table(p.kp.id).p2p64(p.near, p.kp, p.qs, p.ys, s);
+  kernel_table(p.kp.id).p2p64(p.near_own, p.kp, p.qs, p.ys, s);
   ++*launches;
   if (tm) tm->mark(s, "scatter");
   k_scatter<<<gb, 256, 0, s>>>(p.ys, p.perm, N, y);

@@ -198,7 +198,8 @@ __device__ __forceinline__ double decode_q32(uint32_t u, double2 dec) {
 
 // Leaf-level data for the near field.
 struct NearView {
-  long nleaf = 0;
+  long nleaf = 0;  // leaves of the launch: leaf0 .. leaf0 + nleaf - 1 (a shard's range, else all)
+  long leaf0 = 0;
   int nmax = 0;
   const double2* pts = nullptr;        // sorted points
   const int32_t* leaf_start = nullptr; // quadtree order
@@ -257,7 +258,37 @@ struct MatvecPlan {
   LevelSet levels;       // levels 2..L for the M2L launch
   NearView near;
   Tuning tune;
+  // A shard of one problem (afmm_set_shard): the stored-block M2L and the
+  // L2L of the levels at and below shard_level, and the near field, run only
+  // over the shard's subtrees (contiguous box ranges); the gather, the M2M,
+  // the on-the-fly M2L and the upper levels run whole on every shard, and the
+  // potentials of points outside the shard come out as zeros.  Unsharded,
+  // these equal levels / lv / near.
+  int shard_index = 0, shard_count = 1, shard_level = 0;
+  LevelSet levels_m2l;
+  LevelView lv_down[kMaxLevels];
+  NearView near_own;
 };
+
+// Level and box range [k0, k1) of shard `index` of `count` on a tree of
+// levels 2..L: the shallowest level with at least four boxes per shard (the
+// deepest level when none has), boxes split evenly (a KD tree's boxes of one
+// level hold equal point counts).  Returns false when the tree has fewer
+// leaves than shards.
+inline bool shard_range(int L, int index, int count, int& level, long& k0, long& k1) {
+  if (count < 1 || index < 0 || index >= count || L < 2) return false;
+  level = L;
+  for (int j = 2; j <= L; ++j)
+    if ((1L << (2 * j)) >= 4L * count) {
+      level = j;
+      break;
+    }
+  const long nb = 1L << (2 * level);
+  if (nb < count) return false;
+  k0 = nb * index / count;
+  k1 = nb * (index + 1) / count;
+  return true;
+}
 
 // Near-field launch shape: NT threads per target group (targets rounded up to
 // a warp multiple), G groups splitting the (up to 9) source leaves.

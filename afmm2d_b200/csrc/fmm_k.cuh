@@ -45,7 +45,7 @@ template <class K>
 __global__ void k_p2p64(NearView nv, KernelParams kp, const double* __restrict__ qs, double* __restrict__ ys, int NT,
                         int G) {
   extern __shared__ __align__(16) unsigned char smem[];
-  p2p64_leaf<K>(nv, kp, qs, ys, NT, G, blockIdx.x, smem);
+  p2p64_leaf<K>(nv, kp, qs, ys, NT, G, nv.leaf0 + blockIdx.x, smem);
 }
 
 template <class K>

@@ -112,12 +112,13 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
                   cudaStream_t s, StageTimer* tm, int64_t* launches) {
   if (!ms.ready) throw Error{AFMM_BAD_ARG, "mixed precision operators are not set up"};
   const int N = p.N;
-  NearView nv = p.near;
+  NearView nv = p.near_own;
   nv.anchor = ms.leaf_anchor;
   nv.rel = ms.rel;
   nv.span = ms.leaf_span;
   for (int c = 0; c < nrhs; ++c) {
     if (tm) tm->mark(s, "gather");
+    if (p.shard_count > 1) AFMM_CUDA(cudaMemsetAsync(ms.ys, 0, sizeof(double) * (size_t)N, s));
     k_gather_mixed<<<nb(N, 256), 256, 0, s>>>(q + (long)c * ldq, p.perm, N, ms.qs, ms.qs32);
     AFMM_LAUNCH_CHECK();
     ++*launches;
@@ -130,7 +131,8 @@ void matvec_mixed(const MatvecPlan& p, MixedState& ms, const double* q, int64_t 
     const bool q32 = p.levels.nlev > 0 && p.levels.lv[0].m2l_q != nullptr;
     const bool stored = q32 || (p.levels.nlev > 0 && p.levels.lv[0].m2l != nullptr);
     const uint32_t otf = stored ? p.tune.otf_mixed : 0xffffffffu;
-    const LevelSet st = level_subset(p.levels, otf, false), fly = level_subset(p.levels, otf, true);
+    // a shard's boxes at the sharded levels for the stored form; the on-the-fly levels whole
+    const LevelSet st = level_subset(p.levels_m2l, otf, false), fly = level_subset(p.levels, otf, true);
     if (st.nlev > 0) {
       m2l_apply_stored(p, st, q32, s);
       ++*launches;

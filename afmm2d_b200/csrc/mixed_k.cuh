@@ -90,7 +90,7 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
   __shared__ float s_dx[9], s_dy[9], s_thr[9];
-  const long b = blockIdx.x;
+  const long b = nv.leaf0 + blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const float a32 = (float)kp.a, p32 = (float)kp.param;

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
   __shared__ float2 s_udel[kUnionMax];
   __shared__ unsigned char s_chleaf[kChunksMax], s_choff[kChunksMax], s_chfirst[kChunksMax];
   const int tid = threadIdx.x, warp = tid >> 5;
-  const long b1 = 2L * blockIdx.x, b2 = b1 + 1;
+  const long b1 = nv.leaf0 + 2L * blockIdx.x, b2 = b1 + 1;  // leaf0 is even
   const int n1 = nv.leaf_cnt[b1], n2 = nv.leaf_cnt[b2];
   const int s01 = nv.leaf_start[b1], s02 = nv.leaf_start[b2];
   const double2 a1 = nv.anchor[b1];
@@ -279,7 +279,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_p2p_tc(NearView nv, KernelParam
 template <class K>
 void p2p_tc_batched16(const NearView& nv, const KernelParams& kp, const uint2* qhl, double* ys, int L, int* err,
                       cudaStream_t s) {
-  if (nv.nmax > kLeafMax || (nv.nleaf & 1)) throw Error{AFMM_BAD_ARG, "tcgen05 near field takes leaves of <= 64 points"};
+  if (nv.nmax > kLeafMax || (nv.nleaf & 1) || (nv.leaf0 & 1))
+    throw Error{AFMM_BAD_ARG, "tcgen05 near field takes leaves of <= 64 points in sibling pairs"};
   allow_smem(k_p2p_tc<K>, kSmem);
   k_p2p_tc<K><<<(int)(nv.nleaf / 2), kThreads, kSmem, s>>>(nv, kp, qhl, ys, L, err);
   AFMM_LAUNCH_CHECK();

@@ -231,6 +231,24 @@ afmm_status afmm_measure_fma_peaks(double* fp64_tflops, double* fp32_tflops);
  * kernels.  Replaces no reference interface. */
 afmm_status afmm_measure_fp64_pipes(double* dmma_tflops, double* dfma_tflops, double* both_tflops);
 
+/* Sharding one problem over several GPUs (or processes): every shard holds
+ * the whole assembled problem (each process builds it; setup is
+ * deterministic, so the operators are identical), and afmm_set_shard(h,
+ * index, count) makes the handle's matvecs compute only the potentials of
+ * shard `index`'s points -- the points of its subtrees: the boxes [k0, k1) of
+ * the shallowest level with at least four boxes per shard, split evenly
+ * (afmm_shard_range) -- and write zeros for every other point, so that the
+ * sum of the shards' outputs (an all-reduce) is the whole product, bit for
+ * bit.  Per shard the M2L (stored blocks), the L2L at and below that level
+ * and the near field run over its subtrees only; the gather, the M2M, the
+ * upper levels and the on-the-fly M2L run whole.  After afmm_assemble;
+ * count = 1 restores the whole problem.  No reference counterpart (the
+ * reference is single-process, src/AFMM2DTree.cpp:1099-1225); handles in a
+ * set may not be sharded.  afmm_shard_range needs no device. */
+afmm_status afmm_set_shard(afmm_handle* h, int index, int count);
+afmm_status afmm_get_shard(afmm_handle* h, int* index, int* count, int* level);
+afmm_status afmm_shard_range(int nlevels, int index, int count, int* level, int64_t* k0, int64_t* k1);
+
 /* KD-tree permutation without any device allocation.  It has no counterpart
  * in the reference; it computes the same permutation as afmm_create /
  * afmm_get_permutation.  For callers that cannot allocate GPU memory: a

@@ -318,3 +318,40 @@ def test_tcgen05_integer_m2l(kernel, tol, wl):
     for c in (0, 7, 15):
         assert_rel(Yi[:, c], Ym[:, c], 1e-8)
         assert_rel(Yi[:, c], a.computeMatVecProduct(Q[:, c]), MIXED_TOL)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel,tol,wl", [("one_over_r", 6, "mixture4m"), ("log", 10, "uniform1m")])
+def test_sharded_matvec_sums_to_whole(kernel, tol, wl):
+    """afmm_set_shard: each shard computes its subtrees' potentials (zeros
+    elsewhere); the shards' outputs sum to the whole product bit for bit in
+    every precision, for even and uneven splits; count 1 restores it."""
+    pts, _, _ = workloads.make(wl, N=65536)
+    a = A.AFMM(65536, 64, tol, pts, kernel=kernel)
+    a.assemble()
+    Q = np.random.default_rng(9).standard_normal((65536, 16))
+    whole = {"fp64": a.computeMatVecProduct(Q[:, 3]), "mixed": a.computeMatVecProduct(Q[:, 3], precision="mixed"),
+             "batched": a.computeMatVecProduct(Q, precision="mixed"),
+             "fp64_batched": a.computeMatVecProduct(Q, precision="fp64_batched")}
+    for count in (2, 3, 5):
+        sums = {k: np.zeros_like(v) for k, v in whole.items()}
+        owned = np.zeros(65536, bool)
+        for i in range(count):
+            a.set_shard(i, count)
+            assert a.shard()[:2] == (i, count)
+            ys = {"fp64": a.computeMatVecProduct(Q[:, 3]),
+                  "mixed": a.computeMatVecProduct(Q[:, 3], precision="mixed"),
+                  "batched": a.computeMatVecProduct(Q, precision="mixed"),
+                  "fp64_batched": a.computeMatVecProduct(Q, precision="fp64_batched")}
+            mine = ys["fp64"] != 0
+            assert not (owned & mine).any()  # disjoint shards
+            owned |= mine
+            for k in ys:
+                sums[k] += ys[k]
+        assert owned.all()
+        for k in whole:
+            np.testing.assert_array_equal(sums[k], whole[k])
+    a.set_shard(0, 1)
+    np.testing.assert_array_equal(a.computeMatVecProduct(Q[:, 3]), whole["fp64"])
+    with pytest.raises(A.AFMMError):
+        a.set_shard(2, 2)

@@ -59,3 +59,28 @@ def test_reference_arm_runs_on_rank0_only():
     """, timeout=300)
     assert '"impl": "reference"' in outs[0]
     assert '"impl"' not in outs[1]
+
+
+def test_shard_outputs_combine_gloo():
+    """Sharding one problem: the ranks' partitions of the tree tile it, and
+    the all-reduce of outputs that are nonzero only on each rank's own part
+    gives the whole vector exactly (afmm2d_b200.shard.combine)."""
+    outs = run_ranks("""
+        import numpy as np, torch
+        import afmm2d_b200 as A
+        from afmm2d_b200 import shard
+        world = dist.get_world_size()
+        lev, k0, k1 = A.shard_range(6, rank, world)
+        got = [None] * world
+        dist.all_gather_object(got, (lev, k0, k1))
+        assert all(g[0] == lev for g in got) and got[0][1] == 0 and got[-1][2] == 4 ** lev
+        assert all(got[i][2] == got[i + 1][1] for i in range(world - 1))
+        full = np.random.default_rng(5).standard_normal(4 ** lev * 7)
+        part = np.zeros_like(full)
+        part[k0 * 7:k1 * 7] = full[k0 * 7:k1 * 7]
+        t = shard.combine(torch.from_numpy(part))
+        assert np.array_equal(t.numpy(), full)
+        print("RESULT ok", lev, k0, k1)
+    """)
+    for o in outs:
+        assert "RESULT ok" in o
