@@ -36,4 +36,4 @@ class ShardedMatvec:
         """y = K q for device tensors holding nrhs columns of N values each
         (column-major: column c at offset c * N), on every rank."""
         self.afmm.matvec_device(q.data_ptr(), y.data_ptr(), nrhs, self.afmm.N, precision)  # returns when done
-        return combine(y, self.group)
+        return combine(y, self.group) if self.world > 1 else y

@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--profile-once", action="store_true", help="only run setup + 2 matvecs (for ncu)")
     ap.add_argument("--tuning", default="auto", choices=["auto", "default"],
                     help="auto: run the library's autotuner during setup (default); default: built-in parameters")
+    ap.add_argument("--shard", action="store_true",
+                    help="under torchrun: one problem split over the ranks by subtrees (strong scaling) instead of "
+                         "one replica per rank")
     ap.add_argument("--set", action="append", default=[], metavar="KEY=VALUE",
                     help="tuning value applied after --tuning (repeatable; keys as AFMM.tuning(), e.g. p2p_tc=1)")
     return ap.parse_args()
@@ -630,12 +633,110 @@ def run_many(args):
     st.close()
 
 
+def run_sharded(args):
+    """--shard: one problem over all ranks.  Every rank builds the whole
+    problem, computes its subtrees' share of each 16-RHS mixed matvec
+    (afmm_set_shard) and one NCCL all-reduce sums the shards; value = N * nrhs
+    / the max over ranks of the step time (strong scaling: the work is the
+    problem's whatever the rank count).  e2e adds the host copies of the
+    charges (every rank) and of the result."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import afmm2d_b200 as A
+    from afmm2d_b200 import shard, workloads
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:  # one shard: the whole problem through the same code
+        dist.init_process_group("gloo", init_method="file://" + tempfile.mktemp(), rank=0, world_size=1)
+    R = args.nrhs
+    pts, q, p = workloads.make(args.workload, N=args.N)
+    N = len(pts)
+    Q = np.random.Generator(np.random.PCG64(p["seed"] + 1)).standard_normal((N, R))
+    t0 = time.perf_counter()
+    a = A.AFMM(N, p["M"], p["tol"], pts, kernel=p["kernel"])
+    a.assemble()
+    setup_s = time.perf_counter() - t0
+    if args.tuning == "auto":
+        a.autotune()
+    overrides = tuning_overrides(args)
+    if overrides:
+        a.set_tuning(**overrides)
+    sm = shard.ShardedMatvec(a)
+    dev = f"cuda:{local}"
+    hQ = torch.from_numpy(np.asfortranarray(Q).T.copy()).pin_memory()
+    hY = torch.empty_like(hQ).pin_memory()
+    dQ = hQ.to(dev)
+    dY = torch.empty_like(dQ)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        dist.barrier()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms))
+
+    clk = ClockSampler(local)
+    clk.start()
+    t_dev = timed(lambda: sm.matvec_device(dQ, dY, R, "mixed"))
+
+    def e2e_step():
+        dQ.copy_(hQ, non_blocking=True)
+        sm.matvec_device(dQ, dY, R, "mixed")
+        hY.copy_(dY, non_blocking=True)
+
+    t_e2e = timed(e2e_step)
+    clocks = clk.stop()
+    t_dev, t_e2e = max_over_ranks([t_dev, t_e2e], dist if world > 1 else None, dev)
+    # the sharded product against this rank's whole one (rank 0 checks)
+    err = None
+    if rank == 0:
+        a.set_shard(0, 1)
+        whole = torch.empty_like(dQ)
+        a.matvec_device(dQ.data_ptr(), whole.data_ptr(), R, N, "mixed")
+        err = float(torch.max(torch.abs(whole - dY)).item())
+    lev = A.shard_range(a.nLevels, rank, world)[0]
+    line = {"metric": metric_name(args.workload, N, p, R), "value": N * R / (t_dev * 1e-3), "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_dev,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "N": N, "kernel": p["kernel"], "M": p["M"], "TOL_POW": p["tol"],
+                       "nrhs": R, "precision": "mixed, batched", "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"one problem in {world} subtree shards (level {lev}) + all-reduce"},
+            "max_abs_diff_sharded_vs_whole": err, "setup_s": setup_s, "clocks": clocks, "roofline": None,
+            "gpu_launches": None,
+            "e2e": {"value": N * R / (t_e2e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 8 * N * R,
+                    "d2h_bytes_per_step": 8 * N * R, "ms_per_step": t_e2e}}
+    dist.barrier()
+    dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    a.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "many":
         run_many(args)
+    elif args.shard:
+        run_sharded(args)
     else:
         run_ours(args)
 
