@@ -1389,11 +1389,31 @@ void do_autotune(afmm_handle* h, int what) {
       if (of_ms < 0.97f * st_ms) om |= 1u << t;
       MatvecPlan pc = p;
       pc.levels = one;
+      pc.levels_m2l = one;  // (unsharded views while tuning)
       pc.tune.otf_batched = 0;
       const float sb = time_ms(s, reps, [&] { m2l_batched(pc, h->batch, R, 0, s); });
       pc.tune.otf_batched = 0xffffffffu;
       const float fb = time_ms(s, reps, [&] { m2l_batched(pc, h->batch, R, 0, s); });
       if (fb < 0.97f * sb) ob |= 1u << t;
+    }
+    // the masks as a whole against all stored: per-level timings miss how
+    // the levels share the GPU inside one launch, so keep a mask only when
+    // the combined launch confirms it
+    if (om) {
+      const LevelSet st = level_subset(p.levels, om, false), fly = level_subset(p.levels, om, true);
+      const float mask_ms = time_ms(s, reps, [&] {
+        m2l_apply_stored(p, st, q32, s);
+        m2l_apply_otf(p, fly, s);
+      });
+      const float all_ms = time_ms(s, reps, [&] { m2l_apply_stored(p, p.levels, q32, s); });
+      if (!(mask_ms < 0.97f * all_ms)) om = 0;
+    }
+    if (ob) {
+      p.tune.otf_batched = ob;
+      const float mask_ms = time_ms(s, reps, [&] { m2l_batched(p, h->batch, R, 0, s); });
+      p.tune.otf_batched = 0;
+      const float all_ms = time_ms(s, reps, [&] { m2l_batched(p, h->batch, R, 0, s); });
+      if (!(mask_ms < 0.97f * all_ms)) ob = 0;
     }
     p.tune.otf_mixed = om;
     p.tune.otf_batched = ob;

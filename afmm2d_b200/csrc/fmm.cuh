@@ -320,6 +320,8 @@ __device__ __forceinline__ void m2m_row(const LevelView& v, const double* __rest
   const double* P = v.l2p_rm + v.l2p_off[b] + c;  // (i, c) at i*r + c
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   int i = 0;
+  // (unrolled: more loads in flight; each partial sum keeps its order)
+#pragma unroll 4
   for (; i + 3 < n; i += 4) {
     a0 += P[(long)i * r] * src[i];
     a1 += P[(long)(i + 1) * r] * src[i + 1];
@@ -372,6 +374,7 @@ __device__ __forceinline__ void l2l_row(const LevelView& v, double* __restrict__
   const double* yb = v.yhat + v.skel_off[b];
   double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
   int c = 0;
+#pragma unroll 4
   for (; c + 3 < r; c += 4) {
     a0 += P[(long)c * n] * yb[c];
     a1 += P[(long)(c + 1) * n] * yb[c + 1];
