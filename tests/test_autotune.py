@@ -81,4 +81,4 @@ def test_set_tuning_values_and_forms():
     assert A.lib().afmm_set_tuning(a._h, v.ctypes.data_as(ctypes.c_void_p), 7) == 0
     assert a.tuning()["m2l_tc"] == 1
     with pytest.raises(A.AFMMError):
-        a.set_tuning(m2l_tc=2)
+        a.set_tuning(m2l_tc=3)
