@@ -1649,6 +1649,7 @@ afmm_status afmm_eval_error(afmm_handle* h, int nsample, uint64_t seed, double* 
   if (!h || !rel_err) return AFMM_BAD_ARG;
   return guard(h, [&] {
     if (!h->have_last) throw Error{AFMM_BAD_ARG, "no FP64 matvec has been computed yet"};
+    if (h->plan.shard_count > 1) throw Error{AFMM_BAD_ARG, "afmm_eval_error on a sharded handle (its output is partial)"};
     const long nleaf = h->lv[h->L].nbox;
     std::vector<long> leaves;
     if (nsample <= 0 || nsample >= nleaf) {
