@@ -35,7 +35,7 @@ namespace {
 // With RC >= 8 the row is also written as interleaved TF32 high / low parts
 // (the tensor-core near field's charges), otherwise as FP32; neither when the
 // pass is FP64 throughout.
-constexpr int kTileJ = 64;
+constexpr int kTileJ = 128;
 
 template <int RC>
 __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols,
