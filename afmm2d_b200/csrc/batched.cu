@@ -72,16 +72,25 @@ __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, 
 // Scatter through a shared-memory transpose: a block takes kTileJ consecutive
 // points, reads their sorted rows ys[iperm[j]][0:RC], and writes each column
 // of y as one contiguous run.
+// With ys_near, the near field's potentials are added to the far field's
+// (the one addition the near-field kernels would have made into ys).
 template <int RC>
-__global__ void __launch_bounds__(256) k_scatter_b(const double* __restrict__ ys, const int32_t* __restrict__ iperm,
-                                                   int N, int ncols, double* y, int64_t ldy) {
+__global__ void __launch_bounds__(256) k_scatter_b(const double* __restrict__ ys, const double* __restrict__ ys_near,
+                                                   const int32_t* __restrict__ iperm, int N, int ncols, double* y,
+                                                   int64_t ldy) {
   __shared__ double tile[RC][kTileJ + 1];
   const long j0 = (long)blockIdx.x * kTileJ;
   for (int idx = threadIdx.x; idx < (RC / 2) * kTileJ; idx += blockDim.x) {
     const int jj = idx / (RC / 2), cp = idx % (RC / 2);
     const long j = j0 + jj;
     if (j >= N) continue;
-    const double2 v = *reinterpret_cast<const double2*>(ys + (long)iperm[j] * RC + 2 * cp);
+    const long o = (long)iperm[j] * RC + 2 * cp;
+    double2 v = *reinterpret_cast<const double2*>(ys + o);
+    if (ys_near) {
+      const double2 w = *reinterpret_cast<const double2*>(ys_near + o);
+      v.x += w.x;
+      v.y += w.y;
+    }
     tile[2 * cp][jj] = v.x;
     tile[2 * cp + 1][jj] = v.y;
   }
@@ -697,17 +706,20 @@ struct Pass {
   // Near field of the pass: the mixed 16-column form on tcgen05 tiles when
   // tuned so (leaves of at most 64 points), else mma.sync tiles (TF32x3 in
   // mixed precision, FP64 in FP64-batched passes), FMA for 4 columns.
-  static void p2p(const MatvecPlan& p, BatchState& bs, const NearView& nv, int fp64, cudaStream_t s) {
+  // (adds into ys_out)
+  static void p2p(const MatvecPlan& p, BatchState& bs, const NearView& nv, int fp64, cudaStream_t s,
+                  double* ys_out = nullptr) {
     const KernelTable& kt = kernel_table(p.kp.id);
+    double* ys = ys_out ? ys_out : bs.ys;
     if (RC == 16 && !fp64 && p.tune.p2p_tc && nv.nmax <= 64 && bs.err_dev) {
-      kt.p2p_tc16(nv, p.kp, bs.qhl, bs.ys, p.L, bs.err_dev, s);
+      kt.p2p_tc16(nv, p.kp, bs.qhl, ys, p.L, bs.err_dev, s);
     } else if (fp64) {
       if (RC < 8) throw Error{AFMM_BAD_ARG, "FP64 batched passes take 8 or 16 columns"};
-      kt.p2p_dmma[RC == 16](nv, p.kp, bs.qs, bs.ys, s);
+      kt.p2p_dmma[RC == 16](nv, p.kp, bs.qs, ys, s);
     } else if (RC >= 8) {
-      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, bs.ys, s);
+      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, ys, s);
     } else {
-      kt.p2p_b4(nv, p.kp, bs.qs32, bs.ys, s);
+      kt.p2p_b4(nv, p.kp, bs.qs32, ys, s);
     }
   }
 
@@ -722,6 +734,18 @@ struct Pass {
     k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl, fp64);
     AFMM_LAUNCH_CHECK();
     ++*launches;
+    // the near field does not depend on the far field: it runs on its own
+    // lower-priority stream into ys_near, filling what the far-field
+    // kernels leave of the GPU
+    const bool overlap = bs.s_near != nullptr;
+    if (overlap) {
+      AFMM_CUDA(cudaEventRecord(bs.ev_q, s));
+      AFMM_CUDA(cudaStreamWaitEvent(bs.s_near, bs.ev_q, 0));
+      AFMM_CUDA(cudaMemsetAsync(bs.ys_near, 0, sizeof(double) * (size_t)N * RC, bs.s_near));
+      p2p(p, bs, nv, fp64, bs.s_near, bs.ys_near);
+      AFMM_CUDA(cudaEventRecord(bs.ev_near, bs.s_near));
+      ++*launches;
+    }
     if (tm) tm->mark(s, "m2m");
     for (int j = p.L; j >= 2; --j) {
       const LevelView& v = p.lv[j];
@@ -759,11 +783,16 @@ struct Pass {
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
+    // (overlapped: the "p2p" stage is the wait for the near field's end)
     if (tm) tm->mark(s, "p2p");
-    p2p(p, bs, nv, fp64, s);
-    ++*launches;
+    if (overlap) {
+      AFMM_CUDA(cudaStreamWaitEvent(s, bs.ev_near, 0));
+    } else {
+      p2p(p, bs, nv, fp64, s);
+      ++*launches;
+    }
     if (tm) tm->mark(s, "scatter");
-    k_scatter_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(bs.ys, p.iperm, N, ncols, y, ldy);
+    k_scatter_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(bs.ys, overlap ? bs.ys_near : nullptr, p.iperm, N, ncols, y, ldy);
     AFMM_LAUNCH_CHECK();
     ++*launches;
   }
@@ -813,6 +842,12 @@ void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStr
     hq[t] = bs.qhat[t + 2];
     hy[t] = bs.yhat[t + 2];
   }
+  bs.ys_near = arena.alloc<double>((size_t)p.N * RC);
+  int least = 0, greatest = 0;  // the near field's stream at the lowest priority
+  AFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  AFMM_CUDA(cudaStreamCreateWithPriority(&bs.s_near, cudaStreamNonBlocking, least));
+  AFMM_CUDA(cudaEventCreateWithFlags(&bs.ev_q, cudaEventDisableTiming));
+  AFMM_CUDA(cudaEventCreateWithFlags(&bs.ev_near, cudaEventDisableTiming));
   AFMM_CUDA(cudaHostAlloc((void**)&bs.err_host, sizeof(int), cudaHostAllocMapped));
   *bs.err_host = 0;
   AFMM_CUDA(cudaHostGetDevicePointer((void**)&bs.err_dev, bs.err_host, 0));

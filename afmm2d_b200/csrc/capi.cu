@@ -426,7 +426,11 @@ void create_layout(afmm_handle* h);
 // Streams and events of a handle (afmm_create, afmm_load).
 void create_streams(afmm_handle* h) {
   AFMM_CUDA(cudaGetDevice(&h->device));
-  AFMM_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  // the handle's stream at the highest priority: batched passes run their
+  // near field beside the far field on a lowest-priority stream
+  int least = 0, greatest = 0;
+  AFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  AFMM_CUDA(cudaStreamCreateWithPriority(&h->stream, cudaStreamNonBlocking, greatest));
   AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_h2d, cudaStreamNonBlocking));
   AFMM_CUDA(cudaStreamCreateWithFlags(&h->s_d2h, cudaStreamNonBlocking));
   for (cudaEvent_t* e : {&h->ev_in[0], &h->ev_in[1], &h->ev_done[0], &h->ev_done[1], &h->ev_out[0], &h->ev_out[1],

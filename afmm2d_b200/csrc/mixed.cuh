@@ -37,8 +37,16 @@ struct BatchState {
   double** d_yhat_lv = nullptr;
   int* err_host = nullptr;  // host-mapped flag set by a kernel whose bounded wait gave up
   int* err_dev = nullptr;   // its device address
+  // The near field runs on its own lower-priority stream beside the far
+  // field, into ys_near (zeroed per pass); the scatter adds it to ys.
+  double* ys_near = nullptr;
+  cudaStream_t s_near = nullptr;
+  cudaEvent_t ev_q = nullptr, ev_near = nullptr;
   ~BatchState() {
     if (err_host) cudaFreeHost(err_host);
+    if (ev_q) cudaEventDestroy(ev_q);
+    if (ev_near) cudaEventDestroy(ev_near);
+    if (s_near) cudaStreamDestroy(s_near);
   }
 };
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s);
