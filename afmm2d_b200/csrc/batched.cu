@@ -742,7 +742,9 @@ struct Pass {
       AFMM_CUDA(cudaEventRecord(bs.ev_q, s));
       AFMM_CUDA(cudaStreamWaitEvent(bs.s_near, bs.ev_q, 0));
       AFMM_CUDA(cudaMemsetAsync(bs.ys_near, 0, sizeof(double) * (size_t)N * RC, bs.s_near));
+      const int sp = tm ? tm->span_begin(bs.s_near, "p2p_kernel") : -1;  // the kernel's own duration
       p2p(p, bs, nv, fp64, bs.s_near, bs.ys_near);
+      if (tm) tm->span_end(bs.s_near, sp);
       AFMM_CUDA(cudaEventRecord(bs.ev_near, bs.s_near));
       ++*launches;
     }

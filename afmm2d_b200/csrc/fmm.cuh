@@ -214,7 +214,29 @@ struct NearView {
 struct StageTimer {
   std::vector<std::pair<std::string, cudaEvent_t>> marks;
   size_t used = 0;
-  void reset() { used = 0; }
+  // spans timed on another stream (a stage that overlaps the marked ones)
+  struct Span {
+    std::string name;
+    cudaEvent_t b, e;
+  };
+  std::vector<Span> spans;
+  size_t nspans = 0;
+  void reset() {
+    used = 0;
+    nspans = 0;
+  }
+  int span_begin(cudaStream_t s, const char* name) {
+    if (nspans == spans.size()) {
+      Span sp{name, nullptr, nullptr};
+      cudaEventCreate(&sp.b);
+      cudaEventCreate(&sp.e);
+      spans.push_back(sp);
+    }
+    spans[nspans].name = name;
+    cudaEventRecord(spans[nspans].b, s);
+    return (int)nspans++;
+  }
+  void span_end(cudaStream_t s, int i) { cudaEventRecord(spans[(size_t)i].e, s); }
   void mark(cudaStream_t s, const char* name) {
     if (used == marks.size()) {
       cudaEvent_t e;
@@ -239,9 +261,24 @@ struct StageTimer {
         }
       if (!found) out.push_back({marks[i].first, ms});
     }
+    for (size_t i = 0; i < nspans; ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, spans[i].b, spans[i].e);
+      bool found = false;
+      for (auto& o : out)
+        if (o.first == spans[i].name) {
+          o.second += ms;
+          found = true;
+        }
+      if (!found) out.push_back({spans[i].name, ms});
+    }
   }
   ~StageTimer() {
     for (auto& m : marks) cudaEventDestroy(m.second);
+    for (auto& sp : spans) {
+      cudaEventDestroy(sp.b);
+      cudaEventDestroy(sp.e);
+    }
   }
 };
 
