@@ -394,7 +394,9 @@ class AFMM:
         _check(lib().afmm_set_tuning(self._h, _ptr(v), len(v)), self._h)
 
     def set_profiling(self, on=True):
-        _check(lib().afmm_set_profiling(self._h, 1 if on else 0), self._h)
+        """True / 1: per-stage CUDA events; 2: the same with the batched near
+        field run after the far field (each stage its kernels' own time)."""
+        _check(lib().afmm_set_profiling(self._h, int(on)), self._h)
 
     def stage_times(self):
         """Per-stage device milliseconds of the last matvec (profiling on)."""

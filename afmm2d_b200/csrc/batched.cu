@@ -31,16 +31,15 @@ namespace {
 
 // Gather through a shared-memory transpose: a block takes kTileJ consecutive
 // points, reads each column of q as one contiguous run, and writes each
-// point's sorted row qs[iperm[j]][0:RC] (one 128-byte line for RC = 16).
-// With RC >= 8 the row is also written as interleaved TF32 high / low parts
-// (the tensor-core near field's charges), otherwise as FP32; neither when the
-// pass is FP64 throughout.
+// point's sorted row qs[iperm[j]][0:RC] (one 128-byte line for RC = 16),
+// and also as interleaved TF32 high / low parts (the tensor-core near
+// field's charges) unless the pass is FP64 throughout.
 constexpr int kTileJ = 128;
 
 template <int RC>
 __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, int64_t ldq, int ncols,
-                                                  const int32_t* __restrict__ iperm, int N, double* qs, float* qs32,
-                                                  uint2* qhl, int fp64_only) {
+                                                  const int32_t* __restrict__ iperm, int N, double* qs, uint2* qhl,
+                                                  int fp64_only) {
   __shared__ double tile[RC][kTileJ + 1];
   const long j0 = (long)blockIdx.x * kTileJ;
   for (int idx = threadIdx.x; idx < RC * kTileJ; idx += blockDim.x) {
@@ -57,15 +56,10 @@ __global__ void __launch_bounds__(256) k_gather_b(const double* __restrict__ q, 
     const long d = (long)iperm[j] * RC + 2 * cp;
     *reinterpret_cast<double2*>(qs + d) = make_double2(v0, v1);
     if (fp64_only) continue;
-    const float f0 = (float)v0, f1 = (float)v1;
-    if (RC >= 8) {
-      uint4 hl;
-      split_tf32(f0, hl.x, hl.y);
-      split_tf32(f1, hl.z, hl.w);
-      *reinterpret_cast<uint4*>(qhl + d) = hl;
-    } else {
-      *reinterpret_cast<float2*>(qs32 + d) = make_float2(f0, f1);
-    }
+    uint4 hl;
+    split_tf32((float)v0, hl.x, hl.y);
+    split_tf32((float)v1, hl.z, hl.w);
+    *reinterpret_cast<uint4*>(qhl + d) = hl;
   }
 }
 
@@ -99,65 +93,6 @@ __global__ void __launch_bounds__(256) k_scatter_b(const double* __restrict__ ys
     const int c = idx / kTileJ, jj = idx % kTileJ;
     const long j = j0 + jj;
     if (c < ncols && j < N) y[(long)c * ldy + j] = tile[c][jj];
-  }
-}
-
-// M2M: one thread per output row; qhat[row] = sum_i L2P[i][c] src[i].
-template <int RC>
-__global__ void k_m2m_b(LevelView v, const double* __restrict__ src_all, int leaf, double* qhat) {
-  const long row = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (row >= v.nrows) return;
-  const int b = v.skel_box[row];
-  const int r = v.rank[b];
-  const int c = (int)(row - v.skel_off[b]);
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const double* src = src_all + (long)(leaf ? v.leaf_start[b] : v.node_off[b]) * RC;
-  const double* P = v.l2p_rm + v.l2p_off[b] + c;
-  double acc[RC];
-#pragma unroll
-  for (int k = 0; k < RC; ++k) acc[k] = 0.0;
-  for (int i = 0; i < n; ++i) {
-    const double p = P[(long)i * r];
-    double s[RC];
-    load_vec<RC>(src + (long)i * RC, s);
-#pragma unroll
-    for (int k = 0; k < RC; ++k) acc[k] = fma(p, s[k], acc[k]);
-  }
-  store_vec<RC>(qhat + row * RC, acc);
-}
-
-// L2L: one thread per node row; child incoming potential += L2P yhat, or the
-// leaf potential = L2P yhat.
-template <int RC>
-__global__ void k_l2l_b(LevelView v, const double* __restrict__ yhat, double* __restrict__ child_yhat,
-                        double* __restrict__ ys, int leaf) {
-  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= v.nnodes) return;
-  const int b = v.node_box[g];
-  const int r = v.rank[b];
-  const int n = v.node_off[b + 1] - v.node_off[b];
-  const int i = (int)(g - v.node_off[b]);
-  const double* P = v.l2p + v.l2p_off[b] + i;
-  const double* yb = yhat + (long)v.skel_off[b] * RC;
-  double acc[RC];
-#pragma unroll
-  for (int k = 0; k < RC; ++k) acc[k] = 0.0;
-  for (int c = 0; c < r; ++c) {
-    const double p = P[(long)c * n];
-    double yv[RC];
-    load_vec<RC>(yb + (long)c * RC, yv);
-#pragma unroll
-    for (int k = 0; k < RC; ++k) acc[k] = fma(p, yv[k], acc[k]);
-  }
-  if (leaf) {
-    store_vec<RC>(ys + (long)(v.leaf_start[b] + i) * RC, acc);
-  } else {
-    double* out = child_yhat + g * RC;
-    double cur[RC];
-    load_vec<RC>(out, cur);
-#pragma unroll
-    for (int k = 0; k < RC; ++k) cur[k] += acc[k];
-    store_vec<RC>(out, cur);
   }
 }
 
@@ -648,16 +583,16 @@ inline int sm_count() {
 
 template <int RC>
 struct Pass {
+  static_assert(RC == 8 || RC == 16, "passes of 8 or 16 columns (tensor-core tiles)");
   // M2L of every level: the stored blocks (fixed point in mixed precision,
   // FP64 otherwise; kernel-independent), or the entries on the fly (the
   // kernel's table)
   // (the levels of the tuning mask, in mixed precision, on the fly as well)
   static int m2l(const MatvecPlan& p, const double* const* qh, double* const* yh, int fp64, int* err,
                  cudaStream_t s) {
-    constexpr int RM = RC >= 8 ? RC : 8;
     if (p.levels.row0[p.levels.nlev] == 0) return 0;  // every box of ACA rank 0: no far field
-    const bool q32 = RC >= 8 && !fp64 && p.levels.lv[0].m2l_q != nullptr;
-    const bool stored = RC >= 8 && (q32 || p.levels.lv[0].m2l != nullptr);
+    const bool q32 = !fp64 && p.levels.lv[0].m2l_q != nullptr;
+    const bool stored = q32 || p.levels.lv[0].m2l != nullptr;
     const uint32_t otf = !stored ? 0xffffffffu : (fp64 ? 0u : p.tune.otf_batched);
     LevelSet st = level_subset(p.levels_m2l, otf, false);  // a shard's boxes at the sharded levels
     const LevelSet fly = level_subset(p.levels, otf, true);
@@ -688,16 +623,15 @@ struct Pass {
         if (q32) k_m2l_stored_mma_t16<true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
         else k_m2l_stored_mma_t16<false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       } else if (q32) {
-        k_m2l_stored_mma<RM, true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+        k_m2l_stored_mma<RC, true><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       } else {
-        k_m2l_stored_mma<RM, false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
+        k_m2l_stored_mma<RC, false><<<nbk(warps * 32, 128), 128, 0, s>>>(st, qh, yh);
       }
       AFMM_LAUNCH_CHECK();
       ++n;
     }
     if (fly.nlev > 0 && fly.row0[fly.nlev] > 0) {
-      if (RC >= 8) kernel_table(p.kp.id).m2l_otf_mma[RC == 16](fly, p.kp, qh, yh, s);
-      else kernel_table(p.kp.id).m2l_otf_b4(fly, p.kp, qh, yh, s);
+      kernel_table(p.kp.id).m2l_otf_mma[RC == 16](fly, p.kp, qh, yh, s);
       ++n;
     }
     return n;
@@ -705,7 +639,7 @@ struct Pass {
 
   // Near field of the pass: the mixed 16-column form on tcgen05 tiles when
   // tuned so (leaves of at most 64 points), else mma.sync tiles (TF32x3 in
-  // mixed precision, FP64 in FP64-batched passes), FMA for 4 columns.
+  // mixed precision, FP64 in FP64-batched passes).
   // (adds into ys_out)
   static void p2p(const MatvecPlan& p, BatchState& bs, const NearView& nv, int fp64, cudaStream_t s,
                   double* ys_out = nullptr) {
@@ -714,30 +648,26 @@ struct Pass {
     if (RC == 16 && !fp64 && p.tune.p2p_tc && nv.nmax <= 64 && bs.err_dev) {
       kt.p2p_tc16(nv, p.kp, bs.qhl, ys, p.L, bs.err_dev, s);
     } else if (fp64) {
-      if (RC < 8) throw Error{AFMM_BAD_ARG, "FP64 batched passes take 8 or 16 columns"};
       kt.p2p_dmma[RC == 16](nv, p.kp, bs.qs, ys, s);
-    } else if (RC >= 8) {
-      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, ys, s);
     } else {
-      kt.p2p_b4(nv, p.kp, bs.qs32, ys, s);
+      kt.p2p_mma[RC == 16](nv, p.kp, bs.qhl, ys, s);
     }
   }
 
   static void run(const MatvecPlan& p, BatchState& bs, const NearView& nv, const double* q, int64_t ldq, double* y,
                   int64_t ldy, int ncols, int fp64, cudaStream_t s, StageTimer* tm, int64_t* launches) {
-    constexpr int RM = RC >= 8 ? RC : 8;
     const int N = p.N;
     if (p.shard_count > 1) {  // points outside the shard's leaves come out as zeros
       AFMM_CUDA(cudaMemsetAsync(bs.ys, 0, sizeof(double) * (size_t)N * RC, s));
     }
     if (tm) tm->mark(s, "gather");
-    k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qs32, bs.qhl, fp64);
+    k_gather_b<RC><<<nbk(N, kTileJ), 256, 0, s>>>(q, ldq, ncols, p.iperm, N, bs.qs, bs.qhl, fp64);
     AFMM_LAUNCH_CHECK();
     ++*launches;
     // the near field does not depend on the far field: it runs on its own
     // lower-priority stream into ys_near, filling what the far-field
-    // kernels leave of the GPU
-    const bool overlap = bs.s_near != nullptr;
+    // kernels leave of the GPU (after the far field when profiling serially)
+    const bool overlap = bs.s_near != nullptr && !(tm && tm->serial);
     if (overlap) {
       AFMM_CUDA(cudaEventRecord(bs.ev_q, s));
       AFMM_CUDA(cudaStreamWaitEvent(bs.s_near, bs.ev_q, 0));
@@ -753,16 +683,13 @@ struct Pass {
       const LevelView& v = p.lv[j];
       if (v.nrows == 0) continue;
       const double* src = j == p.L ? bs.qs : bs.qhat[j + 1];
-      const int sw = RC >= 8 ? split_warps(v.ncgroups, true) : 0;
+      const int sw = split_warps(v.ncgroups, true);
       if (sw == 8)
-        k_m2m_mma_split<RM, 8><<<(int)v.ncgroups, 256, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
+        k_m2m_mma_split<RC, 8><<<(int)v.ncgroups, 256, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
       else if (sw == 2)
-        k_m2m_mma_split<RM, 2><<<(int)v.ncgroups, 64, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
-      else if (RC >= 8)
-        k_m2m_mma<RM><<<nbk(v.ncgroups * 32, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L,
-                                                               bs.qhat[j]);
+        k_m2m_mma_split<RC, 2><<<(int)v.ncgroups, 64, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
       else
-        k_m2m_b<RC><<<nbk(v.nrows, 128), 128, 0, s>>>(v, j == p.L ? bs.qs : bs.qhat[j + 1], j == p.L, bs.qhat[j]);
+        k_m2m_mma<RC><<<nbk(v.ncgroups * 32, 128), 128, 0, s>>>(v, src, j == p.L, bs.qhat[j]);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
@@ -773,15 +700,12 @@ struct Pass {
       const LevelView& v = p.lv_down[j];  // a shard's subtrees at the sharded levels
       if (v.nnodes == 0) continue;
       // the split follows the whole level, so a shard's rows get the same bits
-      if (RC >= 8 && split_warps(p.lv[j].nncgroups, false) == 8)
-        k_l2l_mma_split<RM, 8><<<(int)v.nncgroups, 256, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
-                                                                bs.ys, j == p.L);
-      else if (RC >= 8)
-        k_l2l_mma<RM><<<nbk(v.nncgroups * 32, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
+      if (split_warps(p.lv[j].nncgroups, false) == 8)
+        k_l2l_mma_split<RC, 8><<<(int)v.nncgroups, 256, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
                                                                 bs.ys, j == p.L);
       else
-        k_l2l_b<RC><<<nbk(v.nnodes, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr, bs.ys,
-                                                       j == p.L);
+        k_l2l_mma<RC><<<nbk(v.nncgroups * 32, 128), 128, 0, s>>>(v, bs.yhat[j], j < p.L ? bs.yhat[j + 1] : nullptr,
+                                                                bs.ys, j == p.L);
       AFMM_LAUNCH_CHECK();
       ++*launches;
     }
@@ -808,8 +732,7 @@ int p2p_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, int rc, int
   nv.rel = ms.rel;
   nv.span = ms.leaf_span;
   if (rc == 16) Pass<16>::p2p(p, bs, nv, fp64, s);
-  else if (rc == 8) Pass<8>::p2p(p, bs, nv, fp64, s);
-  else Pass<4>::p2p(p, bs, nv, fp64, s);
+  else Pass<8>::p2p(p, bs, nv, fp64, s);
   return 1;
 }
 
@@ -821,18 +744,14 @@ void m2l_slice(const LevelView& v, cudaStream_t s) {
 
 int m2l_batched(const MatvecPlan& p, BatchState& bs, int rc, int fp64, cudaStream_t s) {
   if (rc == 16) return Pass<16>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
-  if (rc == 8) return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
-  return Pass<4>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
+  return Pass<8>::m2l(p, bs.d_qhat_lv, bs.d_yhat_lv, fp64, bs.err_dev, s);
 }
 
 void batch_reserve(const MatvecPlan& p, BatchState& bs, DevArena& arena, cudaStream_t s) {
   if (bs.ready) return;
   const int RC = kBatchMax;
   bs.qs = arena.alloc<double>((size_t)p.N * RC);
-  // FP32 charges (passes of fewer than 8 columns) and TF32 parts (8 or more)
-  // are never needed by the same pass: one buffer holds either
-  bs.qhl = arena.alloc<uint2>((size_t)p.N * RC);
-  bs.qs32 = reinterpret_cast<float*>(bs.qhl);
+  bs.qhl = arena.alloc<uint2>((size_t)p.N * RC);  // TF32 parts of the mixed near field
   bs.ys = arena.alloc<double>((size_t)p.N * RC);
   std::vector<const double*> hq(kMaxLevels, nullptr);
   std::vector<double*> hy(kMaxLevels, nullptr);
@@ -870,14 +789,15 @@ void matvec_batched(const MatvecPlan& p, MixedState& ms, BatchState& bs, const d
   nv.span = ms.leaf_span;
   for (int c0 = 0; c0 < nrhs;) {
     const int left = nrhs - c0;
-    // FP64 passes take 8 or 16 columns (tensor-core tiles; unused columns are zero)
-    const int rc = left > 8 ? 16 : (left > 4 || fp64 ? 8 : 4);
+    // passes of 8 or 16 columns (tensor-core tiles; unused columns are zero):
+    // a pass of 8 costs less than a 4-column FMA pass would (measured at the
+    // 4,194,304-point mixture: 6.7 against 10.9 ms)
+    const int rc = left > 8 ? 16 : 8;
     const int nc = std::min(left, rc);
     const double* qc = q + (long)c0 * ldq;
     double* yc = y + (long)c0 * ldy;
     if (rc == 16) Pass<16>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
-    else if (rc == 8) Pass<8>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
-    else Pass<4>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
+    else Pass<8>::run(p, bs, nv, qc, ldq, yc, ldy, nc, fp64, s, tm, launches);
     c0 += nc;
   }
 }

@@ -11,139 +11,12 @@ namespace afmm {
 
 namespace batched_detail {
 
-// M2L on the fly (FP64 entries), one thread per skeleton row of every level.
-template <class K, int RC>
-__global__ void k_m2l_b(LevelSet ls, KernelParams kp, const double* const* __restrict__ qhat_lv,
-                        double* const* __restrict__ yhat_lv) {
-  const long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= ls.row0[ls.nlev]) return;
-  int j = 0;
-  while (j + 1 < ls.nlev && g >= ls.row0[j + 1]) ++j;
-  const LevelView& v = ls.lv[j];
-  const double* qh = qhat_lv[ls.src[j]];
-  const long row = g - ls.row0[j];
-  const int b = v.skel_box[row];
-  const double2 xi = v.skel_xy[row];
-  double acc[RC];
-#pragma unroll
-  for (int k = 0; k < RC; ++k) acc[k] = 0.0;
-  for (int s = 0; s < 40; ++s) {
-    const int c = v.il[(long)b * 40 + s];
-    if (c < 0) continue;
-    const int rc = v.rank[c];
-    const int sc = v.skel_off[c];
-    const double2* xc = v.skel_xy + sc;
-    for (int cc = 0; cc < rc; ++cc) {
-      const double2 p = xc[cc];
-      const double dx = xi.x - p.x, dy = xi.y - p.y;
-      const double kv = K::eval(dx * dx + dy * dy, kp);
-      double q[RC];
-      load_vec<RC>(qh + (long)(sc + cc) * RC, q);
-#pragma unroll
-      for (int k = 0; k < RC; ++k) acc[k] = fma(kv, q[k], acc[k]);
-    }
-  }
-  store_vec<RC>(yhat_lv[ls.src[j]] + row * RC, acc);
-}
-
 template <class K>
 __device__ __forceinline__ float fallback_r2_b(float span_b, float span_c) {
   float e = (span_b + span_c) * 0.0078125f;
   float t = e * e;
   if (K::id == AFMM_KERNEL_LOG) t = fmaxf(t, 4e-10f);
   return t;
-}
-
-// Near field in FP32: one CTA per leaf, one thread per target, all source
-// leaves staged in shared memory (coordinates relative to the target leaf's
-// anchor folded per source leaf; charges as RC-vectors).
-template <class K, int RC>
-__global__ void k_p2p_b(NearView nv, KernelParams kp, const float* __restrict__ qs32, double* __restrict__ ys) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
-  __shared__ float s_dx[9], s_dy[9], s_thr[9];
-  const long b = nv.leaf0 + blockIdx.x;
-  const int n = nv.leaf_cnt[b];
-  const int s0 = nv.leaf_start[b];
-  const float a32 = (float)kp.a, p32 = (float)kp.param;
-  if (threadIdx.x == 0) {
-    const double2 ab = nv.anchor[b];
-    const float sb = nv.span[b];
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (c < 0) continue;
-      const double2 ac = nv.anchor[c];
-      s_src[m] = nv.leaf_start[c];
-      s_cnt[m] = nv.leaf_cnt[c];
-      s_off[m] = off;
-      s_dx[m] = (float)(ab.x - ac.x);
-      s_dy[m] = (float)(ab.y - ac.y);
-      s_thr[m] = fallback_r2_b<K>(sb, nv.span[c]);
-      off += nv.leaf_cnt[c];
-      ++m;
-    }
-    s_off[m] = off;
-    s_ns = m;
-  }
-  __syncthreads();
-  const int ns = s_ns;
-  float4* sq = (float4*)smem;                 // 9*nmax*RC/4
-  float2* sx = (float2*)(sq + 9 * nv.nmax * (RC / 4));
-  for (int m = 0; m < ns; ++m) {
-    const float4* qsrc = reinterpret_cast<const float4*>(qs32 + (long)s_src[m] * RC);
-    const int o = s_off[m], nc = s_cnt[m];
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) sx[o + t] = nv.rel[s_src[m] + t];
-    for (int t = threadIdx.x; t < nc * (RC / 4); t += blockDim.x) sq[o * (RC / 4) + t] = qsrc[t];
-  }
-  __syncthreads();
-  const int i = threadIdx.x;
-  if (i >= n) return;
-  const float2 xi = nv.rel[s0 + i];
-  double acc[RC];
-#pragma unroll
-  for (int k = 0; k < RC; ++k) acc[k] = 0.0;
-  for (int m = 0; m < ns; ++m) {
-    const int o = s_off[m], nc = s_cnt[m];
-    const float ox = xi.x + s_dx[m], oy = xi.y + s_dy[m], thr = s_thr[m];
-    float part[RC];
-#pragma unroll
-    for (int k = 0; k < RC; ++k) part[k] = 0.0f;
-    for (int t = 0; t < nc; ++t) {
-      const float2 p = sx[o + t];
-      const float dx = ox - p.x, dy = oy - p.y;
-      const float R2 = fmaf(dx, dx, dy * dy);
-      float kv;
-      if (R2 < thr) {
-        const int ps = s0 + i, qsrc = s_src[m] + t;
-        if (ps == qsrc) {
-          kv = (float)K::at_zero(kp);
-        } else {
-          const double2 a = nv.pts[ps], c2 = nv.pts[qsrc];
-          kv = (float)K::eval_exact(r2_exact(a.x, a.y, c2.x, c2.y), kp);
-        }
-      } else {
-        kv = K::eval32(R2, a32, p32);
-      }
-      const float4* qv = sq + (o + t) * (RC / 4);
-#pragma unroll
-      for (int k4 = 0; k4 < RC / 4; ++k4) {
-        const float4 w = qv[k4];
-        part[4 * k4] = fmaf(kv, w.x, part[4 * k4]);
-        part[4 * k4 + 1] = fmaf(kv, w.y, part[4 * k4 + 1]);
-        part[4 * k4 + 2] = fmaf(kv, w.z, part[4 * k4 + 2]);
-        part[4 * k4 + 3] = fmaf(kv, w.w, part[4 * k4 + 3]);
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < RC; ++k) acc[k] += (double)part[k];
-  }
-  double* out = ys + (long)(s0 + i) * RC;
-  double cur[RC];
-  load_vec<RC>(out, cur);
-#pragma unroll
-  for (int k = 0; k < RC; ++k) cur[k] += acc[k];
-  store_vec<RC>(out, cur);
 }
 
 // TF32 MMA m16n8k8: lane l = 4g + t holds A[g][t], A[g+8][t], A[g][t+4],
@@ -487,40 +360,25 @@ __global__ void __launch_bounds__(128) k_p2p_dmma(NearView nv, KernelParams kp, 
 
 inline int nbk(long n, int t) { return (int)((n + t - 1) / t); }
 
-// M2L with the entries evaluated on the fly, RC columns per pass: FP64
-// tensor-core tiles (k_m2l_mma) for 8 and 16 columns, one thread per row
-// (k_m2l_b) for 4.
+// M2L with the entries evaluated on the fly, RC = 8 or 16 columns per pass,
+// on FP64 tensor-core tiles (k_m2l_mma).
 template <class K, int RC>
 void m2l_otf_batched(const LevelSet& ls, const KernelParams& kp, const double* const* qh, double* const* yh,
                      cudaStream_t s) {
   if (ls.row0[ls.nlev] == 0) return;
-  if constexpr (RC >= 8) {
-    const long warps = ls.grp0[ls.nlev];
-    k_m2l_mma<K, RC><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
-  } else {
-    const long rows = ls.row0[ls.nlev];
-    k_m2l_b<K, RC><<<nbk(rows, 128), 128, 0, s>>>(ls, kp, qh, yh);
-  }
+  const long warps = ls.grp0[ls.nlev];
+  k_m2l_mma<K, RC><<<nbk(warps * 32, 128), 128, 0, s>>>(ls, kp, qh, yh);
   AFMM_LAUNCH_CHECK();
 }
 
-// Mixed near field of a pass: TF32x3 tensor-core tiles (8 and 16 columns,
-// charges as TF32 parts) or FP32 FMA (4 columns, FP32 charges).
+// Mixed near field of a pass: TF32x3 tensor-core tiles (8 or 16 columns,
+// charges as TF32 parts).
 template <class K, int RC>
 void p2p_mma_batched(const NearView& nv, const KernelParams& kp, const uint2* qhl, double* ys, cudaStream_t s) {
   const int warps = std::min(4, (nv.nmax + 31) / 32);
   const size_t smem = (size_t)9 * ((nv.nmax + 7) / 8 * 8) * sizeof(float2) + (size_t)warps * RC * 32 * sizeof(double);
   allow_smem(k_p2p_mma<K, RC>, smem);
   k_p2p_mma<K, RC><<<(int)nv.nleaf, 32 * warps, smem, s>>>(nv, kp, qhl, ys);
-  AFMM_LAUNCH_CHECK();
-}
-
-template <class K>
-void p2p_fma_batched4(const NearView& nv, const KernelParams& kp, const float* qs32, double* ys, cudaStream_t s) {
-  const int T = (nv.nmax + 31) / 32 * 32;
-  const size_t smem = (size_t)9 * nv.nmax * (sizeof(float) * 4 + sizeof(float2));
-  allow_smem(k_p2p_b<K, 4>, smem);
-  k_p2p_b<K, 4><<<(int)nv.nleaf, T, smem, s>>>(nv, kp, qs32, ys);
   AFMM_LAUNCH_CHECK();
 }
 

@@ -1872,8 +1872,9 @@ afmm_status afmm_get_m2l_stored(afmm_handle* h, int* stored) {
 }
 
 afmm_status afmm_set_profiling(afmm_handle* h, int on) {
-  if (!h) return AFMM_BAD_ARG;
+  if (!h || on < 0 || on > 2) return AFMM_BAD_ARG;
   h->profiling = on != 0;
+  h->timer.serial = on == 2;
   return AFMM_OK;
 }
 

@@ -214,6 +214,9 @@ struct NearView {
 struct StageTimer {
   std::vector<std::pair<std::string, cudaEvent_t>> marks;
   size_t used = 0;
+  // stages run one after another on the launching stream (no near field
+  // beside the far field), so every stage is its kernels' own duration
+  bool serial = false;
   // spans timed on another stream (a stage that overlaps the marked ones)
   struct Span {
     std::string name;

@@ -18,7 +18,7 @@ namespace afmm {
 
 // Bumped whenever KernelTable or an argument type of its launchers changes:
 // a table compiled against other headers is refused at registration.
-constexpr int kKernelTableAbi = 3;
+constexpr int kKernelTableAbi = 4;
 
 // Fingerprint of the layouts of the launchers' argument types (sizes and a
 // few field offsets), recorded in every table where it is compiled: a table
@@ -42,14 +42,10 @@ struct KernelTable {
   // single-RHS mixed path: M2L on the fly (FP64), FP32 near field (mixed_k.cuh)
   void (*m2l_otf)(const LevelSet&, const KernelParams&, cudaStream_t) = nullptr;
   void (*p2p32)(const NearView&, const KernelParams&, const float*, double*, cudaStream_t) = nullptr;
-  // batched passes (batched_k.cuh): M2L on the fly for 4 columns and for
-  // [0] 8 / [1] 16 columns; mixed near field for 4 and for 8 / 16 columns;
-  // FP64 near field for 8 / 16 columns
-  void (*m2l_otf_b4)(const LevelSet&, const KernelParams&, const double* const*, double* const*,
-                     cudaStream_t) = nullptr;
+  // batched passes (batched_k.cuh), [0] 8 / [1] 16 columns: M2L on the fly,
+  // mixed near field, FP64 near field
   void (*m2l_otf_mma[2])(const LevelSet&, const KernelParams&, const double* const*, double* const*,
                          cudaStream_t) = {nullptr, nullptr};
-  void (*p2p_b4)(const NearView&, const KernelParams&, const float*, double*, cudaStream_t) = nullptr;
   void (*p2p_mma[2])(const NearView&, const KernelParams&, const uint2*, double*, cudaStream_t) = {nullptr, nullptr};
   void (*p2p_dmma[2])(const NearView&, const KernelParams&, const double*, double*, cudaStream_t) = {nullptr, nullptr};
   // mixed near field of 16-column passes on tcgen05 tiles (p2p_tc_k.cuh);

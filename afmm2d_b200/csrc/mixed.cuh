@@ -28,8 +28,7 @@ constexpr int kBatchMax = 16;
 struct BatchState {
   bool ready = false;
   double* qs = nullptr;     // sorted charges, point-major N x kBatchMax
-  float* qs32 = nullptr;
-  uint2* qhl = nullptr;     // TF32 high / low parts of qs32, interleaved
+  uint2* qhl = nullptr;     // TF32 high / low parts of the FP32-rounded charges, interleaved
   double* ys = nullptr;     // sorted potentials, point-major
   double* qhat[kMaxLevels] = {nullptr};
   double* yhat[kMaxLevels] = {nullptr};

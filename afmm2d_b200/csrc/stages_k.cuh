@@ -22,10 +22,8 @@ KernelTable make_kernel_table(const char* name) {
   t.p2p64 = &fmm_detail::P2p64Run<K>::run;
   t.m2l_otf = &mixed_detail::M2lOtfRun<K>::run;
   t.p2p32 = &mixed_detail::P2p32Run<K>::run;
-  t.m2l_otf_b4 = &batched_detail::m2l_otf_batched<K, 4>;
   t.m2l_otf_mma[0] = &batched_detail::m2l_otf_batched<K, 8>;
   t.m2l_otf_mma[1] = &batched_detail::m2l_otf_batched<K, 16>;
-  t.p2p_b4 = &batched_detail::p2p_fma_batched4<K>;
   t.p2p_mma[0] = &batched_detail::p2p_mma_batched<K, 8>;
   t.p2p_mma[1] = &batched_detail::p2p_mma_batched<K, 16>;
   t.p2p_dmma[0] = &batched_detail::p2p_dmma_batched<K, 8>;

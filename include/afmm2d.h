@@ -189,8 +189,10 @@ afmm_status afmm_get_l2p(afmm_handle* h, int level, int k, int32_t* rows, int32_
  * on.  names/values arrays of capacity `cap`; *n receives the count.  Stages
  * on the handle's stream are the intervals between consecutive marks; in a
  * batched pass the near field runs on a second stream beside the far field,
- * so its kernel time is the separate "p2p_kernel" entry and "p2p" is the
- * far field's wait for it. */
+ * so its span is the separate "p2p_kernel" entry and "p2p" is the far
+ * field's wait for it.  afmm_set_profiling(h, 2) profiles with the near
+ * field run after the far field on the handle's stream (same results), so
+ * that "p2p" is the near-field kernel's own duration. */
 afmm_status afmm_set_profiling(afmm_handle* h, int on);
 afmm_status afmm_get_stage_times(afmm_handle* h, int cap, const char** names, double* ms, int* n);
 /* Setup wall times in seconds: [create, assemble]. */

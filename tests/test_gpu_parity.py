@@ -245,7 +245,7 @@ def correctly_rounded_kernel(kernel, a, p, q, param=0.01):
 
 @pytest.mark.parametrize("nrhs", [3, 8, 21])
 def test_batched_mixed_vs_fp64(nrhs):
-    """Batched mixed path (passes of 4, 8 and 16 right-hand sides, ragged
+    """Batched mixed path (passes of 8 and 16 right-hand sides, ragged
     remainders) against the FP64 path, column by column."""
     pts, _, _ = workloads.make("mixture4m", N=65536)
     a = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
@@ -255,6 +255,32 @@ def test_batched_mixed_vs_fp64(nrhs):
     for c in range(nrhs):
         y64 = a.computeMatVecProduct(Q[:, c])
         assert np.linalg.norm(Ym[:, c] - y64) / np.linalg.norm(y64) <= MIXED_TOL, c
+
+
+@pytest.mark.parametrize("precision", ["mixed", "fp64_batched"])
+def test_batched_near_field_beside_or_after_far_field(precision):
+    """The batched near field runs on a second stream beside the far field;
+    profiling mode 2 runs it after the far field on the handle's stream.
+    Both give the same values, and the stage times name the near field's
+    span (beside) or its own duration (after)."""
+    pts, _, _ = workloads.make("mixture4m", N=65536)
+    a = A.AFMM(65536, 64, 6, pts, kernel="one_over_r")
+    a.assemble()
+    Q = np.random.default_rng(5).standard_normal((65536, 16))
+    Y0 = a.computeMatVecProduct(Q, precision=precision)
+    a.set_profiling(True)
+    Y1 = a.computeMatVecProduct(Q, precision=precision)
+    st1 = a.stage_times()
+    a.set_profiling(2)
+    Y2 = a.computeMatVecProduct(Q, precision=precision)
+    st2 = a.stage_times()
+    a.set_profiling(False)
+    np.testing.assert_array_equal(Y1, Y0)
+    np.testing.assert_array_equal(Y2, Y0)
+    assert "p2p_kernel" in st1 and st1["p2p_kernel"] > 0
+    assert "p2p_kernel" not in st2 and st2["p2p"] > 0
+    with pytest.raises(A.AFMMError):
+        a.set_profiling(3)
 
 
 def test_batched_host_device_and_kernels():
