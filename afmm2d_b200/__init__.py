@@ -78,6 +78,7 @@ _SIGS = {
     "afmm_set_get_offsets": [_vp, _vp],
     "afmm_set_get_launches": [_vp, _vp, _vp],
     "afmm_set_get_stream": [_vp, _vp],
+    "afmm_set_sweep_wait_margin": [_vp, _i],
     "afmm_set_get_stage_times": [_vp, _i, _vp, _vp, _vp],
     "afmm_set_destroy": [_vp],
 }
@@ -411,10 +412,10 @@ class AFMM:
         _check(lib().afmm_get_setup_times(self._h, _ptr(t)), self._h)
         out = {"create_s": t[0], "assemble_s": t[1]}
         n = ctypes.c_int()
-        names = (ctypes.c_char_p * 32)()
-        secs = (ctypes.c_double * 32)()
-        _check(lib().afmm_get_setup_phases(self._h, 32, names, secs, ctypes.byref(n)), self._h)
-        out.update({"assemble_" + names[i].decode() + "_s": secs[i] for i in range(min(n.value, 32))})
+        names = (ctypes.c_char_p * 64)()
+        secs = (ctypes.c_double * 64)()
+        _check(lib().afmm_get_setup_phases(self._h, 64, names, secs, ctypes.byref(n)), self._h)
+        out.update({"assemble_" + names[i].decode() + "_s": secs[i] for i in range(min(n.value, 64))})
         return out
 
     def counts(self):
@@ -491,6 +492,10 @@ class AFMMSet:
         s = ctypes.c_void_p()
         self._call("afmm_set_get_stream", ctypes.byref(s))
         return s.value
+
+    def set_sweep_wait_margin(self, margin):
+        """Test hook of the sweeps' bounded waits (afmm_set_sweep_wait_margin)."""
+        self._call("afmm_set_sweep_wait_margin", int(margin))
 
     def stage_times(self):
         """Device milliseconds per stage of the last matvec."""

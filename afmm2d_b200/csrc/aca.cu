@@ -128,8 +128,12 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, AcaScrat
   const size_t n_usp = usp > 0 ? (size_t)ncl * C * usp * n1max : 0;
   const size_t n_piv = (size_t)in.nbox * rcap;
   DevScratch& w = scratch.work;
-  w.reserve(DevScratch::need({n_gscr, sizeof(double) * n_vsp, sizeof(double) * n_usp, sizeof(int32_t) * n_piv,
-                              sizeof(int32_t) * n_piv}));
+  const auto t_res = std::chrono::steady_clock::now();
+  const size_t need = DevScratch::need({n_gscr, sizeof(double) * n_vsp, sizeof(double) * n_usp,
+                                        sizeof(int32_t) * n_piv, sizeof(int32_t) * n_piv});
+  w.reserve(need);
+  out.scratch_bytes = need;
+  out.scratch_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_res).count();
   a.gscr = n_gscr ? w.take<unsigned char>(n_gscr) : nullptr;
   a.vspill = n_vsp ? w.take<double>(n_vsp) : nullptr;
   a.uspill = n_usp ? w.take<double>(n_usp) : nullptr;

@@ -93,6 +93,8 @@ struct AcaLevelOut {
   std::vector<int32_t> h_rank, h_skel_off;
   std::vector<int64_t> h_l2p_off;
   double aca_s = 0, l2p_s = 0;  // wall clock of the two phases
+  double scratch_s = 0;         // wall clock of the working-memory reservation
+  size_t scratch_bytes = 0;     // working memory the level's ACA needs
 };
 
 // Working memory of the ACA and L2P kernels, kept across the levels of one

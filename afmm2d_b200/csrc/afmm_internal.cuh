@@ -11,6 +11,7 @@
 
 #include "../../include/afmm2d.h"
 #include "exact_math.cuh"
+#include "fast_math.cuh"
 
 namespace afmm {
 
@@ -94,9 +95,9 @@ struct KLog {
   }
   // a = 2^-L, so dividing by a twice is the exact scaling by 1/a^2: both
   // branches are evaluated without divergence and selected (same bits as
-  // 0.5*R2*log(R2)/a/a and 0.5*log(R2))
+  // 0.5*R2*l/a/a and 0.5*l); l is the table-driven log (within one ulp)
   __device__ __forceinline__ static double eval(double R2, const KernelParams& p) {
-    const double l = log(R2);
+    const double l = log_tang(R2);
     const double near = ((0.5 * R2) * l) * p.inv_a2;
     const double r = R2 < p.a2 ? near : 0.5 * l;
     return R2 < 1e-10 ? 0.0 : r;

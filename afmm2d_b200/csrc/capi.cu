@@ -103,7 +103,7 @@ struct afmm_handle {
   // assemble phases (wall clock, s): the rest of assemble is host work
   std::vector<std::pair<std::string, double>> setup_phase{
       {"aca", 0.0}, {"l2p", 0.0}, {"m2l_blocks", 0.0}, {"transpose_mixed", 0.0}, {"tables_alloc", 0.0},
-      {"m2l_cudamalloc", 0.0}, {"level_prep", 0.0}, {"aca_alloc_other", 0.0}};
+      {"m2l_cudamalloc", 0.0}, {"level_prep", 0.0}, {"aca_alloc_other", 0.0}, {"aca_scratch_reserve", 0.0}};
   bool have_last = false;
   // host-pointer matvecs: copy streams
   cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
@@ -593,6 +593,8 @@ void do_assemble(afmm_handle* h) {
     h->setup_phase[1].second += out.l2p_s;
     h->setup_phase.push_back({"aca_level" + std::to_string(j), out.aca_s});
     h->setup_phase.push_back({"aca_cluster_level" + std::to_string(j), (double)out.cluster});
+    h->setup_phase[8].second += out.scratch_s;
+    h->setup_phase.push_back({"aca_scratch_gb_level" + std::to_string(j), (double)out.scratch_bytes * 1e-9});
     v.skel_off = out.skel_off;
     v.skel_ids = out.skel_ids;
     v.cpiv_ids = out.cpiv_ids;
@@ -2100,6 +2102,8 @@ afmm_status afmm_set_matvec(afmm_set* st, const double* q, double* y, int mem_de
     ++st->graph_launches;
     AFMM_CUDA(cudaMemcpyAsync(y, st->plan.y, bytes, mem_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     AFMM_CUDA(cudaStreamSynchronize(s));
+    if (*st->plan.h_err)
+      throw Error{AFMM_TIMEOUT, "afmm_set_matvec: a sweep's wait for the level below gave up (output incomplete)"};
     return AFMM_OK;
   } catch (const Error& e) {
     st->err = e.msg;
@@ -2142,6 +2146,21 @@ afmm_status afmm_set_get_stream(afmm_set* st, void** stream) {
   if (!st || !stream) return AFMM_BAD_ARG;
   *stream = (void*)st->stream;
   return AFMM_OK;
+}
+
+afmm_status afmm_set_sweep_wait_margin(afmm_set* st, int margin) {
+  if (!st) return AFMM_BAD_ARG;
+  try {
+    if (margin < 0) throw Error{AFMM_BAD_ARG, "afmm_set_sweep_wait_margin: margin >= 0"};
+    AFMM_CUDA(cudaStreamSynchronize(st->stream));
+    st->plan.up.margin = margin;
+    st->plan.down.margin = margin;
+    set_recapture(st->plan, st->stream);
+    return AFMM_OK;
+  } catch (const Error& e) {
+    st->err = e.msg;
+    return e.status;
+  }
 }
 
 afmm_status afmm_set_destroy(afmm_set* st) {

@@ -348,9 +348,19 @@ inline P2pShape p2p_shape(int nmax) {
 // single-problem kernels (fmm.cu) and the fused many-problem kernels (set.cu)
 // so both give the same bits.
 
+// Loads of values that may have been written earlier in the same launch (the
+// persistent many-problem sweeps): kL2 reads them through L2 (ld.global.cg),
+// which other SMs' published stores reach; otherwise an ordinary load.
+template <bool kL2>
+__device__ __forceinline__ double ld_src(const double* p) {
+  if constexpr (kL2) return __ldcg(p);
+  else return *p;
+}
+
 // M2M (src/AFMM2DTree.cpp:1129-1154): qhat[row] = (L2P_b^T src_b)[row] over
 // the row-major L2P copy; src_b = leaf charges, or the concatenated outgoing
 // charges of children 0..3.
+template <bool kL2 = false>
 __device__ __forceinline__ void m2m_row(const LevelView& v, const double* __restrict__ src_all, int leaf, long row) {
   const int b = v.skel_box[row];
   const int r = v.rank[b];
@@ -363,12 +373,12 @@ __device__ __forceinline__ void m2m_row(const LevelView& v, const double* __rest
   // (unrolled: more loads in flight; each partial sum keeps its order)
 #pragma unroll 4
   for (; i + 3 < n; i += 4) {
-    a0 += P[(long)i * r] * src[i];
-    a1 += P[(long)(i + 1) * r] * src[i + 1];
-    a2 += P[(long)(i + 2) * r] * src[i + 2];
-    a3 += P[(long)(i + 3) * r] * src[i + 3];
+    a0 += P[(long)i * r] * ld_src<kL2>(src + i);
+    a1 += P[(long)(i + 1) * r] * ld_src<kL2>(src + i + 1);
+    a2 += P[(long)(i + 2) * r] * ld_src<kL2>(src + i + 2);
+    a3 += P[(long)(i + 3) * r] * ld_src<kL2>(src + i + 3);
   }
-  for (; i < n; ++i) a0 += P[(long)i * r] * src[i];
+  for (; i < n; ++i) a0 += P[(long)i * r] * ld_src<kL2>(src + i);
   v.qhat[row] = (a0 + a1) + (a2 + a3);
 }
 
@@ -404,6 +414,7 @@ __device__ __forceinline__ void m2l_row(const LevelView& v, long row) {
 // L2L (src/AFMM2DTree.cpp:1180-1197): t = (L2P_b yhat_b)[node row g] over the
 // column-major L2P, added to the child's incoming potential (node row g of
 // level j is skeleton row g of level j+1), or written as the leaf potential.
+template <bool kL2 = false>
 __device__ __forceinline__ void l2l_row(const LevelView& v, double* __restrict__ child_yhat, double* __restrict__ ys,
                                         int leaf, long g) {
   const int b = v.node_box[g];
@@ -416,12 +427,12 @@ __device__ __forceinline__ void l2l_row(const LevelView& v, double* __restrict__
   int c = 0;
 #pragma unroll 4
   for (; c + 3 < r; c += 4) {
-    a0 += P[(long)c * n] * yb[c];
-    a1 += P[(long)(c + 1) * n] * yb[c + 1];
-    a2 += P[(long)(c + 2) * n] * yb[c + 2];
-    a3 += P[(long)(c + 3) * n] * yb[c + 3];
+    a0 += P[(long)c * n] * ld_src<kL2>(yb + c);
+    a1 += P[(long)(c + 1) * n] * ld_src<kL2>(yb + c + 1);
+    a2 += P[(long)(c + 2) * n] * ld_src<kL2>(yb + c + 2);
+    a3 += P[(long)(c + 3) * n] * ld_src<kL2>(yb + c + 3);
   }
-  for (; c < r; ++c) a0 += P[(long)c * n] * yb[c];
+  for (; c < r; ++c) a0 += P[(long)c * n] * ld_src<kL2>(yb + c);
   const double t = (a0 + a1) + (a2 + a3);
   if (leaf) ys[v.leaf_start[b] + i] = t;
   else child_yhat[g] += t;

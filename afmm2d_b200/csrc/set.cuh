@@ -48,8 +48,33 @@ struct SetProblem {
   P2pShape shape;
 };
 
+// A persistent sweep (every level of every problem in one launch): items are
+// tiles of kSweepTile rows of one depth's flat row space (segs[depth]), listed
+// in dependency order; CTAs take them in list order from a ticket counter.
+constexpr int kSweepTile = 128;
+struct SweepPlan {
+  const SetSegs* segs = nullptr;    // per depth (device array)
+  const int32_t* item_depth = nullptr;
+  const int64_t* item_row0 = nullptr;
+  int nitems = 0;
+  int grid = 0;                     // resident CTAs launched
+  int margin = 0;                   // added to every awaited row count (0; > 0 only to test the time limit)
+};
+
+// Counters of the persistent sweeps, zeroed at the start of every replay.
+struct SweepSync {
+  int* ticket = nullptr;  // [2]: up-sweep, down-sweep
+  int* done_up = nullptr; // nprob x kMaxLevels: M2M rows published per (problem, level)
+  int* done_dn = nullptr; // nprob x kMaxLevels: L2L node rows published per (problem, level)
+  int* err = nullptr;     // [1]: a wait gave up (AFMM_TIMEOUT)
+  size_t bytes = 0;       // size of the block starting at ticket
+};
+
 struct SetPlan {
   SetDev dev;
+  SweepPlan up, down;
+  SweepSync sync;
+  int* h_err = nullptr;     // pinned copy of sync.err, written at the end of every replay
   int kernel_id = 0;
   long total_points = 0;
   int p2p_threads = 0;
@@ -71,8 +96,11 @@ void set_stage_times(const SetPlan& sp, std::vector<std::pair<std::string, doubl
 
 // Builds the device tables (allocated from `arena`) and the graph on stream s.
 void set_build(SetPlan& sp, const std::vector<SetProblem>& probs, DevArena& arena, cudaStream_t s);
-// One FP64 matvec of every problem: sp.q -> sp.y (graph replay on s).
+// One FP64 matvec of every problem: sp.q -> sp.y (graph replay on s).  After
+// the stream completes, *sp.h_err is nonzero if a sweep's bounded wait gave up.
 void set_matvec(SetPlan& sp, cudaStream_t s);
+// Re-records the graph after a change of the sweeps' parameters.
+void set_recapture(SetPlan& sp, cudaStream_t s);
 void set_release(SetPlan& sp);
 
 }  // namespace afmm

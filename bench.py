@@ -432,6 +432,15 @@ def run_ours(args):
                      "flop_definition": "2*nrhs flops per stored M2L entry (tile padding not counted)",
                      "ms": sb[dom]}
         roof_dmma["frac"] = roof_dmma["achieved"] / dmma_peak
+    # the headline roofline is the binding one: of the kernel's two floors
+    # (algorithmic bytes / HBM peak, FP64 tensor flops / DMMA peak) the longer,
+    # i.e. the larger fraction of the same duration; the other stays beside it
+    roof_other = None
+    if roof_dmma is not None and roof.get("frac") is not None and roof_dmma["frac"] > roof["frac"]:
+        roof_dmma["traffic"] = roof.get("traffic")
+        roof_dmma["binding"] = (f"FP64 tensor floor {roof_dmma['algorithmic_flops'] / (dmma_peak * 1e12) * 1e3:.2f} ms "
+                                f"> HBM floor {roof['algorithmic_bytes'] / (roof['peak'] * 1e9) * 1e3:.2f} ms")
+        roof_other, roof = roof, roof_dmma
     line = {"metric": metric_name(args.workload, N, p, R), "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_dev["batched"], "higher_is_better": True, "scaling": "weak",
@@ -454,7 +463,7 @@ def run_ours(args):
             "counts": counts,
             "roofline": roof, "roofline_fp64_m2l": roof64, "fma_peaks_tflops": {"fp64": fp64_peak, "fp32": fp32_peak},
             "fp64_pipes_tflops": {"dmma": dmma_peak, "dfma": dfma_peak, "dmma_and_dfma_together": both_peak},
-            "roofline_dmma_m2l": roof_dmma,
+            "roofline_dmma_m2l": roof_dmma, "roofline_hbm_m2l": roof_other,
             "clocks": clocks, "gpu_launches": int(launches["batched"]),
             "e2e": {"value": world * N * R / t_e2e, "unit": UNIT, "h2d_bytes_per_step": 8 * N * R,
                     "d2h_bytes_per_step": 8 * N * R, "ms_per_step": t_e2e * 1e3, "nrhs": R}}

@@ -334,8 +334,12 @@ afmm_status afmm_destroy(afmm_handle* h);
  * handles on the current device with one kernel id (the handles stay owned
  * by the caller and must outlive the set) and records, once, a CUDA graph in
  * which every stage of the FP64 matvec is one fused launch over all problems
- * (gather, M2M per depth below the leaves, M2L of all levels, L2L per level,
- * near field, scatter).  afmm_set_matvec replays it: q and y hold the
+ * (gather; the M2M of every level as one persistent up-sweep; M2L of all
+ * levels; the L2L of every level as one persistent down-sweep; near field;
+ * scatter).  In a sweep, work items wait on the device, each for at most
+ * two seconds, until the level they read is complete; a wait that gives up
+ * makes afmm_set_matvec return AFMM_TIMEOUT (the output is then incomplete;
+ * the set stays usable).  afmm_set_matvec replays it: q and y hold the
  * problems' charges / potentials back to back in handle order (problem p at
  * offsets[p] .. offsets[p+1], each in its own original point order), host or
  * device memory.  Each problem's result has the same bits as its own FP64
@@ -352,6 +356,11 @@ afmm_status afmm_set_get_launches(afmm_set* s, int* launches_per_matvec, int64_t
  * inside the graph between stages); names stay valid until the next call. */
 afmm_status afmm_set_get_stage_times(afmm_set* s, int cap, const char** names, double* ms, int* n);
 afmm_status afmm_set_get_stream(afmm_set* s, void** stream);
+/* Test hook for the sweeps' time limit: adds `margin` (>= 0) to every row
+ * count that a sweep's item waits for, so with margin > 0 no wait can be
+ * satisfied and the next afmm_set_matvec returns AFMM_TIMEOUT after the limit;
+ * 0 (the default) restores normal operation.  Re-records the graph. */
+afmm_status afmm_set_sweep_wait_margin(afmm_set* s, int margin);
 afmm_status afmm_set_destroy(afmm_set* s);
 const char* afmm_set_last_error(afmm_set* s);
 

@@ -99,3 +99,27 @@ def test_set_rejects_mixed_kernels_and_unassembled_handles():
     with pytest.raises(A.AFMMError) as e:
         A.AFMMSet([a, c])
     assert e.value.status == 6
+
+
+@pytest.mark.gpu
+def test_set_sweep_wait_gives_up_with_timeout_status():
+    """The persistent sweeps' device waits are bounded: with the test margin
+    no wait can be satisfied, the matvec returns AFMM_TIMEOUT after the time
+    limit instead of hanging, and the set works again once it is removed."""
+    import time
+    probs, hs = _problems(4, 8192)
+    st = A.AFMMSet(hs)
+    qs = [q for _, q in probs]
+    good = st.matvec(qs)
+    st.set_sweep_wait_margin(1)
+    t0 = time.perf_counter()
+    with pytest.raises(A.AFMMError) as e:
+        st.matvec(qs)
+    assert e.value.status == 4  # AFMM_TIMEOUT
+    assert time.perf_counter() - t0 < 60
+    st.set_sweep_wait_margin(0)
+    again = st.matvec(qs)
+    assert all(np.array_equal(a, b) for a, b in zip(good, again))
+    with pytest.raises(A.AFMMError):
+        st.set_sweep_wait_margin(-1)
+    st.close()
