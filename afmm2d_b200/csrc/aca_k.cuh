@@ -147,7 +147,7 @@ __device__ inline ArgMax cluster_argmax(cg::cluster_group& cluster, ArgMax m, do
 }
 
 template <class K>
-__global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
+__global__ void __launch_bounds__(ACA_T, 2) k_aca(AcaArgs A) {
   cg::cluster_group cluster = cg::this_cluster();
   const int C = (int)cluster.num_blocks();
   const int crank = (int)cluster.block_rank();
@@ -291,7 +291,23 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
           for (int j = tid; j < nloc; j += ACA_T) {
             double2 c = cols_xy[j];
             double v = K::eval_exact(r2_exact(rr.x, rr.y, c.x, c.y), A.kp);
-            for (int l = 0; l < k; ++l) v = __dsub_rn(v, __dmul_rn(uri[l], Vrow(l)[j]));
+            // the reference's order of subtractions; sixteen V loads issued ahead
+            int l = 0;
+            for (; l + 16 <= k; l += 16) {
+              double w[16];
+#pragma unroll
+              for (int t = 0; t < 16; ++t) w[t] = Vrow(l + t)[j];
+#pragma unroll
+              for (int t = 0; t < 16; ++t) v = __dsub_rn(v, __dmul_rn(uri[l + t], w[t]));
+            }
+            for (; l + 4 <= k; l += 4) {
+              double w[4];
+#pragma unroll
+              for (int t = 0; t < 4; ++t) w[t] = Vrow(l + t)[j];
+#pragma unroll
+              for (int t = 0; t < 4; ++t) v = __dsub_rn(v, __dmul_rn(uri[l + t], w[t]));
+            }
+            for (; l < k; ++l) v = __dsub_rn(v, __dmul_rn(uri[l], Vrow(l)[j]));
             Vk[j] = v;
             if (col_ok[j]) am_add(mm, v, lo + j);
           }
@@ -335,7 +351,15 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
           for (int i = tid; i < n1; i += ACA_T) {
             double2 r = rows_xy[i];
             double u = K::eval_exact(r2_exact(r.x, r.y, s_colxy[0], s_colxy[1]), A.kp);
-            for (int l = 0; l < k; ++l) u = __dsub_rn(u, __dmul_rn(vcol[l], Urow(l)[i]));
+            int l = 0;
+            for (; l + 4 <= k; l += 4) {
+              const double w0 = Urow(l)[i], w1 = Urow(l + 1)[i], w2 = Urow(l + 2)[i], w3 = Urow(l + 3)[i];
+              u = __dsub_rn(u, __dmul_rn(vcol[l], w0));
+              u = __dsub_rn(u, __dmul_rn(vcol[l + 1], w1));
+              u = __dsub_rn(u, __dmul_rn(vcol[l + 2], w2));
+              u = __dsub_rn(u, __dmul_rn(vcol[l + 3], w3));
+            }
+            for (; l < k; ++l) u = __dsub_rn(u, __dmul_rn(vcol[l], Urow(l)[i]));
             Uk[i] = u;
           }
           __syncthreads();
@@ -346,7 +370,21 @@ __global__ void __launch_bounds__(ACA_T) k_aca(AcaArgs A) {
           for (int l = warp; l <= k; l += ACA_WARPS) {
             const double* Vl = Vrow(l);
             dd sv{0.0, 0.0};
-            for (int j = lane; j < nloc; j += 32) {
+            int j = lane;
+            for (; j + 480 < nloc; j += 512) {  // same order of additions, loads issued ahead
+              double a[16], c[16];
+#pragma unroll
+              for (int t = 0; t < 16; ++t) {
+                a[t] = Vl[j + 32 * t];
+                c[t] = Vk[j + 32 * t];
+              }
+#pragma unroll
+              for (int t = 0; t < 16; ++t) {
+                const double p = __dmul_rn(a[t], c[t]);
+                sv = dd_add(sv, dd{p, __fma_rn(a[t], c[t], -p)});
+              }
+            }
+            for (; j < nloc; j += 32) {
               const double a = Vl[j], c = Vk[j];
               const double p = __dmul_rn(a, c);
               sv = dd_add(sv, dd{p, __fma_rn(a, c, -p)});

@@ -108,11 +108,13 @@ struct KLog {
     if (R2 < a * a) return __fdiv_rn(0.5f * R2 * l, a * a);
     return 0.5f * l;
   }
-  // ln(R2) = lg2(R2) ln 2; lg2.approx has absolute error ~2^-22
+  // ln(R2) = lg2(R2) ln 2; lg2.approx has absolute error ~2^-22.  a = 2^-L,
+  // so 1/a^2 is an exact power of two (loop-invariant): the near branch
+  // multiplies instead of dividing
   __device__ __forceinline__ static float eval32_pos(float R2, float a, float) {
     if (R2 < 1e-10f) return 0.0f;
     const float l = __log2f(R2) * 0.693147180559945309f;
-    if (R2 < a * a) return __fdividef(0.5f * R2 * l, a * a);
+    if (R2 < a * a) return (0.5f * R2 * l) * __frcp_rn(a * a);
     return 0.5f * l;
   }
 };
@@ -156,8 +158,13 @@ struct KGaussian {
   __device__ __forceinline__ static float eval32(float R2, float, float param) {
     return expf(-__fdiv_rn(R2, param));
   }
+  // exp(-R2/param) = 2^(R2 c), c = -log2(e)/param (loop-invariant): one
+  // multiply and ex2.approx (relative error ~2^-22, inside the TF32 split)
   __device__ __forceinline__ static float eval32_pos(float R2, float, float param) {
-    return __expf(-__fdividef(R2, param));
+    const float c = __fdiv_rn(-1.44269504088896341f, param);
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(R2 * c));
+    return y;
   }
 };
 
