@@ -48,14 +48,15 @@ struct Error {
 // tensor-core near field (whose operand split allows 2^-21).
 struct KernelParams {
   int id;
-  double a;       // 2^-L
-  double param;   // Gaussian: exp(-R2 / param)
-  double a2;      // a * a
-  double inv_a2;  // 1 / (a * a)
+  double a;              // 2^-L
+  double param;          // Gaussian: exp(-R2 / param)
+  double a2;             // a * a
+  double inv_a2;         // 1 / (a * a)
+  double neg_inv_param;  // -1 / param (the FP64 Gaussian multiplies instead of dividing)
 };
 
 inline KernelParams make_kernel_params(int id, double a, double param) {
-  return KernelParams{id, a, param, a * a, 1.0 / (a * a)};
+  return KernelParams{id, a, param, a * a, 1.0 / (a * a), -1.0 / param};
 }
 
 __device__ __forceinline__ double r2_exact(double xi, double yi, double xj, double yj) {
@@ -154,7 +155,11 @@ struct KGaussian {
   __device__ __forceinline__ static double eval_exact(double R2, const KernelParams& p) {
     return exp_cr(-__ddiv_rn(R2, p.param));
   }
-  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) { return exp(-R2 / p.param); }
+  // R2 * (-1/param) is within one rounding of -R2/param (the setup's
+  // eval_exact keeps the division)
+  __device__ __forceinline__ static double eval(double R2, const KernelParams& p) {
+    return exp_tang(R2 * p.neg_inv_param);
+  }
   __device__ __forceinline__ static float eval32(float R2, float, float param) {
     return expf(-__fdiv_rn(R2, param));
   }

@@ -1,7 +1,8 @@
-// FP64 natural logarithm for the matvec's kernel entries (near field, FP64
-// tensor-tile near field, on-the-fly M2L); the setup keeps the correctly
-// rounded log_cr of exact_math.cuh.
+// FP64 natural logarithm and exponential for the matvec's kernel entries
+// (near field, FP64 tensor-tile near field, on-the-fly M2L); the setup keeps
+// the correctly rounded log_cr / exp_cr of exact_math.cuh.
 //
+// log_tang:
 // Method: P. T. P. Tang, "Table-driven implementation of the logarithm
 // function in IEEE floating-point arithmetic", ACM TOMS 16(4), 1990.
 // x = 2^k m with m in [1, 2); F = 1 + j/128 is the breakpoint nearest m (j
@@ -13,13 +14,13 @@
 // 2^-42, so the first bracket is exact for every exponent; near x = 1 from
 // either side it is exactly zero (j = 0, k = 0, or j = 128, k = -1), so small
 // results keep full relative accuracy.  About 16 FP64 operations and two
-// table loads (log_table.cuh, L1-resident).  Error within about one ulp for
+// table loads (math_tables.cuh, L1-resident).  Error within about one ulp for
 // positive normal x (tests compare it with the correctly rounded log); zero,
 // subnormal and non-finite inputs give an unspecified value without a trap,
 // which the kernel functors select away (their R2 < 1e-10 branch).
 #pragma once
 
-#include "log_table.cuh"
+#include "math_tables.cuh"
 
 namespace afmm {
 
@@ -45,6 +46,33 @@ __device__ __forceinline__ double log_tang(double x) {
   const double p = q * (u0 * u0);
   const double lo = (fma(kd, kLn2Lo, lnF.y) + u1) + p;
   return hi + (u0 + lo);
+}
+
+// exp_tang: P. T. P. Tang, "Table-driven implementation of the exponential
+// function in IEEE floating-point arithmetic", ACM TOMS 15(2), 1989.
+// x = (32 m + j) ln2/32 + r with N = 32 m + j the integer nearest x 32/ln2,
+// j = N mod 32, |r| <= ln2/64 (r = x - N L1 - N L2, N L1 exact);
+//   exp(x) = 2^m (S_hi + (S_lo + S p(r))),  S = 2^(j/32) = S_hi + S_lo,
+// p(r) = exp(r) - 1 by its Taylor polynomial to r^6 (truncation below
+// 2^-58).  About 13 FP64 operations and one table load.  Error within about
+// one ulp for x in [-708, 709.7] (tests compare it with the correctly rounded
+// exp); below -708 it returns 0 (the true value is under 2^-1021).
+__device__ __forceinline__ double exp_tang(double x) {
+  const double shifter = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+  const double t = fma(x, k32OverLn2, shifter);
+  const int N = __double2loint(t);
+  const double nd = t - shifter;
+  double r = fma(-nd, kLn2Over32Hi, x);  // exact
+  r = fma(-nd, kLn2Over32Lo, r);
+  const double2 S = __ldg(&kExp2J32[N & 31]);
+  double q = fma(1.0 / 720.0, r, 1.0 / 120.0);
+  q = fma(q, r, 1.0 / 24.0);
+  q = fma(q, r, 1.0 / 6.0);
+  q = fma(q, r, 0.5);
+  const double p = fma(q * r, r, r);
+  const double v = S.x + fma(S.x, p, fma(S.y, p, S.y));
+  const double scale = __hiloint2double(((N >> 5) + 1023) << 20, 0);  // 2^m
+  return x < -708.0 ? 0.0 : v * scale;
 }
 
 }  // namespace afmm

@@ -1,8 +1,9 @@
-"""The FP64 matvec logarithm (log_tang, afmm2d_b200/csrc/fast_math.cuh):
-the CPU test restates its steps in Python (exact FMA through fractions) with
-the generated breakpoint table and checks it against the correctly rounded
-log; the GPU test checks the library's own FP64 log-kernel entries against
-the setup's correctly rounded ones."""
+"""The FP64 matvec logarithm and exponential (log_tang, exp_tang in
+afmm2d_b200/csrc/fast_math.cuh): the CPU tests restate their steps in Python
+(exact FMA through fractions) with the generated tables (math_tables.cuh) and
+check them against the correctly rounded functions; the GPU tests check the
+library's own FP64 log and Gaussian kernel entries against the setup's
+correctly rounded ones."""
 import math
 import os
 import re
@@ -16,7 +17,7 @@ CSRC = os.path.join(os.path.dirname(__file__), "..", "afmm2d_b200", "csrc")
 
 
 def _table():
-    s = open(os.path.join(CSRC, "log_table.cuh")).read()
+    s = open(os.path.join(CSRC, "math_tables.cuh")).read()
     inv_block = s[s.index("kLogInvF[129]"):s.index("};")]
     inv = [float.fromhex(v) for v in re.findall(r"(-?0x[0-9a-f.]+p[-+]\d+)", inv_block)]
     ln_block = s[s.index("kLogLnF[129]"):]
@@ -112,3 +113,89 @@ def test_device_log_kernel_entries_within_one_ulp():
     ul = np.abs(fast[far] - exact[far]) / np.spacing(np.abs(exact[far]))
     assert far.sum() > 0.9 * n
     assert ul.max() <= 1.0
+
+
+def _exp_table():
+    s = open(os.path.join(CSRC, "math_tables.cuh")).read()
+    blk = s[s.index("kExp2J32[32]"):]
+    blk = blk[:blk.index("};")]
+    pairs = re.findall(r"\{(-?0x[0-9a-f.]+p[-+]\d+), (-?0x[0-9a-f.]+p[-+]\d+)\}", blk)
+    S = [(float.fromhex(a), float.fromhex(b)) for a, b in pairs]
+    c = {k: float.fromhex(re.search(k + r" = (\S+);", s).group(1)) for k in ("kLn2Over32Hi", "kLn2Over32Lo", "k32OverLn2")}
+    assert len(S) == 32
+    return S, c
+
+
+def exp_tang(x, T):
+    """The device function's operations in IEEE double, one rounding each."""
+    S, c = T
+    shifter = 6755399441055744.0
+    t = _fma(x, c["k32OverLn2"], shifter)
+    nd = t - shifter
+    N = int(nd)
+    r = _fma(-nd, c["kLn2Over32Hi"], x)
+    r = _fma(-nd, c["kLn2Over32Lo"], r)
+    hi, lo = S[N & 31]
+    q = _fma(1.0 / 720.0, r, 1.0 / 120.0)
+    q = _fma(q, r, 1.0 / 24.0)
+    q = _fma(q, r, 1.0 / 6.0)
+    q = _fma(q, r, 0.5)
+    p = _fma(q * r, r, r)
+    v = hi + _fma(hi, p, _fma(lo, p, lo))
+    return 0.0 if x < -708.0 else v * 2.0 ** (N >> 5)
+
+
+def _cr_exp(x):
+    getcontext().prec = 50
+    return float(Decimal(x).exp())
+
+
+def test_exp_table_is_consistent():
+    S, c = _exp_table()
+    getcontext().prec = 50
+    for j in range(32):
+        err = Decimal(S[j][0]) + Decimal(S[j][1]) - (Decimal(2) ** (Decimal(j) / 32))
+        assert abs(err) < Decimal(2) ** -104
+    l1 = Fraction(c["kLn2Over32Hi"])
+    assert l1 * 2 ** 42 == int(l1 * 2 ** 42)
+    assert abs(Decimal(c["kLn2Over32Hi"]) + Decimal(c["kLn2Over32Lo"]) - Decimal(2).ln() / 32) < Decimal(2) ** -95
+
+
+def test_restated_exp_within_one_ulp():
+    T = _exp_table()
+    rng = np.random.default_rng(4)
+    xs = list(-np.exp(rng.uniform(math.log(1e-12), math.log(700.0), 3000)))  # the Gaussian's -R2/param
+    xs += list(rng.uniform(-708.0, 709.0, 1000))
+    xs += [0.0, -0.0, 1e-300, -1e-300, -708.0, 709.0, math.log(2) / 64, -math.log(2) / 64]
+    xs += [(n + 0.5) * math.log(2) / 32 * (1 + s * 2 ** -45) for n in range(-40, 40) for s in (-1, 1)]
+    worst = 0.0
+    for x in xs:
+        x = float(x)
+        worst = max(worst, _ulps(exp_tang(x, T), _cr_exp(x)))
+    assert worst <= 1.0, worst
+    assert exp_tang(-708.5, T) == 0.0
+
+
+@pytest.mark.gpu
+def test_device_gaussian_entries_within_bound():
+    """FP64 Gaussian entries exp(R2 * (-1/param)) against the setup's correctly
+    rounded exp(-R2/param), x = R2/param: the argument carries two roundings
+    (of -1/param and of the product), relative 2^-52 at most, which moves
+    exp(-x) by at most 2|x| ulps; with the exp's own ulp the bound is
+    1 + 2|x| ulps."""
+    import afmm2d_b200 as A
+    rng = np.random.default_rng(9)
+    n = 200000
+    xy1 = rng.uniform(0, 1, (n, 2))
+    xy2 = xy1.copy()
+    xy2[:, 0] += np.exp(rng.uniform(np.log(1e-5), np.log(0.5), n)) * rng.choice([-1.0, 1.0], n)
+    param = 0.01
+    fast = A.kernel_eval("gaussian", 2.0 ** -7, xy1, xy2, mode="fp64", param=param)
+    exact = A.kernel_eval("gaussian", 2.0 ** -7, xy1, xy2, mode="exact", param=param)
+    dx = xy1[:, 0] - xy2[:, 0]
+    x = dx * dx / param
+    ok = exact > 1e-300
+    ul = np.abs(fast[ok] - exact[ok]) / np.spacing(exact[ok])
+    assert ok.sum() > 0.5 * n
+    assert np.all(ul <= 1.0 + 2.0 * x[ok] + 1e-9), float(np.max(ul - 2.0 * x[ok]))
+    assert np.median(ul) == 0.0
