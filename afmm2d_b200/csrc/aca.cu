@@ -105,6 +105,27 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, AcaScrat
   if (ncl <= 0) throw Error{AFMM_CUDA_ERR, "ACA kernel cannot be resident (cluster occupancy 0)"};
   ncl = (int)std::min<long>(ncl, std::max<long>(1, in.nbox));
   const int vsp = rcap - vcap, usp = rcap - ucap;
+  // The spill slots are sized for the worst-case rank min(n1, n2) of every
+  // cluster in flight, which on levels of large ranks (e.g. rank ~900 boxes
+  // of a 16M-point spiral) exceeds the device: keep them within half of the
+  // memory that is free (counting the pool's buffer, released before it
+  // grows) by running fewer clusters; each cluster then takes more boxes in
+  // turn, and the results do not change.
+  {
+    size_t free_b = 0, total_b = 0;
+    AFMM_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t have = (free_b + scratch.work.cap) / 2;
+    const size_t per_cl = (size_t)C * (gslot + sizeof(double) * ((size_t)std::max(vsp, 0) * chunk +
+                                                                 (size_t)std::max(usp, 0) * n1max));
+    const size_t fixed = 2 * sizeof(int32_t) * (size_t)in.nbox * rcap + 4096;
+    if (per_cl > 0) {
+      const long fit = have > fixed ? (long)((have - fixed) / per_cl) : 0;
+      if (fit < 1)
+        throw Error{AFMM_OOM, "ACA working memory of one cluster (" + std::to_string(per_cl) +
+                                  " bytes) exceeds half of the free device memory"};
+      ncl = (int)std::min<long>(ncl, fit);
+    }
+  }
   AcaArgs a;
   a.nbox = (int)in.nbox;
   a.pts = in.pts;
