@@ -120,25 +120,21 @@ __global__ void __launch_bounds__(128) k_p2p_mma(NearView nv, KernelParams kp, c
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const float a32 = (float)kp.a, p32 = (float)kp.param;
-  if (threadIdx.x == 0) {
-    const double2 ab = nv.anchor[b];
-    const float sb = nv.span[b];
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long cbx = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (cbx < 0) continue;
-      const double2 ac = nv.anchor[cbx];
-      s_src[m] = nv.leaf_start[cbx];
-      s_cnt[m] = nv.leaf_cnt[cbx];
-      s_coff[m] = off;
-      s_dx[m] = (float)(ab.x - ac.x);
-      s_dy[m] = (float)(ab.y - ac.y);
-      s_thr[m] = fmaxf(fallback_r2_b<K>(sb, nv.span[cbx]), 1.0e-30f);
-      off += (nv.leaf_cnt[cbx] + 7) >> 3;
-      ++m;
+  if (threadIdx.x < 32) {
+    const NearSlots sl = near_slots<8>(nv, b, threadIdx.x);
+    if (sl.m >= 0) {
+      const double2 ab = nv.anchor[b], ac = nv.anchor[sl.c];
+      s_src[sl.m] = sl.start;
+      s_cnt[sl.m] = sl.cnt;
+      s_coff[sl.m] = sl.off;
+      s_dx[sl.m] = (float)(ab.x - ac.x);
+      s_dy[sl.m] = (float)(ab.y - ac.y);
+      s_thr[sl.m] = fmaxf(fallback_r2_b<K>(nv.span[b], nv.span[sl.c]), 1.0e-30f);
     }
-    s_coff[m] = off;
-    s_ns = m;
+    if (threadIdx.x == 0) {
+      s_coff[sl.ns] = sl.total;
+      s_ns = sl.ns;
+    }
   }
   __syncthreads();
   const int ns = s_ns;
@@ -285,19 +281,17 @@ __global__ void __launch_bounds__(128) k_p2p_dmma(NearView nv, KernelParams kp, 
   const long b = nv.leaf0 + blockIdx.x;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
-  if (threadIdx.x == 0) {
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long cbx = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (cbx < 0) continue;
-      s_src[m] = nv.leaf_start[cbx];
-      s_cnt[m] = nv.leaf_cnt[cbx];
-      s_coff[m] = off;
-      off += (nv.leaf_cnt[cbx] + 3) >> 2;
-      ++m;
+  if (threadIdx.x < 32) {
+    const NearSlots sl = near_slots<4>(nv, b, threadIdx.x);
+    if (sl.m >= 0) {
+      s_src[sl.m] = sl.start;
+      s_cnt[sl.m] = sl.cnt;
+      s_coff[sl.m] = sl.off;
     }
-    s_coff[m] = off;
-    s_ns = m;
+    if (threadIdx.x == 0) {
+      s_coff[sl.ns] = sl.total;
+      s_ns = sl.ns;
+    }
   }
   __syncthreads();
   const int ns = s_ns;

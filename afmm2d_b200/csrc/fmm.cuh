@@ -438,6 +438,49 @@ __device__ __forceinline__ void l2l_row(const LevelView& v, double* __restrict__
   else child_yhat[g] += t;
 }
 
+// Source slots of leaf b's near field (neighbours 0..7, then the leaf itself),
+// fetched by warp 0 in one round of loads instead of a walk by one thread
+// (nine dependent neighbour -> leaf lookups): lane s < 9 reads slot s, the
+// existing slots keep their order (compacted by a ballot), and a slot's
+// offset is the sum of units(count) = ceil(count / UNIT) over the existing
+// slots before it.  In lane s: the source leaf c (-1: no neighbour), its
+// compacted index m (-1 if none), start, count, offset; in every lane the
+// number of existing slots ns and the total of their units.  Warp 0, all 32
+// lanes, only.
+struct NearSlots {
+  long c;
+  int m, start, cnt, off, total, ns;
+};
+
+template <int UNIT>
+__device__ __forceinline__ NearSlots near_slots(const NearView& nv, long b, int lane) {
+  NearSlots r;
+  r.c = -1;
+  r.start = 0;
+  r.cnt = 0;
+  if (lane < 9) {
+    r.c = lane < 8 ? (long)nv.nbr[b * 8 + lane] : b;
+    if (r.c >= 0) {
+      r.start = nv.leaf_start[r.c];
+      r.cnt = nv.leaf_cnt[r.c];
+    }
+  }
+  const bool ok = lane < 9 && r.c >= 0;
+  const unsigned valid = __ballot_sync(0xffffffffu, ok);
+  const int u = ok ? (r.cnt + UNIT - 1) / UNIT : 0;
+  int pre = u;  // inclusive prefix over lanes 0..lane
+#pragma unroll
+  for (int o = 1; o < 16; o <<= 1) {
+    const int t = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += t;
+  }
+  r.off = pre - u;
+  r.total = __shfl_sync(0xffffffffu, pre, 8);
+  r.ns = __popc(valid);
+  r.m = ok ? __popc(valid & ((1u << lane) - 1u)) : -1;
+  return r;
+}
+
 // Near field (src/AFMM2DTree.cpp:1199-1213) of leaf b: neighbours 0..7 and the
 // leaf itself, kernel evaluated on the fly.  Run by one CTA of at least
 // NT * G threads: all source leaves are staged in shared memory (`smem`:
@@ -450,19 +493,17 @@ __device__ __forceinline__ void p2p64_leaf(const NearView& nv, const KernelParam
   __shared__ int s_src[9], s_cnt[9], s_off[10], s_ns;
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
-  if (threadIdx.x == 0) {
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (c < 0) continue;
-      s_src[m] = nv.leaf_start[c];
-      s_cnt[m] = nv.leaf_cnt[c];
-      s_off[m] = off;
-      off += nv.leaf_cnt[c];
-      ++m;
+  if (threadIdx.x < 32) {
+    const NearSlots sl = near_slots<1>(nv, b, threadIdx.x);
+    if (sl.m >= 0) {
+      s_src[sl.m] = sl.start;
+      s_cnt[sl.m] = sl.cnt;
+      s_off[sl.m] = sl.off;
     }
-    s_off[m] = off;
-    s_ns = m;
+    if (threadIdx.x == 0) {
+      s_off[sl.ns] = sl.total;
+      s_ns = sl.ns;
+    }
   }
   __syncthreads();
   const int ns = s_ns;

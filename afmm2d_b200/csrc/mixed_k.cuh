@@ -94,25 +94,21 @@ __global__ void k_p2p32(NearView nv, KernelParams kp, const float* __restrict__ 
   const int n = nv.leaf_cnt[b];
   const int s0 = nv.leaf_start[b];
   const float a32 = (float)kp.a, p32 = (float)kp.param;
-  if (threadIdx.x == 0) {
-    const double2 ab = nv.anchor[b];
-    const float sb = nv.span[b];
-    int m = 0, off = 0;
-    for (int slot = 0; slot < 9; ++slot) {
-      const long c = slot < 8 ? nv.nbr[b * 8 + slot] : b;
-      if (c < 0) continue;
-      const double2 ac = nv.anchor[c];
-      s_src[m] = nv.leaf_start[c];
-      s_cnt[m] = nv.leaf_cnt[c];
-      s_off[m] = off;
-      s_dx[m] = (float)(ab.x - ac.x);
-      s_dy[m] = (float)(ab.y - ac.y);
-      s_thr[m] = fallback_r2<K>(sb, nv.span[c]);
-      off += nv.leaf_cnt[c];
-      ++m;
+  if (threadIdx.x < 32) {
+    const NearSlots sl = near_slots<1>(nv, b, threadIdx.x);
+    if (sl.m >= 0) {
+      const double2 ab = nv.anchor[b], ac = nv.anchor[sl.c];
+      s_src[sl.m] = sl.start;
+      s_cnt[sl.m] = sl.cnt;
+      s_off[sl.m] = sl.off;
+      s_dx[sl.m] = (float)(ab.x - ac.x);
+      s_dy[sl.m] = (float)(ab.y - ac.y);
+      s_thr[sl.m] = fallback_r2<K>(nv.span[b], nv.span[sl.c]);
     }
-    s_off[m] = off;
-    s_ns = m;
+    if (threadIdx.x == 0) {
+      s_off[sl.ns] = sl.total;
+      s_ns = sl.ns;
+    }
   }
   __syncthreads();
   const int ns = s_ns;
