@@ -219,17 +219,23 @@ void aca_level(const AcaLevelIn& in, AcaLevelOut& out, DevArena& arena, AcaScrat
     size_t rest = sizeof(double2) * rmax + sizeof(int) * rmax + 64;
     bool global_factor = fa + rest + sizeof(double) * (size_t)rmax * 32 > budget2;
     size_t base = (global_factor ? 0 : fa) + rest;
-    p.xs = (int)std::min<size_t>(L2P_T, (budget2 - base) / (sizeof(double) * rmax));
+    // with the factor in global memory the solve columns go there too: all
+    // L2P_T threads solve (shared memory would hold only ~26 columns at rank
+    // ~900) and the CTA's shared footprint stays small
+    p.xs = global_factor ? L2P_T : (int)std::min<size_t>(L2P_T, (budget2 - base) / (sizeof(double) * rmax));
     if (p.xs < 1) throw Error{AFMM_BAD_ARG, "box rank " + std::to_string(rmax) + " too large for the L2P solve"};
-    size_t sm = base + sizeof(double) * (size_t)rmax * p.xs;
+    size_t sm = base + (global_factor ? 0 : sizeof(double) * (size_t)rmax * p.xs);
     p.rmax = rmax;
     int grid = (int)in.nbox;
     p.gscratch = nullptr;
+    p.gx = nullptr;
     if (global_factor) {
       grid = (int)std::min<long>(in.nbox, 148 * 8);
       const size_t n_fac = (size_t)grid * rmax * rmax;
-      scratch.factors.reserve(DevScratch::need({sizeof(double) * n_fac}));
+      const size_t n_x = (size_t)grid * rmax * p.xs;
+      scratch.factors.reserve(DevScratch::need({sizeof(double) * n_fac, sizeof(double) * n_x}));
       p.gscratch = scratch.factors.take<double>(n_fac);
+      p.gx = scratch.factors.take<double>(n_x);
     }
     kernel_table(in.kp.id).l2p_run(p, sm, global_factor, grid, s);
     *launches += 1;

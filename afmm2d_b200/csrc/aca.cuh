@@ -64,6 +64,7 @@ struct L2pArgs {
   int xs;            // rows of L2P solved at once (one per thread)
   int rmax;          // largest rank of the level
   double* gscratch;  // gridDim.x * rmax^2 when the factor lives in global memory
+  double* gx;        // gridDim.x * rmax * xs solve columns, with the factor in global memory
 };
 
 struct AcaLevelIn {

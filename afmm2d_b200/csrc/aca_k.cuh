@@ -511,8 +511,11 @@ __global__ void __launch_bounds__(L2P_T) k_l2p(L2pArgs P) {
     const int rr2 = GA ? 0 : ((r * r + 1) & ~1);  // keep the double2 array 16-byte aligned
     double* Am = GA ? P.gscratch + (size_t)blockIdx.x * P.rmax * P.rmax : (double*)smem;  // r x r, row-major
     double2* cxy = (double2*)((double*)smem + rr2);  // r pivot-column points
-    double* X = (double*)(cxy + r);                  // r x xs scratch, one column per solving thread
-    int* perm = (int*)(X + (size_t)r * P.xs);        // r
+    // r x xs scratch, one column per solving thread: shared memory, or with the
+    // factor in global memory (large ranks) a per-CTA global slot, so that every
+    // thread solves and the CTA's small shared footprint lets several CTAs share an SM
+    double* X = GA ? P.gx + (size_t)blockIdx.x * P.rmax * P.xs : (double*)(cxy + r);
+    int* perm = GA ? (int*)(cxy + r) : (int*)(X + (size_t)r * P.xs);  // r
     const int so = P.skel_off[b];
     __syncthreads();
     for (int l = threadIdx.x; l < r; l += L2P_T) {
