@@ -199,3 +199,16 @@ def test_device_gaussian_entries_within_bound():
     assert ok.sum() > 0.5 * n
     assert np.all(ul <= 1.0 + 2.0 * x[ok] + 1e-9), float(np.max(ul - 2.0 * x[ok]))
     assert np.median(ul) == 0.0
+
+
+def test_committed_tables_match_their_generator(tmp_path):
+    """math_tables.cuh is exactly what make_math_tables.py writes."""
+    import importlib.util
+    import shutil
+    src = os.path.join(CSRC, "make_math_tables.py")
+    shutil.copy(src, tmp_path / "make_math_tables.py")
+    spec = importlib.util.spec_from_file_location("make_math_tables_copy", tmp_path / "make_math_tables.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    mod.main()  # writes beside the copy
+    assert (tmp_path / "math_tables.cuh").read_text() == open(os.path.join(CSRC, "math_tables.cuh")).read()
